@@ -1,0 +1,162 @@
+/*
+ * snusolver_b200 -- C-ABI of the B200 numeric factorize-and-solve path of
+ * SnuSolver (a nested-dissection sparse LU without pivoting).
+ *
+ * Plain pointers and sizes only.  Every call returns an snu_status; on error
+ * snu_last_error(h) describes it and no output buffer is left half-written.
+ * A handle owns its plan (host) and its factors (device); the caller owns
+ * every array it passes.  One handle may be used by one thread at a time;
+ * different handles are independent.
+ *
+ * Reference interfaces replaced (paths inside rhrnald/snusolver):
+ *   snu_construct   SnuMat::SnuMat (src/SnuMat.cu:67-112): ordering,
+ *                   structure, allocation and value distribution.
+ *   snu_factorize   the numeric half of SnuMat::solve
+ *                   (src/SnuMat_factorize.cu:213-284, src/kernel_sparse.cu:
+ *                   1011-1037): leaf LU, leaf Schur, separator fronts.
+ *   snu_solve       the solve half of SnuMat::solve
+ *                   (src/SnuMat_factorize.cu:286-356, kernel_sparse.cu:
+ *                   915-944): forward/back substitution and unpermute.
+ *   snu_refactor    new values on the same pattern: the value scatter chain
+ *                   perm_map -> coo_val -> loc_val -> LU_data / MM_buf
+ *                   (src/SnuMat_construct.cu:177-178,
+ *                   src/SnuMat_distribute_data.cu:19-56,
+ *                   src/kernel_sparse.cu:1012-1016).
+ *   snu_read_mtx    read_matrix (src/read_matrix.cpp:50-107).
+ *   snu_get_*       read back the reference's own data layouts (ordering,
+ *                   COO split, leaf LU pattern and values, dense separator
+ *                   blocks) for parity checks; no reference counterpart.
+ */
+#ifndef SNUSOLVER_B200_H
+#define SNUSOLVER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SNU_API __attribute__((visibility("default")))
+#else
+#define SNU_API
+#endif
+
+typedef enum snu_status {
+  SNU_OK = 0,
+  SNU_EINVAL = 1,     /* bad argument, malformed matrix or unsupported input */
+  SNU_ENOMEM = 2,     /* host or device allocation failed / over budget */
+  SNU_ESINGULAR = 3,  /* a non-finite value appeared in the factors */
+  SNU_ETIMEOUT = 4,   /* a bounded device wait gave up */
+  SNU_ECUDA = 5,      /* a CUDA runtime call failed */
+  SNU_ESTATE = 6,     /* call out of order (e.g. solve before factorize) */
+  SNU_ENOTCONV = 7    /* refinement did not reach the tolerance */
+} snu_status;
+
+typedef enum snu_precision {
+  SNU_FP64 = 0,     /* factors and solves in FP64 (reference semantics) */
+  SNU_FP32_IR = 1   /* FP32 factors + FP64 residual iterative refinement */
+} snu_precision;
+
+typedef struct snu_opts {
+  int nleaves;          /* leaves of the separator tree (the reference's MPI
+                           rank count np); power of two, 1..512; default 8 */
+  int precision;        /* snu_precision; default SNU_FP64 */
+  double pivot_eps;     /* static pivot of leaf pivots: |p| < eps -> +-eps
+                           (src/param.h:3, kernel_sparse.cu:742-749); 1e-15 */
+  double ir_tol;        /* FP32_IR: target ||b-Ax||inf/(||A||inf||x||inf+||b||inf);
+                           default 1e-10 */
+  int ir_max_iter;      /* FP32_IR: refinement steps before the FP64 fallback;
+                           default 10 */
+  int device;           /* CUDA device ordinal; default 0 */
+  int64_t mem_budget;   /* bytes of device memory the handle may hold; 0 = no limit */
+  int reserved[8];
+} snu_opts;
+
+typedef struct snu_stats {
+  int n, nnz, nleaves, nfronts, nlevels;
+  int64_t factor_entries;   /* stored factor entries (all fronts) */
+  int64_t device_bytes;     /* device memory held by the handle */
+  double analyze_s;         /* ordering + symbolic (host) */
+  double factor_s;          /* last factorize / refactor, device time */
+  double solve_s;           /* last solve (including refinement), device time */
+  double factor_flops;      /* algorithmic flops of one factorization */
+  int ir_iters;             /* refinement steps of the last solve */
+  int fp64_fallback;        /* 1 if the last solve fell back to FP64 factors */
+  double backward_error;    /* last solve: max over columns of the relative residual */
+  int tiny_pivots;          /* leaf pivots replaced by +-pivot_eps */
+  int reserved[7];
+} snu_stats;
+
+typedef struct snu_handle snu_handle;
+
+SNU_API void snu_default_opts(snu_opts* opts);
+SNU_API snu_status snu_create(snu_handle** h, const snu_opts* opts);
+SNU_API snu_status snu_destroy(snu_handle* h);
+SNU_API const char* snu_last_error(const snu_handle* h);
+SNU_API const char* snu_status_string(snu_status s);
+
+/* Ordering and symbolic structure only (host); no device work. */
+SNU_API snu_status snu_analyze(snu_handle* h, int n, int nnz,
+                               const int* rowptr, const int* colidx);
+/* snu_analyze + device plan + values (host arrays, reference CSR order). */
+SNU_API snu_status snu_construct(snu_handle* h, int n, int nnz,
+                                 const int* rowptr, const int* colidx,
+                                 const double* vals);
+SNU_API snu_status snu_factorize(snu_handle* h);
+/* New values for the same pattern (host array, CSR order), then factorize. */
+SNU_API snu_status snu_refactor(snu_handle* h, const double* vals);
+/* X = A^-1 B for nrhs columns; B, X column-major host arrays with leading
+   dimension ldb >= n.  X may alias B. */
+SNU_API snu_status snu_solve(snu_handle* h, const double* B, double* X,
+                             int nrhs, int ldb);
+/* Same with device arrays on a CUDA stream (cudaStream_t, may be NULL). */
+SNU_API snu_status snu_solve_device(snu_handle* h, const double* dB,
+                                    double* dX, int nrhs, int ldb,
+                                    void* stream);
+SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st);
+
+/* ---- parity read-back in the reference's layouts (host arrays) ---- */
+/* order[n] (order[old] = new) and sizes[2*nleaves-1]. */
+SNU_API snu_status snu_get_ordering(const snu_handle* h, int* order,
+                                    int* sizes);
+/* block_start[2*nleaves], block_size[2*nleaves] (global, heap numbering). */
+SNU_API snu_status snu_get_blocks(const snu_handle* h, int* block_start,
+                                  int* block_size);
+/* perm_map[nnz], coo_r[nnz], coo_c[nnz] (SnuMat_construct.cu:40-159). */
+SNU_API snu_status snu_get_coo(const snu_handle* h, int* perm_map, int* coo_r,
+                               int* coo_c);
+/* info[8] = {leaf, leaf_size, dense_row, core_n, core_nnz, LU_nnz, 0, 0} of
+   the leaf owned by reference rank `rank`.  LU_nnz is 0 until the pattern
+   is requested with snu_get_leaf_pattern. */
+SNU_API snu_status snu_get_leaf_info(snu_handle* h, int rank, int* info);
+/* LU_rowptr[core_n+1], LU_colidx[LU_nnz], LU_diag[core_n],
+   LU_bias[leaf_size], core_map[core_nnz] (kernel_sparse.cu:368-596).
+   Any pointer may be NULL. */
+SNU_API snu_status snu_get_leaf_pattern(snu_handle* h, int rank,
+                                        int* LU_rowptr, int* LU_colidx,
+                                        int* LU_diag, int* LU_bias,
+                                        int* core_map);
+/* Leaf factor values in the LU pattern slots, LU_data[LU_nnz], as the
+   reference holds them after core_run (kernel_sparse.cu:1011-1037). */
+SNU_API snu_status snu_get_leaf_factor(snu_handle* h, int rank,
+                                       double* LU_data);
+/* Dense separator factor block LU[{i,j}] (column-major, bs[i] x bs[j]) for
+   j == i or j an ancestor of i (the U part) or i an ancestor of j (the L
+   part), as the owner rank holds it after SnuMat::solve. */
+SNU_API snu_status snu_get_dense_block(snu_handle* h, int i, int j,
+                                       double* out);
+
+/* ---- MatrixMarket input (read_matrix.cpp semantics) ---- */
+/* Reads a coordinate file into CSR arrays allocated with malloc (free with
+   snu_free).  expand_symmetric mirrors symmetric files (reference: off). */
+SNU_API snu_status snu_read_mtx(const char* path, int expand_symmetric,
+                                int* n, int* nnz, int** rowptr, int** colidx,
+                                double** vals);
+SNU_API void snu_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SNUSOLVER_B200_H */

@@ -1,0 +1,404 @@
+// C-ABI of snusolver_b200 (declared in include/snusolver_b200.h).
+#include "../../include/snusolver_b200.h"
+
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "host/fronts.h"
+#include "host/structure.h"
+
+// CUDA runtime calls used directly here (host staging for snu_solve).
+#include <cuda_runtime_api.h>
+
+struct snu_handle {
+  snu_opts opts;
+  std::string err;
+  snu::Structure S;
+  snu::FrontPlan FP;
+  std::vector<int> rowptr, colidx;
+  std::unique_ptr<snu::Engine> eng;
+  int state = 0;  // 0 empty, 1 analyzed, 2 constructed, 3 factorized
+  snu_stats stats;
+  double* dB = nullptr;  // staging for host solves
+  size_t dcap = 0;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+snu_status fail(snu_handle* h, snu_status s, const std::string& msg) {
+  if (h)
+    h->err = msg;
+  else
+    g_err = msg;
+  return s;
+}
+
+snu_status from_engine(snu_handle* h, int rc) {
+  if (rc == snu::ENG_OK) return SNU_OK;
+  h->err = h->eng ? h->eng->error() : std::string("engine error");
+  switch (rc) {
+    case snu::ENG_EINVAL: return SNU_EINVAL;
+    case snu::ENG_ENOMEM: return SNU_ENOMEM;
+    case snu::ENG_ESINGULAR: return SNU_ESINGULAR;
+    case snu::ENG_ETIMEOUT: return SNU_ETIMEOUT;
+    case snu::ENG_ESTATE: return SNU_ESTATE;
+    case snu::ENG_ENOTCONV: return SNU_ENOTCONV;
+    default: return SNU_ECUDA;
+  }
+}
+
+double now_s() {
+  return std::chrono::duration<double>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+bool valid_csr(int n, int nnz, const int* rowptr, const int* colidx,
+               std::string& why) {
+  if (n <= 0) return why = "n must be positive", false;
+  if (nnz < 0) return why = "nnz must be non-negative", false;
+  if (!rowptr || (nnz > 0 && !colidx)) return why = "null CSR array", false;
+  if (rowptr[0] != 0 || rowptr[n] != nnz)
+    return why = "rowptr must start at 0 and end at nnz", false;
+  for (int i = 0; i < n; i++)
+    if (rowptr[i + 1] < rowptr[i]) return why = "rowptr not monotone", false;
+  for (int k = 0; k < nnz; k++)
+    if (colidx[k] < 0 || colidx[k] >= n)
+      return why = "column index out of range", false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+SNU_API const char* snu_status_string(snu_status s) {
+  switch (s) {
+    case SNU_OK: return "SNU_OK";
+    case SNU_EINVAL: return "SNU_EINVAL";
+    case SNU_ENOMEM: return "SNU_ENOMEM";
+    case SNU_ESINGULAR: return "SNU_ESINGULAR";
+    case SNU_ETIMEOUT: return "SNU_ETIMEOUT";
+    case SNU_ECUDA: return "SNU_ECUDA";
+    case SNU_ESTATE: return "SNU_ESTATE";
+    case SNU_ENOTCONV: return "SNU_ENOTCONV";
+  }
+  return "unknown status";
+}
+
+SNU_API void snu_default_opts(snu_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->nleaves = 8;
+  o->precision = SNU_FP64;
+  o->pivot_eps = 1e-15;
+  o->ir_tol = 1e-10;
+  o->ir_max_iter = 10;
+  o->device = 0;
+  o->mem_budget = 0;
+}
+
+SNU_API snu_status snu_create(snu_handle** out, const snu_opts* opts) {
+  if (!out) return fail(nullptr, SNU_EINVAL, "null handle pointer");
+  *out = nullptr;
+  snu_opts o;
+  snu_default_opts(&o);
+  if (opts) o = *opts;
+  if (o.nleaves < 2 || o.nleaves > 512 || (o.nleaves & (o.nleaves - 1)))
+    return fail(nullptr, SNU_EINVAL, "nleaves must be a power of two in 2..512");
+  if (o.precision != SNU_FP64 && o.precision != SNU_FP32_IR)
+    return fail(nullptr, SNU_EINVAL, "unknown precision");
+  if (!(o.pivot_eps >= 0) || !(o.ir_tol > 0) || o.ir_max_iter < 0)
+    return fail(nullptr, SNU_EINVAL, "bad tolerance options");
+  snu_handle* h = new (std::nothrow) snu_handle();
+  if (!h) return fail(nullptr, SNU_ENOMEM, "out of host memory");
+  h->opts = o;
+  std::memset(&h->stats, 0, sizeof h->stats);
+  *out = h;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_destroy(snu_handle* h) {
+  if (!h) return SNU_OK;
+  if (h->dB) cudaFree(h->dB);
+  h->eng.reset();
+  delete h;
+  return SNU_OK;
+}
+
+SNU_API const char* snu_last_error(const snu_handle* h) {
+  return h ? h->err.c_str() : g_err.c_str();
+}
+
+SNU_API snu_status snu_analyze(snu_handle* h, int n, int nnz,
+                               const int* rowptr, const int* colidx) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  std::string why;
+  if (!valid_csr(n, nnz, rowptr, colidx, why)) return fail(h, SNU_EINVAL, why);
+  double t0 = now_s();
+  std::vector<int> order, sizes;
+  std::string err;
+  if (snu::compute_ordering(n, nnz, rowptr, colidx, h->opts.nleaves, order,
+                            sizes, err))
+    return fail(h, SNU_EINVAL, err);
+  if (snu::build_structure(n, nnz, rowptr, colidx, h->opts.nleaves, order,
+                           sizes, h->S, err))
+    return fail(h, SNU_EINVAL, err);
+  h->rowptr.assign(rowptr, rowptr + n + 1);
+  h->colidx.assign(colidx, colidx + nnz);
+  h->state = 1;
+  h->eng.reset();
+  h->stats.n = n;
+  h->stats.nnz = nnz;
+  h->stats.nleaves = h->opts.nleaves;
+  h->stats.analyze_s = now_s() - t0;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_construct(snu_handle* h, int n, int nnz,
+                                 const int* rowptr, const int* colidx,
+                                 const double* vals) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (nnz > 0 && !vals) return fail(h, SNU_EINVAL, "null values");
+  snu_status s = snu_analyze(h, n, nnz, rowptr, colidx);
+  if (s != SNU_OK) return s;
+  double t0 = now_s();
+  std::string err;
+  snu::FrontOptions fo;
+  if (snu::build_front_plan(h->S, fo, h->FP, err)) {
+    h->state = 1;
+    return fail(h, SNU_EINVAL, err);
+  }
+  snu::EngineOptions eo;
+  eo.device = h->opts.device;
+  eo.pivot_eps = h->opts.pivot_eps;
+  eo.ir_tol = h->opts.ir_tol;
+  eo.ir_max_iter = h->opts.ir_max_iter;
+  eo.mem_budget = h->opts.mem_budget;
+  h->eng = snu::make_engine(eo, err);
+  if (!h->eng) return fail(h, SNU_ECUDA, "CUDA engine unavailable: " + err);
+  int rc = h->eng->setup(h->S, h->FP, rowptr, colidx);
+  if (rc) return from_engine(h, rc);
+  rc = h->eng->set_values(vals);
+  if (rc) return from_engine(h, rc);
+  h->stats.analyze_s += now_s() - t0;
+  h->stats.nfronts = h->FP.nfronts;
+  h->stats.nlevels = h->FP.nlevels;
+  h->stats.factor_entries = h->FP.factor_entries;
+  h->stats.factor_flops = h->FP.flops;
+  h->stats.device_bytes = h->eng->device_bytes();
+  h->state = 2;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_factorize(snu_handle* h) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 2) return fail(h, SNU_ESTATE, "factorize before construct");
+  double sec = 0;
+  int prec = h->opts.precision == SNU_FP64 ? 0 : 1;
+  int rc = h->eng->factorize(prec, &sec);
+  h->stats.tiny_pivots = h->eng->tiny_pivots();
+  h->stats.device_bytes = h->eng->device_bytes();
+  if (rc) {
+    h->state = 2;
+    return from_engine(h, rc);
+  }
+  h->stats.factor_s = sec;
+  h->state = 3;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_refactor(snu_handle* h, const double* vals) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 2) return fail(h, SNU_ESTATE, "refactor before construct");
+  if (h->S.nnz > 0 && !vals) return fail(h, SNU_EINVAL, "null values");
+  int rc = h->eng->set_values(vals);
+  if (rc) return from_engine(h, rc);
+  h->state = 2;
+  return snu_factorize(h);
+}
+
+SNU_API snu_status snu_solve_device(snu_handle* h, const double* dB,
+                                    double* dX, int nrhs, int ldb,
+                                    void* stream) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 3) return fail(h, SNU_ESTATE, "solve before factorize");
+  if (!dB || !dX || nrhs <= 0 || ldb < h->S.n)
+    return fail(h, SNU_EINVAL, "bad right-hand side arguments");
+  snu::SolveReport rep;
+  int prec = h->opts.precision == SNU_FP64 ? 0 : 1;
+  int rc = h->eng->solve(dB, dX, nrhs, ldb, stream, prec, &rep);
+  if (rc) return from_engine(h, rc);
+  h->stats.solve_s = rep.seconds;
+  h->stats.ir_iters = rep.ir_iters;
+  h->stats.fp64_fallback = rep.fp64_fallback;
+  h->stats.backward_error = rep.backward_error;
+  h->stats.device_bytes = h->eng->device_bytes();
+  if (prec == 1 && !(rep.backward_error <= h->opts.ir_tol))
+    return fail(h, SNU_ENOTCONV,
+                "refinement stopped at backward error " +
+                    std::to_string(rep.backward_error));
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_solve(snu_handle* h, const double* B, double* X,
+                             int nrhs, int ldb) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 3) return fail(h, SNU_ESTATE, "solve before factorize");
+  if (!B || !X || nrhs <= 0 || ldb < h->S.n)
+    return fail(h, SNU_EINVAL, "bad right-hand side arguments");
+  const int n = h->S.n;
+  size_t need = (size_t)n * nrhs * 2;
+  if (need > h->dcap) {
+    if (h->dB) cudaFree(h->dB);
+    h->dB = nullptr;
+    h->dcap = 0;
+    if (cudaMalloc((void**)&h->dB, need * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(h, SNU_ENOMEM, "cannot allocate right-hand side staging");
+    }
+    h->dcap = need;
+  }
+  double* dB = h->dB;
+  double* dX = h->dB + (size_t)n * nrhs;
+  for (int r = 0; r < nrhs; r++)
+    if (cudaMemcpy(dB + (size_t)r * n, B + (size_t)r * ldb, sizeof(double) * n,
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(h, SNU_ECUDA, "host to device copy failed");
+  snu_status s = snu_solve_device(h, dB, dX, nrhs, n, nullptr);
+  if (s != SNU_OK && s != SNU_ENOTCONV) return s;
+  for (int r = 0; r < nrhs; r++)
+    if (cudaMemcpy(X + (size_t)r * ldb, dX + (size_t)r * n, sizeof(double) * n,
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(h, SNU_ECUDA, "device to host copy failed");
+  return s;
+}
+
+SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st) {
+  if (!h || !st) return fail(nullptr, SNU_EINVAL, "null argument");
+  *st = h->stats;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_get_ordering(const snu_handle* h, int* order,
+                                    int* sizes) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 1) return fail(const_cast<snu_handle*>(h), SNU_ESTATE, "not analyzed");
+  if (order) std::memcpy(order, h->S.order.data(), sizeof(int) * h->S.n);
+  if (sizes)
+    std::memcpy(sizes, h->S.sizes.data(), sizeof(int) * h->S.sizes.size());
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_get_blocks(const snu_handle* h, int* block_start,
+                                  int* block_size) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 1) return fail(const_cast<snu_handle*>(h), SNU_ESTATE, "not analyzed");
+  size_t m = h->S.block_start.size();
+  if (block_start) std::memcpy(block_start, h->S.block_start.data(), sizeof(int) * m);
+  if (block_size) std::memcpy(block_size, h->S.block_size.data(), sizeof(int) * m);
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_get_coo(const snu_handle* h, int* perm_map, int* coo_r,
+                               int* coo_c) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 1) return fail(const_cast<snu_handle*>(h), SNU_ESTATE, "not analyzed");
+  size_t m = h->S.perm_map.size();
+  if (perm_map) std::memcpy(perm_map, h->S.perm_map.data(), sizeof(int) * m);
+  if (coo_r) std::memcpy(coo_r, h->S.coo_r.data(), sizeof(int) * m);
+  if (coo_c) std::memcpy(coo_c, h->S.coo_c.data(), sizeof(int) * m);
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_get_leaf_info(snu_handle* h, int rank, int* info) {
+  if (!h || !info) return fail(h, SNU_EINVAL, "null argument");
+  if (h->state < 1) return fail(h, SNU_ESTATE, "not analyzed");
+  if (rank < 0 || rank >= h->S.np) return fail(h, SNU_EINVAL, "bad rank");
+  const snu::LeafStructure& L = h->S.leaves[rank];
+  int v[8] = {L.leaf, L.leaf_size, L.dense_row, L.core_n,
+              L.core_nnz, L.LU_nnz, 0, 0};
+  std::memcpy(info, v, sizeof v);
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_get_leaf_pattern(snu_handle* h, int rank,
+                                        int* LU_rowptr, int* LU_colidx,
+                                        int* LU_diag, int* LU_bias,
+                                        int* core_map) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 1) return fail(h, SNU_ESTATE, "not analyzed");
+  if (rank < 0 || rank >= h->S.np) return fail(h, SNU_EINVAL, "bad rank");
+  snu::LeafStructure& L = h->S.leaves[rank];
+  if (L.LU_rowptr.empty()) {
+    std::string err;
+    if (snu::leaf_symbfact(L, err)) return fail(h, SNU_EINVAL, err);
+  }
+  if (LU_rowptr) std::memcpy(LU_rowptr, L.LU_rowptr.data(), sizeof(int) * (L.core_n + 1));
+  if (LU_colidx) std::memcpy(LU_colidx, L.LU_colidx.data(), sizeof(int) * L.LU_nnz);
+  if (LU_diag) std::memcpy(LU_diag, L.LU_diag.data(), sizeof(int) * L.core_n);
+  if (LU_bias) std::memcpy(LU_bias, L.LU_bias.data(), sizeof(int) * L.leaf_size);
+  if (core_map) std::memcpy(core_map, L.core_map.data(), sizeof(int) * L.core_nnz);
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_get_leaf_factor(snu_handle* h, int rank,
+                                       double* LU_data) {
+  if (!h || !LU_data) return fail(h, SNU_EINVAL, "null argument");
+  if (h->state < 3) return fail(h, SNU_ESTATE, "not factorized");
+  if (rank < 0 || rank >= h->S.np) return fail(h, SNU_EINVAL, "bad rank");
+  snu::LeafStructure& L = h->S.leaves[rank];
+  if (L.LU_rowptr.empty()) {
+    std::string err;
+    if (snu::leaf_symbfact(L, err)) return fail(h, SNU_EINVAL, err);
+  }
+  return from_engine(h, h->eng->leaf_factor(h->S, rank, LU_data));
+}
+
+SNU_API snu_status snu_get_dense_block(snu_handle* h, int i, int j,
+                                       double* out) {
+  if (!h || !out) return fail(h, SNU_EINVAL, "null argument");
+  if (h->state < 3) return fail(h, SNU_ESTATE, "not factorized");
+  if (i < 1 || j < 1 || i >= h->S.np || j >= h->S.np)
+    return fail(h, SNU_EINVAL, "blocks must be separators (1..nleaves-1)");
+  return from_engine(h, h->eng->dense_block(h->S, i, j, out));
+}
+
+SNU_API snu_status snu_read_mtx(const char* path, int expand_symmetric,
+                                int* n, int* nnz, int** rowptr, int** colidx,
+                                double** vals) {
+  if (!path || !n || !nnz || !rowptr || !colidx || !vals)
+    return fail(nullptr, SNU_EINVAL, "null argument");
+  snu::Csr A;
+  std::string err;
+  if (snu::read_mtx(path, A, expand_symmetric != 0, err))
+    return fail(nullptr, SNU_EINVAL, err);
+  *n = A.n;
+  *nnz = A.nnz;
+  *rowptr = (int*)std::malloc(sizeof(int) * (A.n + 1));
+  *colidx = (int*)std::malloc(sizeof(int) * std::max(1, A.nnz));
+  *vals = (double*)std::malloc(sizeof(double) * std::max(1, A.nnz));
+  if (!*rowptr || !*colidx || !*vals) {
+    std::free(*rowptr);
+    std::free(*colidx);
+    std::free(*vals);
+    return fail(nullptr, SNU_ENOMEM, "out of host memory");
+  }
+  std::memcpy(*rowptr, A.rowptr.data(), sizeof(int) * (A.n + 1));
+  if (A.nnz) {
+    std::memcpy(*colidx, A.colidx.data(), sizeof(int) * A.nnz);
+    std::memcpy(*vals, A.data.data(), sizeof(double) * A.nnz);
+  }
+  return SNU_OK;
+}
+
+SNU_API void snu_free(void* p) { std::free(p); }
+
+}  // extern "C"

@@ -1,0 +1,400 @@
+// Device kernels of the multifrontal factorization and solve (sm_100a).
+//
+// All fronts live in one arena, column-major with their own leading
+// dimension.  Kernels are batched over the fronts of one tree level; every
+// launch takes precomputed task lists so a whole factorization is a fixed
+// sequence of launches (capturable in a CUDA graph).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace snu {
+
+constexpr int NB = 64;  // panel width of the blocked partial factorization
+constexpr int TB = 64;  // tile height of the blocked triangular solves
+
+struct FrontDev {
+  int p, q, ld, parent;
+  int guard, pad0;
+  int64_t off;      // arena offset of F
+  int64_t idx_off;  // into gidx
+  int64_t rel_off;  // into rel
+  int64_t w_off;    // solve work offset (elements per right-hand side)
+};
+
+struct GemmProb {
+  int m, n, k;
+  int lda, ldb, ldc;
+  int64_t a, b, c;  // element offsets from the A, B, C base pointers
+};
+
+struct GemmTile {
+  int prob, tm, tn;
+};
+
+struct EaTask {
+  int child, j;
+};
+
+struct PanelTask {
+  int front, kind, chunk;  // kind 0: rows of the L panel; 1: columns of U
+};
+
+// ---------------------------------------------------------------- assembly
+
+// F[pos[i]] = vals[vidx[i]]: original entries into their fronts (the
+// reference's value chain A.data -> coo_val -> loc_val -> LU_data / MM_buf,
+// SnuMat_construct.cu:177-178, SnuMat_distribute_data.cu:19-56,
+// kernel_sparse.cu:1012-1016, composed once on the host).
+template <typename T>
+__global__ void k_assemble(const int64_t* __restrict__ pos,
+                           const int* __restrict__ vidx,
+                           const double* __restrict__ vals, T* __restrict__ F,
+                           int64_t count) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (; i < count; i += stride) F[pos[i]] = (T)vals[vidx[i]];
+}
+
+// Extend-add: column j of a child's update matrix F22 is added into its
+// parent through the child's relative index map (core_GEMM scatter +
+// core_reduction + core_update, kernel_sparse.cu:54-90, 953-994; the
+// separator-level reduction + vectorAdd, SnuMat_factorize.cu:22-27, 78-124).
+template <typename T>
+__global__ void k_extend_add(const EaTask* __restrict__ tasks,
+                             const FrontDev* __restrict__ fr,
+                             const int* __restrict__ rel, T* __restrict__ F) {
+  const EaTask t = tasks[blockIdx.x];
+  const FrontDev c = fr[t.child];
+  const FrontDev pf = fr[c.parent];
+  const int* r = rel + c.rel_off;
+  const T* src = F + c.off + (int64_t)(c.p + t.j) * c.ld + c.p;
+  T* dst = F + pf.off + (int64_t)r[t.j] * pf.ld;
+  for (int i = threadIdx.x; i < c.q; i += blockDim.x) dst[r[i]] += src[i];
+}
+
+// ------------------------------------------------- blocked partial LU steps
+
+// LU without pivoting of the kb x kb diagonal block at (k0, k0) of every
+// active front, in shared memory.  Leaf fronts apply the reference's static
+// pivot (|p| < eps -> +-eps, kernel_sparse.cu:742-749); separator fronts do
+// not guard, like cusolverDnDgetrf without ipiv (kernel_cuda.cu:67).
+// flags[0] counts replaced pivots, flags[1] is set on a zero or non-finite
+// pivot.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_diag_lu(const int* __restrict__ active, const FrontDev* __restrict__ fr,
+              T* __restrict__ F, int k0, double eps, int* flags) {
+  __shared__ T D[NB * NB];
+  const FrontDev f = fr[active[blockIdx.x]];
+  const int kb = min(NB, f.p - k0);
+  T* base = F + f.off + k0 + (int64_t)k0 * f.ld;
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+    int i = e % kb, j = e / kb;
+    D[i + j * NB] = base[i + (int64_t)j * f.ld];
+  }
+  __syncthreads();
+  const T teps = (T)eps;
+  for (int kk = 0; kk < kb; kk++) {
+    if (threadIdx.x == 0) {
+      T piv = D[kk + kk * NB];
+      if (f.guard && piv < teps && piv > -teps) {
+        piv = piv < (T)0 ? -teps : teps;
+        D[kk + kk * NB] = piv;
+        atomicAdd(flags, 1);
+      }
+      if (!(piv != (T)0) || !isfinite((double)piv)) flags[1] = 1;
+    }
+    __syncthreads();
+    const T piv = D[kk + kk * NB];
+    for (int i = kk + 1 + threadIdx.x; i < kb; i += blockDim.x)
+      D[i + kk * NB] /= piv;
+    __syncthreads();
+    const int m = kb - kk - 1;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      int i = kk + 1 + e % m, j = kk + 1 + e / m;
+      D[i + j * NB] -= D[i + kk * NB] * D[kk + j * NB];
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+    int i = e % kb, j = e / kb;
+    base[i + (int64_t)j * f.ld] = D[i + j * NB];
+  }
+}
+
+// Panel solves after the diagonal block: rows below it become
+// L = A U_D^-1 (trsm right/upper/non-unit, kernel_cuda.cu:98-121) and
+// columns right of it become U = L_D^-1 A (trsm left/lower/unit,
+// kernel_cuda.cu:74-97).  One thread per row or column.
+template <typename T>
+__global__ void __launch_bounds__(128)
+    k_panel_trsm(const PanelTask* __restrict__ tasks,
+                 const FrontDev* __restrict__ fr, T* __restrict__ F, int k0) {
+  __shared__ T D[NB * NB];
+  const PanelTask t = tasks[blockIdx.x];
+  const FrontDev f = fr[t.front];
+  const int kb = min(NB, f.p - k0);
+  const int dim = f.p + f.q;
+  const T* dsrc = F + f.off + k0 + (int64_t)k0 * f.ld;
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+    int i = e % kb, j = e / kb;
+    D[i + j * NB] = dsrc[i + (int64_t)j * f.ld];
+  }
+  __syncthreads();
+  const int idx = k0 + kb + t.chunk * blockDim.x + threadIdx.x;
+  if (idx >= dim) return;
+  if (t.kind == 0) {
+    T* row = F + f.off + idx + (int64_t)k0 * f.ld;
+    for (int j = 0; j < kb; j++) {
+      T s = row[(int64_t)j * f.ld];
+      for (int i = 0; i < j; i++) s -= row[(int64_t)i * f.ld] * D[i + j * NB];
+      row[(int64_t)j * f.ld] = s / D[j + j * NB];
+    }
+  } else {
+    T* col = F + f.off + k0 + (int64_t)idx * f.ld;
+    for (int i = 1; i < kb; i++) {
+      T s = col[i];
+      for (int j = 0; j < i; j++) s -= D[i + j * NB] * col[j];
+      col[i] = s;
+    }
+  }
+}
+
+// ------------------------------------------------------------ batched GEMM
+
+// C -= A B (mode 0) or C = A B (mode 1) for a list of column-major
+// problems; one CTA per BM x BN tile (the reference's cublasDgemm with
+// alpha = -1, beta = 1, kernel_cuda.cu:147-176, batched over fronts).
+template <typename T, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+    k_gemm(const GemmTile* __restrict__ tiles,
+           const GemmProb* __restrict__ probs, const T* __restrict__ Abase,
+           const T* __restrict__ Bbase, T* __restrict__ Cbase, int mode) {
+  constexpr int NX = BM / TM, NY = BN / TN, NT = NX * NY;
+  __shared__ T As[BK][BM + 1];
+  __shared__ T Bs[BK][BN + 1];
+  const GemmTile tl = tiles[blockIdx.x];
+  const GemmProb P = probs[tl.prob];
+  const int m0 = tl.tm * BM, n0 = tl.tn * BN;
+  const T* A = Abase + P.a;
+  const T* B = Bbase + P.b;
+  T* C = Cbase + P.c;
+  const int tid = threadIdx.x, tx = tid % NX, ty = tid / NX;
+  T acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; i++)
+#pragma unroll
+    for (int j = 0; j < TN; j++) acc[i][j] = (T)0;
+  for (int k0 = 0; k0 < P.k; k0 += BK) {
+    for (int e = tid; e < BM * BK; e += NT) {
+      int i = e % BM, l = e / BM, gi = m0 + i, gl = k0 + l;
+      As[l][i] = (gi < P.m && gl < P.k) ? A[gi + (int64_t)gl * P.lda] : (T)0;
+    }
+    for (int e = tid; e < BK * BN; e += NT) {
+      int l = e % BK, j = e / BK, gl = k0 + l, gj = n0 + j;
+      Bs[l][j] = (gl < P.k && gj < P.n) ? B[gl + (int64_t)gj * P.ldb] : (T)0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < BK; l++) {
+      T a[TM], b[TN];
+#pragma unroll
+      for (int i = 0; i < TM; i++) a[i] = As[l][tx + i * NX];
+#pragma unroll
+      for (int j = 0; j < TN; j++) b[j] = Bs[l][ty + j * NY];
+#pragma unroll
+      for (int i = 0; i < TM; i++)
+#pragma unroll
+        for (int j = 0; j < TN; j++) acc[i][j] += a[i] * b[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < TN; j++) {
+    int gj = n0 + ty + j * NY;
+    if (gj >= P.n) continue;
+#pragma unroll
+    for (int i = 0; i < TM; i++) {
+      int gi = m0 + tx + i * NX;
+      if (gi >= P.m) continue;
+      T* c = C + gi + (int64_t)gj * P.ldc;
+      *c = mode ? acc[i][j] : *c - acc[i][j];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ solves
+
+// Work vectors: front f holds dim x nrhs values at W + w_off * nrhs.
+template <typename T>
+__global__ void k_solve_init(const int* __restrict__ list,
+                             const FrontDev* __restrict__ fr,
+                             const int* __restrict__ gidx,
+                             const double* __restrict__ B, int ldb, int nrhs,
+                             T* __restrict__ W) {
+  const FrontDev f = fr[list[blockIdx.y]];
+  const int dim = f.p + f.q;
+  T* w = W + f.w_off * nrhs;
+  const int* g = gidx + f.idx_off;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < dim * nrhs;
+       e += gridDim.x * blockDim.x) {
+    int t = e % dim, r = e / dim;
+    w[t + (int64_t)r * dim] = t < f.p ? (T)B[g[t] + (int64_t)r * ldb] : (T)0;
+  }
+}
+
+// Update vectors of children (their Q rows after the forward sweep) are
+// added into the parent's work vector, in child-rank order.
+template <typename T>
+__global__ void k_solve_ea(const int* __restrict__ list,
+                           const FrontDev* __restrict__ fr,
+                           const int* __restrict__ rel, int nrhs,
+                           T* __restrict__ W) {
+  const FrontDev c = fr[list[blockIdx.x]];
+  const FrontDev pf = fr[c.parent];
+  const int dimc = c.p + c.q, dimp = pf.p + pf.q;
+  const T* src = W + c.w_off * nrhs;
+  T* dst = W + pf.w_off * nrhs;
+  const int* r = rel + c.rel_off;
+  for (int e = threadIdx.x; e < c.q * nrhs; e += blockDim.x) {
+    int i = e % c.q, k = e / c.q;
+    dst[r[i] + (int64_t)k * dimp] += src[c.p + i + (int64_t)k * dimc];
+  }
+}
+
+// Solve of one kb x kb diagonal tile for every right-hand side: unit lower
+// (forward, upper = 0) or non-unit upper (backward, upper = 1).  One warp
+// per right-hand side, column-oriented so each step is one warp-wide axpy.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_solve_diag(const int* __restrict__ active,
+                 const FrontDev* __restrict__ fr, const T* __restrict__ F,
+                 int k0, int nrhs, int upper, T* __restrict__ W) {
+  __shared__ T D[TB * TB];
+  __shared__ T x[8][TB];
+  const FrontDev f = fr[active[blockIdx.x]];
+  const int kb = min(TB, f.p - k0);
+  const int dim = f.p + f.q;
+  const T* src = F + f.off + k0 + (int64_t)k0 * f.ld;
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+    int i = e % kb, j = e / kb;
+    D[i + j * TB] = src[i + (int64_t)j * f.ld];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  T* Wf = W + f.w_off * nrhs;
+  for (int r = warp; r < nrhs; r += blockDim.x / 32) {
+    T* w = Wf + (int64_t)r * dim + k0;
+    for (int i = lane; i < kb; i += 32) x[warp][i] = w[i];
+    __syncwarp();
+    if (!upper) {
+      for (int j = 0; j < kb; j++) {
+        T y = x[warp][j];
+        for (int i = j + 1 + lane; i < kb; i += 32) x[warp][i] -= D[i + j * TB] * y;
+        __syncwarp();
+      }
+    } else {
+      for (int j = kb - 1; j >= 0; j--) {
+        T y = x[warp][j] / D[j + j * TB];
+        __syncwarp();
+        if (lane == 0) x[warp][j] = y;
+        for (int i = lane; i < j; i += 32) x[warp][i] -= D[i + j * TB] * y;
+        __syncwarp();
+      }
+    }
+    for (int i = lane; i < kb; i += 32) w[i] = x[warp][i];
+    __syncwarp();
+  }
+}
+
+// Backward sweep helpers: X_Q of every front is gathered into the Q rows of
+// its work vector; after the sweep X_P is scattered to the solution.
+template <typename T>
+__global__ void k_solve_gather_q(const int* __restrict__ list,
+                                 const FrontDev* __restrict__ fr,
+                                 const int* __restrict__ gidx,
+                                 const double* __restrict__ X, int ldx,
+                                 int nrhs, T* __restrict__ W) {
+  const FrontDev f = fr[list[blockIdx.y]];
+  const int dim = f.p + f.q;
+  T* w = W + f.w_off * nrhs;
+  const int* g = gidx + f.idx_off;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < f.q * nrhs;
+       e += gridDim.x * blockDim.x) {
+    int t = e % f.q, r = e / f.q;
+    w[f.p + t + (int64_t)r * dim] = (T)X[g[f.p + t] + (int64_t)r * ldx];
+  }
+}
+
+template <typename T>
+__global__ void k_solve_scatter_p(const int* __restrict__ list,
+                                  const FrontDev* __restrict__ fr,
+                                  const int* __restrict__ gidx,
+                                  const T* __restrict__ W, int nrhs,
+                                  double* __restrict__ X, int ldx) {
+  const FrontDev f = fr[list[blockIdx.y]];
+  const int dim = f.p + f.q;
+  const T* w = W + f.w_off * nrhs;
+  const int* g = gidx + f.idx_off;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < f.p * nrhs;
+       e += gridDim.x * blockDim.x) {
+    int t = e % f.p, r = e / f.p;
+    X[g[t] + (int64_t)r * ldx] = (double)w[t + (int64_t)r * dim];
+  }
+}
+
+// ------------------------------------------------ FP64 refinement helpers
+
+// R = B - A X on the original CSR (FP64), one thread per row.
+__global__ void k_residual(int n, const int* __restrict__ rowptr,
+                           const int* __restrict__ colidx,
+                           const double* __restrict__ vals,
+                           const double* __restrict__ B, int ldb,
+                           const double* __restrict__ X, int ldx, int nrhs,
+                           double* __restrict__ R, int ldr) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int a = rowptr[i], e = rowptr[i + 1];
+  for (int r = 0; r < nrhs; r++) {
+    const double* x = X + (int64_t)r * ldx;
+    double s = 0;
+    for (int k = a; k < e; k++) s += vals[k] * x[colidx[k]];
+    R[i + (int64_t)r * ldr] = B[i + (int64_t)r * ldb] - s;
+  }
+}
+
+// out[r] = max_i |M(i, r)| (non-negative doubles compare like their bit
+// patterns, so a 64-bit integer atomicMax reduces them).
+__global__ void k_colmax(int n, int nrhs, const double* __restrict__ M, int ld,
+                         unsigned long long* out) {
+  for (int r = 0; r < nrhs; r++) {
+    double m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+      m = fmax(m, fabs(M[i + (int64_t)r * ld]));
+    for (int o = 16; o > 0; o >>= 1)
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out + r, __double_as_longlong(m));
+  }
+}
+
+// X += D (column-major, nrhs columns).
+__global__ void k_axpy_cols(int n, int nrhs, const double* __restrict__ D,
+                            int ldd, double* __restrict__ X, int ldx) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n * nrhs) return;
+  int i = (int)(e % n), r = (int)(e / n);
+  X[i + (int64_t)r * ldx] += D[i + (int64_t)r * ldd];
+}
+
+// Column copy with leading dimensions (Y = X).
+__global__ void k_copy_cols(int n, int nrhs, const double* __restrict__ X,
+                            int ldx, double* __restrict__ Y, int ldy) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n * nrhs) return;
+  int i = (int)(e % n), r = (int)(e / n);
+  Y[i + (int64_t)r * ldy] = X[i + (int64_t)r * ldx];
+}
+
+}  // namespace snu

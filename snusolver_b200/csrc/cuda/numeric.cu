@@ -1,0 +1,746 @@
+// CUDA numeric engine: device plan, level-by-level multifrontal
+// factorization (FP64 or FP32), blocked triangular solves over the front
+// tree and FP64 iterative refinement.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "../engine.h"
+#include "kernels.cuh"
+
+namespace snu {
+
+namespace {
+
+#define CK(call)                                                         \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess) {                                             \
+      err_ = std::string(#call) + ": " + cudaGetErrorString(e_);         \
+      return ENG_ECUDA;                                                  \
+    }                                                                    \
+  } while (0)
+
+#define CKL()                                                            \
+  do {                                                                   \
+    cudaError_t e_ = cudaGetLastError();                                 \
+    if (e_ != cudaSuccess) {                                             \
+      err_ = std::string("kernel launch: ") + cudaGetErrorString(e_);    \
+      return ENG_ECUDA;                                                  \
+    }                                                                    \
+  } while (0)
+
+template <typename T>
+struct DevVec {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+struct GemmBatch {
+  GemmProb* probs = nullptr;
+  GemmTile* tiles = nullptr;
+  int ntiles = 0;
+};
+
+struct Step {
+  int k0 = 0;
+  int* active = nullptr;
+  int nactive = 0;
+  PanelTask* panel = nullptr;
+  int npanel = 0;
+  GemmBatch trail;
+};
+
+struct LevelSched {
+  int f0 = 0, f1 = 0;  // fronts [f0, f1)
+  int64_t mem0 = 0, mem1 = 0;
+  int64_t asm0 = 0, asm1 = 0;
+  std::vector<EaTask*> ea;  // per child rank
+  std::vector<int> nea;
+  std::vector<int*> ea_children;  // per child rank (solve)
+  std::vector<int> nea_children;
+  int* list = nullptr;  // fronts of the level
+  int* listq = nullptr; // fronts of the level with q > 0
+  int nlistq = 0;
+  std::vector<Step> steps;
+  GemmBatch f22;
+};
+
+struct SolveSched {
+  // per level: forward step GEMMs, backward F12 GEMM, backward step GEMMs
+  std::vector<std::vector<GemmBatch>> fwd, bwd;
+  std::vector<GemmBatch> bq;
+};
+
+constexpr int GBM = 64, GBN = 64;
+
+class CudaEngine : public Engine {
+ public:
+  explicit CudaEngine(const EngineOptions& o) : opt_(o) {}
+  ~CudaEngine() override { release(); }
+
+  int init() {
+    CK(cudaSetDevice(opt_.device));
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ev0_));
+    CK(cudaEventCreate(&ev1_));
+    return ENG_OK;
+  }
+
+  const std::string& error() const override { return err_; }
+  int64_t device_bytes() const override { return bytes_; }
+  int tiny_pivots() const override { return tiny_; }
+
+  int setup(const Structure& s, const FrontPlan& fp, const int* rowptr,
+            const int* colidx) override {
+    CK(cudaSetDevice(opt_.device));
+    n_ = s.n;
+    nnz_ = s.nnz;
+    fp_ = &fp;
+    nfronts_ = fp.nfronts;
+    nlevels_ = fp.nlevels;
+    arena_ = fp.arena;
+    // fronts
+    frh_.resize(nfronts_);
+    int64_t woff = 0;
+    wtot_ = 0;
+    for (int f = 0; f < nfronts_; f++) {
+      const FrontInfo& fi = fp.fronts[f];
+      FrontDev d;
+      d.p = fi.p;
+      d.q = fi.q;
+      d.ld = fi.ld;
+      d.parent = fi.parent;
+      d.guard = fi.guard;
+      d.pad0 = 0;
+      d.off = fi.offset;
+      d.idx_off = fi.idx_offset;
+      d.rel_off = fi.rel_offset;
+      d.w_off = woff;
+      woff += fi.p + fi.q;
+      frh_[f] = d;
+    }
+    wtot_ = woff;
+    int rc;
+    if ((rc = upload(d_fr_, frh_))) return rc;
+    if ((rc = upload(d_gidx_, fp.gidx))) return rc;
+    if ((rc = upload(d_rel_, fp.rel))) return rc;
+    if ((rc = upload(d_asm_pos_, fp.asm_pos))) return rc;
+    if ((rc = upload(d_asm_val_, fp.asm_val))) return rc;
+    std::vector<int> rp(rowptr, rowptr + n_ + 1), ci(colidx, colidx + nnz_);
+    rowptr_h_ = rp;
+    if ((rc = upload(d_rowptr_, rp))) return rc;
+    if ((rc = upload(d_colidx_, ci))) return rc;
+    if ((rc = alloc(d_vals_, (size_t)std::max(1, nnz_)))) return rc;
+    if ((rc = alloc(d_flags_, 4))) return rc;
+    if ((rc = alloc(d_norms_, 3 * 64))) return rc;
+    if ((rc = build_schedule())) return rc;
+    have64_ = have32_ = false;
+    return ENG_OK;
+  }
+
+  int set_values(const double* vals) override {
+    CK(cudaSetDevice(opt_.device));
+    CK(cudaMemcpyAsync(d_vals_, vals, sizeof(double) * nnz_,
+                       cudaMemcpyHostToDevice, stream_));
+    // ||A||_inf for the backward error
+    anorm_ = 0;
+    for (int i = 0; i < n_; i++) {
+      double s = 0;
+      for (int k = rowptr_h_[i]; k < rowptr_h_[i + 1]; k++) s += std::fabs(vals[k]);
+      anorm_ = std::max(anorm_, s);
+    }
+    have64_ = have32_ = false;
+    CK(cudaStreamSynchronize(stream_));
+    return ENG_OK;
+  }
+
+  int factorize(int precision, double* seconds) override {
+    CK(cudaSetDevice(opt_.device));
+    int rc;
+    if (precision == 0) {
+      if (!d_F64_ && (rc = alloc(d_F64_, (size_t)arena_))) return rc;
+    } else {
+      if (!d_F32_ && (rc = alloc(d_F32_, (size_t)arena_))) return rc;
+    }
+    CK(cudaMemsetAsync(d_flags_, 0, 4 * sizeof(int), stream_));
+    CK(cudaEventRecord(ev0_, stream_));
+    rc = precision == 0 ? run_factor<double>(d_F64_) : run_factor<float>(d_F32_);
+    if (rc) return rc;
+    CK(cudaEventRecord(ev1_, stream_));
+    int flags[4];
+    CK(cudaMemcpyAsync(flags, d_flags_, sizeof flags, cudaMemcpyDeviceToHost,
+                       stream_));
+    CK(cudaStreamSynchronize(stream_));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    if (seconds) *seconds = ms * 1e-3;
+    tiny_ = flags[0];
+    if (precision == 0)
+      have64_ = true;
+    else
+      have32_ = true;
+    if (flags[1]) {
+      err_ = "zero or non-finite pivot in the factorization";
+      return ENG_ESINGULAR;
+    }
+    return ENG_OK;
+  }
+
+  int solve(const double* dB, double* dX, int nrhs, int ldb, void* stream,
+            int precision, SolveReport* rep) override {
+    CK(cudaSetDevice(opt_.device));
+    if (nrhs <= 0 || ldb < n_) {
+      err_ = "bad nrhs or ldb";
+      return ENG_EINVAL;
+    }
+    if ((precision == 0 && !have64_) || (precision == 1 && !have32_)) {
+      err_ = "solve before factorize";
+      return ENG_ESTATE;
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : stream_;
+    int rc;
+    if ((rc = ensure_solve(nrhs))) return rc;
+    bnorm_.clear();
+    CK(cudaEventRecord(ev0_, st));
+    SolveReport r;
+    if (precision == 0) {
+      if ((rc = tree_solve<double>(d_F64_, d_W64_, dB, ldb, dX, ldb, nrhs, st)))
+        return rc;
+      if ((rc = residual_norms(dB, ldb, dX, ldb, nrhs, st, &r.backward_error)))
+        return rc;
+    } else {
+      if ((rc = refine(dB, ldb, dX, ldb, nrhs, st, &r))) return rc;
+    }
+    CK(cudaEventRecord(ev1_, st));
+    CK(cudaEventSynchronize(ev1_));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    r.seconds = ms * 1e-3;
+    if (rep) *rep = r;
+    return ENG_OK;
+  }
+
+  int leaf_factor(const Structure& s, int rank, double* out) override {
+    if (!have64_) {
+      err_ = "no FP64 factorization";
+      return ENG_ESTATE;
+    }
+    const LeafStructure& L = s.leaves[rank];
+    if (L.LU_rowptr.empty() && L.core_n > 0) {
+      err_ = "leaf pattern not computed";
+      return ENG_ESTATE;
+    }
+    std::vector<double> F;
+    int rc;
+    if ((rc = arena_to_host(F))) return rc;
+    const FrontPlan& fp = *fp_;
+    for (int r = 0; r < L.core_n; r++) {
+      for (int k = L.LU_rowptr[r]; k < L.LU_rowptr[r + 1]; k++) {
+        int c = L.LU_colidx[k];
+        int piv = std::min(r, c);
+        if (piv >= L.leaf_size) {
+          out[k] = 0;
+          continue;
+        }
+        int f = fp.pivot_front[rank][piv];
+        int pr = front_position(fp, f, r), pc = front_position(fp, f, c);
+        if (pr < 0 || pc < 0) {
+          out[k] = 0;  // structurally zero in the symmetric front pattern
+          continue;
+        }
+        const FrontInfo& fi = fp.fronts[f];
+        out[k] = F[fi.offset + pr + (int64_t)pc * fi.ld];
+      }
+    }
+    return ENG_OK;
+  }
+
+  int dense_block(const Structure& s, int i, int j, double* out) override {
+    if (!have64_) {
+      err_ = "no FP64 factorization";
+      return ENG_ESTATE;
+    }
+    const FrontPlan& fp = *fp_;
+    int owner = std::max(i, j), anc = std::min(i, j);
+    if (owner >= s.np || fp.sep_front[owner] < 0) {
+      err_ = "not a separator block";
+      return ENG_EINVAL;
+    }
+    int a = owner;
+    while (a > anc) a /= 2;
+    if (a != anc) {
+      err_ = "blocks are not ancestor-related";
+      return ENG_EINVAL;
+    }
+    int f = fp.sep_front[owner];
+    const FrontInfo& fi = fp.fronts[f];
+    auto local = [&](int blk) {
+      int o = 0;
+      for (int b = owner; b >= 1; b /= 2) {
+        if (b == blk) return o;
+        o += s.block_size[b];
+      }
+      return -1;
+    };
+    int ro = local(i), co = local(j);
+    int m = s.block_size[i], nn = s.block_size[j];
+    std::vector<double> F;
+    int rc;
+    if ((rc = arena_to_host(F, fi.offset, (int64_t)fi.ld * (fi.p + fi.q))))
+      return rc;
+    for (int c = 0; c < nn; c++)
+      for (int r = 0; r < m; r++)
+        out[r + (int64_t)c * m] = F[(ro + r) + (int64_t)(co + c) * fi.ld];
+    return ENG_OK;
+  }
+
+ private:
+  // ------------------------------------------------------------ memory
+  template <typename T>
+  int alloc(T*& p, size_t n) {
+    size_t b = std::max<size_t>(n, 1) * sizeof(T);
+    if (opt_.mem_budget > 0 && bytes_ + (int64_t)b > opt_.mem_budget) {
+      err_ = "device memory budget exceeded";
+      return ENG_ENOMEM;
+    }
+    cudaError_t e = cudaMalloc((void**)&p, b);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      err_ = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+      return ENG_ENOMEM;
+    }
+    bytes_ += (int64_t)b;
+    ptrs_.push_back((void*)p);
+    sizes_.push_back((int64_t)b);
+    return ENG_OK;
+  }
+  template <typename T>
+  int upload(T*& p, const std::vector<T>& v) {
+    int rc = alloc(p, v.size());
+    if (rc) return rc;
+    if (!v.empty())
+      CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return ENG_OK;
+  }
+  void release() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (void* p : ptrs_) cudaFree(p);
+    ptrs_.clear();
+    sizes_.clear();
+    bytes_ = 0;
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (stream_) cudaStreamDestroy(stream_);
+    ev0_ = ev1_ = nullptr;
+    stream_ = nullptr;
+  }
+
+  int arena_to_host(std::vector<double>& F, int64_t off = 0, int64_t cnt = -1) {
+    if (cnt < 0) cnt = arena_;
+    F.assign((size_t)cnt + (size_t)off, 0.0);
+    CK(cudaMemcpy(F.data() + off, d_F64_ + off, sizeof(double) * cnt,
+                  cudaMemcpyDeviceToHost));
+    return ENG_OK;
+  }
+
+  // ---------------------------------------------------------- schedule
+  int gemm_batch(const std::vector<GemmProb>& probs, GemmBatch& gb) {
+    std::vector<GemmTile> tiles;
+    for (size_t k = 0; k < probs.size(); k++) {
+      int tm = (probs[k].m + GBM - 1) / GBM, tn = (probs[k].n + GBN - 1) / GBN;
+      for (int b = 0; b < tn; b++)
+        for (int a = 0; a < tm; a++) tiles.push_back({(int)k, a, b});
+    }
+    gb.ntiles = (int)tiles.size();
+    if (tiles.empty()) return ENG_OK;
+    int rc;
+    if ((rc = upload(gb.probs, probs))) return rc;
+    if ((rc = upload(gb.tiles, tiles))) return rc;
+    return ENG_OK;
+  }
+
+  int build_schedule() {
+    const FrontPlan& fp = *fp_;
+    lv_.assign(nlevels_, LevelSched());
+    int mc = fp.max_children;
+    int rc;
+    for (int l = 0; l < nlevels_; l++) {
+      LevelSched& L = lv_[l];
+      L.f0 = fp.level_start[l];
+      L.f1 = fp.level_start[l + 1];
+      if (L.f1 > L.f0) {
+        const FrontInfo& a = fp.fronts[L.f0];
+        const FrontInfo& b = fp.fronts[L.f1 - 1];
+        L.mem0 = a.offset;
+        L.mem1 = b.offset + (int64_t)b.ld * (b.p + b.q);
+      }
+      L.asm0 = fp.asm_level[l];
+      L.asm1 = fp.asm_level[l + 1];
+      std::vector<int> list, listq;
+      for (int f = L.f0; f < L.f1; f++) {
+        list.push_back(f);
+        if (fp.fronts[f].q > 0) listq.push_back(f);
+      }
+      if ((rc = upload(L.list, list))) return rc;
+      L.nlistq = (int)listq.size();
+      if ((rc = upload(L.listq, listq))) return rc;
+      L.ea.assign(mc, nullptr);
+      L.nea.assign(mc, 0);
+      L.ea_children.assign(mc, nullptr);
+      L.nea_children.assign(mc, 0);
+      for (int r = 0; r < mc; r++) {
+        int b0 = fp.ea_ptr[(size_t)l * mc + r], b1 = fp.ea_ptr[(size_t)l * mc + r + 1];
+        std::vector<EaTask> tasks;
+        std::vector<int> kids;
+        for (int k = b0; k < b1; k++) {
+          int c = fp.ea_child[k];
+          kids.push_back(c);
+          for (int j = 0; j < fp.fronts[c].q; j++) tasks.push_back({c, j});
+        }
+        L.nea[r] = (int)tasks.size();
+        L.nea_children[r] = (int)kids.size();
+        if (!tasks.empty() && (rc = upload(L.ea[r], tasks))) return rc;
+        if (!kids.empty() && (rc = upload(L.ea_children[r], kids))) return rc;
+      }
+      int maxp = 0;
+      for (int f = L.f0; f < L.f1; f++) maxp = std::max(maxp, fp.fronts[f].p);
+      int nsteps = (maxp + NB - 1) / NB;
+      L.steps.assign(nsteps, Step());
+      for (int s = 0; s < nsteps; s++) {
+        Step& S = L.steps[s];
+        S.k0 = s * NB;
+        std::vector<int> act;
+        std::vector<PanelTask> pt;
+        std::vector<GemmProb> gp;
+        for (int f = L.f0; f < L.f1; f++) {
+          const FrontInfo& fi = fp.fronts[f];
+          if (fi.p <= S.k0) continue;
+          act.push_back(f);
+          int kb = std::min(NB, fi.p - S.k0), k1 = S.k0 + kb;
+          int dim = fi.p + fi.q, rem = dim - k1;
+          int chunks = (rem + 127) / 128;
+          for (int c = 0; c < chunks; c++) {
+            pt.push_back({f, 0, c});
+            pt.push_back({f, 1, c});
+          }
+          int64_t o = fi.offset, ld = fi.ld;
+          if (dim - k1 > 0 && fi.p - k1 > 0)
+            gp.push_back({dim - k1, fi.p - k1, kb, fi.ld, fi.ld, fi.ld,
+                          o + k1 + S.k0 * ld, o + S.k0 + k1 * ld,
+                          o + k1 + k1 * ld});
+          if (fi.p - k1 > 0 && fi.q > 0)
+            gp.push_back({fi.p - k1, fi.q, kb, fi.ld, fi.ld, fi.ld,
+                          o + k1 + S.k0 * ld, o + S.k0 + fi.p * ld,
+                          o + k1 + fi.p * ld});
+        }
+        S.nactive = (int)act.size();
+        S.npanel = (int)pt.size();
+        if ((rc = upload(S.active, act))) return rc;
+        if (!pt.empty() && (rc = upload(S.panel, pt))) return rc;
+        if ((rc = gemm_batch(gp, S.trail))) return rc;
+      }
+      std::vector<GemmProb> f22;
+      for (int f = L.f0; f < L.f1; f++) {
+        const FrontInfo& fi = fp.fronts[f];
+        if (fi.p == 0 || fi.q == 0) continue;
+        int64_t o = fi.offset, ld = fi.ld;
+        f22.push_back({fi.q, fi.q, fi.p, fi.ld, fi.ld, fi.ld, o + fi.p,
+                       o + fi.p * ld, o + fi.p + fi.p * ld});
+      }
+      if ((rc = gemm_batch(f22, L.f22))) return rc;
+    }
+    return ENG_OK;
+  }
+
+  int ensure_solve(int nrhs) {
+    auto it = solve_sched_.find(nrhs);
+    if (it != solve_sched_.end()) return ENG_OK;
+    const FrontPlan& fp = *fp_;
+    SolveSched S;
+    S.fwd.resize(nlevels_);
+    S.bwd.resize(nlevels_);
+    S.bq.resize(nlevels_);
+    int rc;
+    for (int l = 0; l < nlevels_; l++) {
+      LevelSched& L = lv_[l];
+      S.fwd[l].resize(L.steps.size());
+      S.bwd[l].resize(L.steps.size());
+      for (size_t s = 0; s < L.steps.size(); s++) {
+        int k0 = (int)s * TB;
+        std::vector<GemmProb> fw, bw;
+        for (int f = L.f0; f < L.f1; f++) {
+          const FrontInfo& fi = fp.fronts[f];
+          if (fi.p <= k0) continue;
+          int kb = std::min(TB, fi.p - k0), k1 = k0 + kb, dim = fi.p + fi.q;
+          int64_t w = frh_[f].w_off * nrhs, o = fi.offset, ld = fi.ld;
+          if (dim - k1 > 0)
+            fw.push_back({dim - k1, nrhs, kb, fi.ld, dim, dim, o + k1 + k0 * ld,
+                          w + k0, w + k1});
+          if (k0 > 0)
+            bw.push_back({k0, nrhs, kb, fi.ld, dim, dim, o + k0 * ld, w + k0, w});
+        }
+        if ((rc = gemm_batch(fw, S.fwd[l][s]))) return rc;
+        if ((rc = gemm_batch(bw, S.bwd[l][s]))) return rc;
+      }
+      std::vector<GemmProb> bq;
+      for (int f = L.f0; f < L.f1; f++) {
+        const FrontInfo& fi = fp.fronts[f];
+        if (fi.p == 0 || fi.q == 0) continue;
+        int dim = fi.p + fi.q;
+        int64_t w = frh_[f].w_off * nrhs, o = fi.offset, ld = fi.ld;
+        bq.push_back({fi.p, nrhs, fi.q, fi.ld, dim, dim, o + fi.p * ld,
+                      w + fi.p, w});
+      }
+      if ((rc = gemm_batch(bq, S.bq[l]))) return rc;
+    }
+    solve_sched_[nrhs] = std::move(S);
+    // work buffers sized for the largest nrhs seen
+    if ((size_t)(wtot_ * nrhs) > wcap_) {
+      wcap_ = (size_t)(wtot_ * nrhs);
+      if ((rc = alloc(d_W64_, wcap_))) return rc;
+      if ((rc = alloc(d_W32_, wcap_))) return rc;
+    }
+    if ((size_t)n_ * nrhs > rcap_) {
+      rcap_ = (size_t)n_ * nrhs;
+      if ((rc = alloc(d_R_, rcap_))) return rc;
+      if ((rc = alloc(d_D_, rcap_))) return rc;
+    }
+    return ENG_OK;
+  }
+
+  // --------------------------------------------------------- launches
+  template <typename T>
+  int launch_gemm(const GemmBatch& gb, const T* A, const T* B, T* C, int mode,
+                  cudaStream_t st) {
+    if (gb.ntiles == 0) return ENG_OK;
+    k_gemm<T, GBM, GBN, 16, 4, 4><<<gb.ntiles, 256, 0, st>>>(
+        gb.tiles, gb.probs, A, B, C, mode);
+    CKL();
+    return ENG_OK;
+  }
+
+  template <typename T>
+  int run_factor(T* F) {
+    cudaStream_t st = stream_;
+    int rc;
+    for (int l = 0; l < nlevels_; l++) {
+      LevelSched& L = lv_[l];
+      if (L.mem1 > L.mem0)
+        CK(cudaMemsetAsync(F + L.mem0, 0, sizeof(T) * (L.mem1 - L.mem0), st));
+      int64_t na = L.asm1 - L.asm0;
+      if (na > 0) {
+        int blocks = (int)std::min<int64_t>((na + 255) / 256, 148 * 16);
+        k_assemble<T><<<blocks, 256, 0, st>>>(d_asm_pos_ + L.asm0,
+                                              d_asm_val_ + L.asm0, d_vals_, F,
+                                              na);
+        CKL();
+      }
+      for (size_t r = 0; r < L.ea.size(); r++) {
+        if (!L.nea[r]) continue;
+        k_extend_add<T><<<L.nea[r], 128, 0, st>>>(L.ea[r], d_fr_, d_rel_, F);
+        CKL();
+      }
+      for (Step& S : L.steps) {
+        k_diag_lu<T><<<S.nactive, 256, 0, st>>>(S.active, d_fr_, F, S.k0,
+                                                opt_.pivot_eps, d_flags_);
+        CKL();
+        if (S.npanel) {
+          k_panel_trsm<T><<<S.npanel, 128, 0, st>>>(S.panel, d_fr_, F, S.k0);
+          CKL();
+        }
+        if ((rc = launch_gemm<T>(S.trail, F, F, F, 0, st))) return rc;
+      }
+      if ((rc = launch_gemm<T>(L.f22, F, F, F, 0, st))) return rc;
+    }
+    return ENG_OK;
+  }
+
+  template <typename T>
+  int tree_solve(const T* F, T* W, const double* B, int ldb, double* X,
+                 int ldx, int nrhs, cudaStream_t st) {
+    SolveSched& S = solve_sched_[nrhs];
+    int rc;
+    for (int l = 0; l < nlevels_; l++) {
+      LevelSched& L = lv_[l];
+      int nf = L.f1 - L.f0;
+      if (!nf) continue;
+      k_solve_init<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_, B,
+                                                   ldb, nrhs, W);
+      CKL();
+      for (size_t r = 0; r < L.ea_children.size(); r++) {
+        if (!L.nea_children[r]) continue;
+        k_solve_ea<T><<<L.nea_children[r], 256, 0, st>>>(
+            L.ea_children[r], d_fr_, d_rel_, nrhs, W);
+        CKL();
+      }
+      for (size_t s = 0; s < L.steps.size(); s++) {
+        Step& St = L.steps[s];
+        k_solve_diag<T><<<St.nactive, 256, 0, st>>>(St.active, d_fr_, F,
+                                                    St.k0, nrhs, 0, W);
+        CKL();
+        if ((rc = launch_gemm<T>(S.fwd[l][s], F, W, W, 0, st))) return rc;
+      }
+    }
+    for (int l = nlevels_ - 1; l >= 0; l--) {
+      LevelSched& L = lv_[l];
+      int nf = L.f1 - L.f0;
+      if (!nf) continue;
+      if (L.nlistq) {
+        k_solve_gather_q<T><<<dim3(8, L.nlistq), 256, 0, st>>>(
+            L.listq, d_fr_, d_gidx_, X, ldx, nrhs, W);
+        CKL();
+        if ((rc = launch_gemm<T>(S.bq[l], F, W, W, 0, st))) return rc;
+      }
+      for (int s = (int)L.steps.size() - 1; s >= 0; s--) {
+        Step& St = L.steps[s];
+        k_solve_diag<T><<<St.nactive, 256, 0, st>>>(St.active, d_fr_, F,
+                                                    St.k0, nrhs, 1, W);
+        CKL();
+        if ((rc = launch_gemm<T>(S.bwd[l][s], F, W, W, 0, st))) return rc;
+      }
+      k_solve_scatter_p<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_,
+                                                        W, nrhs, X, ldx);
+      CKL();
+    }
+    return ENG_OK;
+  }
+
+  // Per-column max norms of up to 64 columns of M into host out[].
+  int colmax(const double* M, int ld, int nrhs, cudaStream_t st,
+             std::vector<double>& out) {
+    int nc = std::min(nrhs, 64);
+    CK(cudaMemsetAsync(d_norms_, 0, sizeof(unsigned long long) * 64, st));
+    k_colmax<<<148, 256, 0, st>>>(n_, nc, M, ld, d_norms_);
+    CKL();
+    std::vector<unsigned long long> h(64);
+    CK(cudaMemcpyAsync(h.data(), d_norms_, sizeof(unsigned long long) * 64,
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    out.assign(nc, 0.0);
+    for (int r = 0; r < nc; r++) memcpy(&out[r], &h[r], 8);
+    return ENG_OK;
+  }
+
+  // Backward error max_r ||B - A X||inf / (||A||inf ||X||inf + ||B||inf)
+  // (the first 64 columns); leaves R = B - A X in d_R_.
+  int residual_norms(const double* B, int ldb, const double* X, int ldx,
+                     int nrhs, cudaStream_t st, double* out) {
+    int rc;
+    if (bnorm_.empty()) {
+      if ((rc = colmax(B, ldb, nrhs, st, bnorm_))) return rc;
+    }
+    k_residual<<<(n_ + 255) / 256, 256, 0, st>>>(n_, d_rowptr_, d_colidx_,
+                                                 d_vals_, B, ldb, X, ldx,
+                                                 nrhs, d_R_, n_);
+    CKL();
+    std::vector<double> rn, xn;
+    if ((rc = colmax(d_R_, n_, nrhs, st, rn))) return rc;
+    if ((rc = colmax(X, ldx, nrhs, st, xn))) return rc;
+    double worst = 0;
+    for (size_t r = 0; r < rn.size(); r++) {
+      double den = anorm_ * xn[r] + bnorm_[r];
+      double be = den > 0 ? rn[r] / den : rn[r];
+      if (!(be == be)) be = INFINITY;
+      worst = std::max(worst, be);
+    }
+    *out = worst;
+    return ENG_OK;
+  }
+
+  // FP32 factors + FP64 residual refinement; FP64 factorization on
+  // stagnation or when the iteration budget runs out.
+  int refine(const double* B, int ldb, double* X, int ldx, int nrhs,
+             cudaStream_t st, SolveReport* rep) {
+    int rc;
+    int total = n_ * nrhs;
+    int blocks = (total + 255) / 256;
+    // x0 = solve32(b)
+    if ((rc = tree_solve<float>(d_F32_, d_W32_, B, ldb, X, ldx, nrhs, st)))
+      return rc;
+    double be = 0, prev = INFINITY;
+    int it = 0, stagnant = 0;
+    for (;;) {
+      if ((rc = residual_norms(B, ldb, X, ldx, nrhs, st, &be))) return rc;
+      if (be <= opt_.ir_tol) break;
+      if (it >= opt_.ir_max_iter || stagnant >= 2) {
+        // FP64 fallback: factor in FP64 and solve the correction exactly
+        if (!have64_) {
+          CK(cudaStreamSynchronize(st));
+          double sec;
+          int frc = factorize(0, &sec);
+          if (frc) return frc;
+        }
+        if ((rc = tree_solve<double>(d_F64_, d_W64_, d_R_, n_, d_D_, n_, nrhs,
+                                     st)))
+          return rc;
+        k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
+        CKL();
+        if ((rc = residual_norms(B, ldb, X, ldx, nrhs, st, &be))) return rc;
+        rep->fp64_fallback = 1;
+        break;
+      }
+      if (be > 0.5 * prev) stagnant++;
+      else stagnant = 0;
+      prev = be;
+      // d = solve32(r); x += d
+      if ((rc = tree_solve<float>(d_F32_, d_W32_, d_R_, n_, d_D_, n_, nrhs, st)))
+        return rc;
+      k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
+      CKL();
+      it++;
+    }
+    rep->ir_iters = it;
+    rep->backward_error = be;
+    return ENG_OK;
+  }
+
+  EngineOptions opt_;
+  std::string err_;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  std::vector<void*> ptrs_;
+  std::vector<int64_t> sizes_;
+  int64_t bytes_ = 0;
+  const FrontPlan* fp_ = nullptr;
+  int n_ = 0, nnz_ = 0, nfronts_ = 0, nlevels_ = 0;
+  int64_t arena_ = 0, wtot_ = 0;
+  size_t wcap_ = 0, rcap_ = 0;
+  std::vector<FrontDev> frh_;
+  FrontDev* d_fr_ = nullptr;
+  int *d_gidx_ = nullptr, *d_rel_ = nullptr, *d_asm_val_ = nullptr;
+  int64_t* d_asm_pos_ = nullptr;
+  int *d_rowptr_ = nullptr, *d_colidx_ = nullptr;
+  double* d_vals_ = nullptr;
+  int* d_flags_ = nullptr;
+  unsigned long long* d_norms_ = nullptr;
+  double* d_F64_ = nullptr;
+  float* d_F32_ = nullptr;
+  double *d_W64_ = nullptr, *d_R_ = nullptr, *d_D_ = nullptr;
+  float* d_W32_ = nullptr;
+  bool have64_ = false, have32_ = false;
+  int tiny_ = 0;
+  double anorm_ = 0;
+  std::vector<double> bnorm_;
+  std::vector<int> rowptr_h_;
+  std::vector<LevelSched> lv_;
+  std::map<int, SolveSched> solve_sched_;
+};
+
+}  // namespace
+
+std::unique_ptr<Engine> make_engine(const EngineOptions& opt, std::string& err) {
+  std::unique_ptr<CudaEngine> e(new CudaEngine(opt));
+  if (e->init()) {
+    err = e->error();
+    return nullptr;
+  }
+  return std::unique_ptr<Engine>(e.release());
+}
+
+}  // namespace snu

@@ -1,0 +1,65 @@
+// Interface between the C-ABI (host, C++) and the CUDA numeric engine.
+// Only plain types cross this boundary; CUDA types stay inside numeric.cu.
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <string>
+
+#include "host/fronts.h"
+#include "host/structure.h"
+
+namespace snu {
+
+enum EngineStatus {
+  ENG_OK = 0,
+  ENG_EINVAL = 1,
+  ENG_ENOMEM = 2,
+  ENG_ESINGULAR = 3,
+  ENG_ETIMEOUT = 4,
+  ENG_ECUDA = 5,
+  ENG_ESTATE = 6,
+  ENG_ENOTCONV = 7
+};
+
+struct EngineOptions {
+  int device = 0;
+  double pivot_eps = 1e-15;
+  double ir_tol = 1e-10;
+  int ir_max_iter = 10;
+  int64_t mem_budget = 0;
+};
+
+struct SolveReport {
+  int ir_iters = 0;
+  int fp64_fallback = 0;
+  double backward_error = 0;
+  double seconds = 0;
+};
+
+class Engine {
+ public:
+  virtual ~Engine() {}
+  // Uploads the plan and the CSR pattern (kept for the FP64 residual).
+  virtual int setup(const Structure& s, const FrontPlan& fp, const int* rowptr,
+                    const int* colidx) = 0;
+  // Copies new values (host, original CSR order) to the device.
+  virtual int set_values(const double* vals) = 0;
+  // Numeric factorization in FP64 (precision 0) or FP32 (precision 1).
+  virtual int factorize(int precision, double* seconds) = 0;
+  // X = A^-1 B on device arrays (column-major, leading dimension ldb) on the
+  // given stream (0 = the engine's stream).  precision 1 runs FP32 factors
+  // with FP64 iterative refinement.
+  virtual int solve(const double* dB, double* dX, int nrhs, int ldb,
+                    void* stream, int precision, SolveReport* rep) = 0;
+  // Parity read-back: leaf factor values in the reference's LU pattern,
+  // and a dense separator block LU[{i, j}].
+  virtual int leaf_factor(const Structure& s, int rank, double* out) = 0;
+  virtual int dense_block(const Structure& s, int i, int j, double* out) = 0;
+  virtual int64_t device_bytes() const = 0;
+  virtual int tiny_pivots() const = 0;
+  virtual const std::string& error() const = 0;
+};
+
+std::unique_ptr<Engine> make_engine(const EngineOptions& opt, std::string& err);
+
+}  // namespace snu
