@@ -31,6 +31,7 @@ struct Msg {
 
 struct Peer {
   int fd = -1;
+  bool closed = false;  // the peer exited (normal at finalize)
   std::vector<char> in;  // bytes read but not yet parsed
   std::deque<Msg> inbox;
 };
@@ -94,7 +95,10 @@ void drain(int peer) {
       g_peer[peer].in.insert(g_peer[peer].in.end(), buf, buf + r);
       continue;
     }
-    if (r == 0) die("peer closed its socket");
+    if (r == 0) {
+      g_peer[peer].closed = true;  // only fatal if we still need its data
+      break;
+    }
     if (errno == EAGAIN || errno == EWOULDBLOCK) break;
     if (errno == EINTR) continue;
     die("recv failed");
@@ -108,7 +112,7 @@ bool progress(int out_peer, int timeout_ms) {
   std::vector<pollfd> fds;
   std::vector<int> who;
   for (int r = 0; r < g_size; r++) {
-    if (r == g_rank) continue;
+    if (r == g_rank || g_peer[r].closed) continue;
     pollfd p{g_peer[r].fd, POLLIN, 0};
     if (r == out_peer) p.events |= POLLOUT;
     fds.push_back(p);
@@ -136,6 +140,7 @@ void send_bytes(int dest, int tag, const void* buf, long long bytes) {
     g_peer[dest].inbox.push_back(std::move(m));
     return;
   }
+  if (g_peer[dest].closed) die("send to a rank that exited");
   Header h{tag, 0, bytes};
   std::vector<char> out(sizeof h + bytes);
   memcpy(out.data(), &h, sizeof h);
@@ -167,6 +172,7 @@ void recv_bytes(int src, int tag, void* buf, long long max_bytes) {
       }
     }
     if (src == g_rank) die("self receive without a matching send");
+    if (g_peer[src].closed) die("peer exited before sending a message");
     progress(-1, 1000);
   }
 }

@@ -295,7 +295,8 @@ class CudaEngine : public Engine {
       return rc;
     for (int c = 0; c < nn; c++)
       for (int r = 0; r < m; r++)
-        out[r + (int64_t)c * m] = F[(ro + r) + (int64_t)(co + c) * fi.ld];
+        out[r + (int64_t)c * m] =
+            F[fi.offset + (ro + r) + (int64_t)(co + c) * fi.ld];
     return ENG_OK;
   }
 

@@ -377,6 +377,58 @@ int build_front_plan(const Structure& s, const FrontOptions& opt,
   }
   for (int l = 1; l <= nlev; l++)
     fp.asm_level[l] = std::max(fp.asm_level[l], fp.asm_level[l - 1]);
+  return validate_front_plan(fp, err);
+}
+
+int validate_front_plan(const FrontPlan& fp, std::string& err) {
+  // Every index a kernel derives from the plan must stay inside its front.
+  for (int f = 0; f < fp.nfronts; f++) {
+    const FrontInfo& fi = fp.fronts[f];
+    int64_t dim = (int64_t)fi.p + fi.q;
+    if (fi.p < 0 || fi.q < 0 || fi.ld < dim || fi.offset < 0 ||
+        fi.offset + (int64_t)fi.ld * dim > fp.arena) {
+      err = "front " + std::to_string(f) + " exceeds the arena";
+      return HOST_EINVAL;
+    }
+    if (fi.idx_offset + dim > (int64_t)fp.gidx.size() ||
+        fi.rel_offset + fi.q > (int64_t)fp.rel.size()) {
+      err = "front " + std::to_string(f) + " index lists out of range";
+      return HOST_EINVAL;
+    }
+    for (int64_t t = 0; t < dim; t++) {
+      int g = fp.gidx[fi.idx_offset + t];
+      if (g < 0 || g >= fp.n) {
+        err = "front index outside the matrix";
+        return HOST_EINVAL;
+      }
+    }
+    if (fi.parent < 0) {
+      if (fi.q != 0) {
+        err = "root front with non-pivots";
+        return HOST_EINVAL;
+      }
+      continue;
+    }
+    if (fi.parent <= f || fi.parent >= fp.nfronts ||
+        fp.fronts[fi.parent].level <= fi.level) {
+      err = "parent front not above its child";
+      return HOST_EINVAL;
+    }
+    const FrontInfo& pf = fp.fronts[fi.parent];
+    int pdim = pf.p + pf.q;
+    for (int t = 0; t < fi.q; t++) {
+      int r = fp.rel[fi.rel_offset + t];
+      if (r < 0 || r >= pdim) {
+        err = "extend-add map outside the parent front";
+        return HOST_EINVAL;
+      }
+    }
+  }
+  for (size_t k = 0; k < fp.asm_pos.size(); k++)
+    if (fp.asm_pos[k] < 0 || fp.asm_pos[k] >= fp.arena) {
+      err = "assembly position outside the arena";
+      return HOST_EINVAL;
+    }
   return HOST_OK;
 }
 

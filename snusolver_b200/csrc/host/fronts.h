@@ -73,6 +73,10 @@ struct FrontOptions {
 int build_front_plan(const Structure& s, const FrontOptions& opt,
                      FrontPlan& fp, std::string& err);
 
+// Checks that every offset and map of the plan stays inside its front, the
+// arena and the matrix (run before any upload to the device).
+int validate_front_plan(const FrontPlan& fp, std::string& err);
+
 // Position of core index `idx` inside leaf front f (-1 if absent).
 int front_position(const FrontPlan& fp, int f, int idx);
 

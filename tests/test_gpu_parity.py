@@ -1,0 +1,180 @@
+"""GPU numeric path against the reference numerics.
+
+FP64 path: factors within 1e-10 of the reference's (normwise per array:
+max |F - F_ref| <= 1e-10 * max |F_ref|), solution within 1e-10 relative,
+relative residual <= 1e-12.  FP32+IR path: relative residual <= 1e-10.
+The references are the golden fixtures (made by oracle/_ref, the reference
+built from its sources) and the C restatement oracle/snu_oracle.c run live.
+"""
+import numpy as np
+import pytest
+
+import snusolver_b200 as snu
+from snusolver_b200 import generators
+from util import (dense_block_array, free_blocks, golden, oracle_solve,
+                  rel_resid)
+
+pytestmark = pytest.mark.gpu
+
+FACTOR_TOL = 1e-10
+X_TOL = 1e-10
+
+
+def _close(got, ref, tol, what):
+    scale = max(np.abs(ref).max() if ref.size else 0.0, 1e-300)
+    err = np.abs(got - ref).max() / scale if ref.size else 0.0
+    assert err <= tol, f"{what}: relative error {err:.3e} > {tol}"
+
+
+@pytest.mark.parametrize("np_", [4, 8])
+def test_matrix20_factors_and_solution(gpu, np_):
+    g = golden(f"matrix20_np{np_}.npz")
+    s = snu.Solver(nleaves=np_).construct(g["rowptr"], g["colidx"], g["vals"])
+    s.factorize()
+    x = s.solve(g["b"])
+    _close(x, g["x"], X_TOL, "x")
+    for r in range(np_):
+        _close(s.leaf_factor(r), g[f"r{r}_LU_data"], FACTOR_TOL, f"leaf {r}")
+    bz = g["block_size"]
+    for key in g:
+        if key.startswith("dense_"):
+            i, j = map(int, key.split("_")[1:3])
+            if bz[i] * bz[j] == 0:
+                continue
+            ref = g[key].reshape((bz[i], bz[j]), order="F")
+            _close(s.dense_block(i, j), ref, FACTOR_TOL, f"LU[{i},{j}]")
+
+
+def test_c1_against_golden_and_oracle(gpu):
+    g = golden("c1_2d128_np8.npz")
+    rp, ci, v, B = generators.config("c1_2d128")
+    s = snu.Solver(nleaves=8).construct(rp, ci, v)
+    s.factorize()
+    x = s.solve(B[:, 0])
+    _close(x, g["x"], X_TOL, "x vs reference")
+    assert rel_resid(rp, ci, v, x, B[:, 0]) <= 1e-12
+    order, sizes = s.ordering()
+    xo, lus, blocks, lib = oracle_solve(rp, ci, v, B[:, 0], 8, order, sizes)
+    try:
+        _close(x, xo, X_TOL, "x vs oracle")
+        for r in range(8):
+            lu = s.leaf_factor(r)
+            _close(lu, lus[r], FACTOR_TOL, f"leaf {r}")
+            idx = g[f"r{r}_LU_data_idx"]
+            _close(lu[idx], g[f"r{r}_LU_data_val"], FACTOR_TOL, f"leaf {r} golden")
+        _, bz = s.blocks()
+        for (i, j), p in blocks.items():
+            if bz[i] * bz[j] == 0:
+                continue
+            ref = dense_block_array(lib, p, bz[i], bz[j])
+            _close(s.dense_block(i, j), ref, FACTOR_TOL, f"LU[{i},{j}]")
+    finally:
+        free_blocks(lib, blocks)
+
+
+def _random_unsym(rng, nx, ny, extra):
+    rp, ci, v = generators.laplace2d_perturbed(nx, ny, seed=int(rng.integers(1 << 30)))
+    n = nx * ny
+    rows = list(np.repeat(np.arange(n), np.diff(rp)))
+    cols, vals = list(ci), list(v)
+    seen = set(zip(rows, cols))
+    for _ in range(extra):
+        r = int(rng.integers(n))
+        c = int(min(n - 1, r + int(rng.integers(2, 4))))
+        if (r, c) not in seen:
+            seen.add((r, c))
+            rows.append(r), cols.append(c), vals.append(0.3 * float(rng.normal()))
+    rows, cols, vals = np.array(rows), np.array(cols), np.array(vals)
+    o = np.lexsort((cols, rows))
+    rowptr = np.zeros(n + 1, np.int64)
+    np.add.at(rowptr, rows + 1, 1)
+    return np.cumsum(rowptr).astype(np.int32), cols[o].astype(np.int32), vals[o]
+
+
+@pytest.mark.parametrize("np_,nx,ny,extra", [(2, 20, 17, 30), (4, 33, 30, 80),
+                                             (16, 48, 41, 150), (32, 70, 64, 100)])
+def test_random_unsymmetric_against_oracle(gpu, np_, nx, ny, extra):
+    rng = np.random.default_rng(7 * np_ + nx)
+    rp, ci, v = _random_unsym(rng, nx, ny, extra)
+    b = rng.uniform(-1, 1, len(rp) - 1)
+    s = snu.Solver(nleaves=np_).construct(rp, ci, v)
+    s.factorize()
+    x = s.solve(b)
+    order, sizes = s.ordering()
+    xo, lus, blocks, lib = oracle_solve(rp, ci, v, b, np_, order, sizes)
+    try:
+        _close(x, xo, X_TOL, "x")
+        for r in range(np_):
+            _close(s.leaf_factor(r), lus[r], FACTOR_TOL, f"leaf {r}")
+    finally:
+        free_blocks(lib, blocks)
+    assert rel_resid(rp, ci, v, x, b) <= 1e-12
+
+
+def test_static_pivot_matches_oracle(gpu):
+    # a leaf pivot that is exactly zero gets +eps, as in kernel_sparse.cu:742-749
+    rp, ci, v = generators.laplace2d_perturbed(12, 12, seed=5)
+    n = 144
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    v = v.copy()
+    s0 = snu.Solver(nleaves=2).analyze(rp, ci)
+    order, sizes = s0.ordering()
+    first = int(np.argmin(order))  # original row eliminated first
+    v[(rows == first) & (ci == first)] = 0.0
+    b = np.ones(n)
+    s = snu.Solver(nleaves=2).construct(rp, ci, v)
+    s.factorize()
+    assert s.stats()["tiny_pivots"] >= 1
+    xo, lus, blocks, lib = oracle_solve(rp, ci, v, b, 2, order, sizes)
+    try:
+        for r in range(2):
+            _close(s.leaf_factor(r), lus[r], FACTOR_TOL, f"leaf {r}")
+    finally:
+        free_blocks(lib, blocks)
+
+
+def test_multiple_rhs_and_refactor(gpu):
+    rp, ci, v = generators.laplace2d_perturbed(64, 64, seed=11)
+    n = len(rp) - 1
+    B = generators.rhs(n, 5, seed=12)
+    s = snu.Solver(nleaves=8).construct(rp, ci, v)
+    s.factorize()
+    X = s.solve(B)
+    for r in range(5):
+        assert rel_resid(rp, ci, v, X[:, r], B[:, r]) <= 1e-12
+        _close(X[:, r], s.solve(B[:, r]), 1e-13, "column solve")
+    rng = np.random.default_rng(13)
+    v2 = v * rng.uniform(0.5, 2.0, len(v))
+    s.refactor(v2)
+    X2 = s.solve(B)
+    fresh = snu.Solver(nleaves=8).construct(rp, ci, v2).factorize()
+    _close(X2, fresh.solve(B), 1e-13, "refactor vs fresh")
+    for r in range(5):
+        assert rel_resid(rp, ci, v2, X2[:, r], B[:, r]) <= 1e-12
+
+
+def test_fp32_ir_reaches_tolerance(gpu):
+    rp, ci, v, B = generators.config("c1_2d128")
+    s = snu.Solver(nleaves=8, precision=snu.FP32_IR).construct(rp, ci, v)
+    s.factorize()
+    x = s.solve(B[:, 0])
+    st = s.stats()
+    assert st["backward_error"] <= 1e-10
+    assert rel_resid(rp, ci, v, x, B[:, 0]) <= 1e-10
+    ref = snu.Solver(nleaves=8).construct(rp, ci, v).factorize().solve(B[:, 0])
+    fwd = np.abs(x - ref).max() / np.abs(ref).max()
+    assert fwd <= 1e-8, fwd
+
+
+def test_solve_device_pointers(gpu):
+    import torch
+    rp, ci, v = generators.laplace2d_perturbed(40, 40, seed=2)
+    n = len(rp) - 1
+    B = generators.rhs(n, 3, seed=4)
+    s = snu.Solver(nleaves=4).construct(rp, ci, v).factorize()
+    dB = torch.from_numpy(np.ascontiguousarray(B.T)).cuda()  # column-major
+    dX = torch.empty_like(dB)
+    s.solve_device(dB.data_ptr(), dX.data_ptr(), 3, n)
+    torch.cuda.synchronize()
+    X = dX.cpu().numpy().T
+    _close(X, s.solve(B), 1e-14, "device vs host solve")
