@@ -117,6 +117,25 @@ SNU_API snu_status snu_solve_device(snu_handle* h, const double* dB,
                                     void* stream);
 SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st);
 
+/* ---- execution control and measurement (no reference counterpart) ---- */
+/* All device work of the handle goes to this cudaStream_t (NULL: the
+   handle's own stream).  Takes effect now, or at snu_construct. */
+SNU_API snu_status snu_set_stream(snu_handle* h, void* stream);
+
+typedef struct snu_kernel_stat {
+  const char* name;   /* kernel family */
+  int64_t launches;   /* launches timed */
+  double seconds;     /* sum of their CUDA-event durations */
+  double flops;       /* algorithmic flops of those launches */
+  double bytes;       /* algorithmic bytes of those launches */
+} snu_kernel_stat;
+/* Per-launch CUDA events for the kernel families whose bit is set in mask
+   (bit order as returned by snu_get_profile); 0 turns timing off. */
+SNU_API snu_status snu_set_profiling(snu_handle* h, unsigned mask);
+SNU_API snu_status snu_get_profile(const snu_handle* h, snu_kernel_stat* out,
+                                   int max, int* count);
+SNU_API snu_status snu_reset_profile(snu_handle* h);
+
 /* ---- parity read-back in the reference's layouts (host arrays) ---- */
 /* order[n] (order[old] = new) and sizes[2*nleaves-1]. */
 SNU_API snu_status snu_get_ordering(const snu_handle* h, int* order,

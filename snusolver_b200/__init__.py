@@ -63,6 +63,16 @@ class _Stats(C.Structure):
                 ("reserved", C.c_int * 7)]
 
 
+class _KStat(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("launches", C.c_int64),
+                ("seconds", C.c_double), ("flops", C.c_double),
+                ("bytes", C.c_double)]
+
+
+KERNEL_FAMILIES = ("assemble", "extend_add", "diag_lu", "panel_trsm",
+                   "gemm_trail", "gemm_schur", "solve_diag", "solve_gemm",
+                   "solve_misc", "residual")
+
 _lib = None
 _I = C.POINTER(C.c_int)
 _D = C.POINTER(C.c_double)
@@ -90,6 +100,11 @@ _EXPORTS = {
     "snu_read_mtx": (C.c_int, [C.c_char_p, C.c_int, _I, _I, C.POINTER(_I),
                                C.POINTER(_I), C.POINTER(_D)]),
     "snu_free": (None, [C.c_void_p]),
+    "snu_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "snu_set_profiling": (C.c_int, [C.c_void_p, C.c_uint]),
+    "snu_get_profile": (C.c_int, [C.c_void_p, C.POINTER(_KStat), C.c_int,
+                                  C.POINTER(C.c_int)]),
+    "snu_reset_profile": (C.c_int, [C.c_void_p]),
 }
 
 
@@ -191,12 +206,18 @@ class Solver:
         self._check(self._lib.snu_refactor(self._h, _dptr(v)))
         return self
 
-    def solve(self, B, allow_notconv=False):
-        """X = A^-1 B for a vector or a column-major (n, nrhs) array."""
+    def solve(self, B, allow_notconv=False, out=None):
+        """X = A^-1 B for a vector or a column-major (n, nrhs) array;
+        ``out`` (same shape, Fortran order, float64) receives X if given."""
         B = np.asarray(B, dtype=np.float64)
         vec = B.ndim == 1
         Bm = np.asfortranarray(B.reshape(self.n, -1))
-        X = np.empty_like(Bm, order="F")
+        if out is not None:
+            X = out.reshape(self.n, -1)
+            if X.dtype != np.float64 or not X.flags.f_contiguous:
+                raise SnuError(1, "out must be a Fortran-ordered float64 array")
+        else:
+            X = np.empty_like(Bm, order="F")
         self._check(self._lib.snu_solve(self._h, _dptr(Bm), _dptr(X),
                                         Bm.shape[1], self.n),
                     allow=(7,) if allow_notconv else ())
@@ -207,6 +228,33 @@ class Solver:
         return self._check(self._lib.snu_solve_device(
             self._h, C.c_void_p(dB), C.c_void_p(dX), nrhs, ldb,
             C.c_void_p(stream or None)), allow=(7,) if allow_notconv else ())
+
+    def set_stream(self, stream):
+        """CUDA stream (integer handle, 0 = the handle's own) for all work."""
+        self._check(self._lib.snu_set_stream(self._h, C.c_void_p(stream or None)))
+        return self
+
+    def set_profiling(self, families=()):
+        """Per-launch CUDA-event timing for the named kernel families."""
+        mask = 0
+        for f in families:
+            mask |= 1 << KERNEL_FAMILIES.index(f)
+        self._check(self._lib.snu_set_profiling(self._h, mask))
+        return self
+
+    def profile(self):
+        arr = (_KStat * 16)()
+        cnt = C.c_int()
+        self._check(self._lib.snu_get_profile(self._h, arr, 16, C.byref(cnt)))
+        return {arr[i].name.decode(): dict(launches=arr[i].launches,
+                                           seconds=arr[i].seconds,
+                                           flops=arr[i].flops,
+                                           bytes=arr[i].bytes)
+                for i in range(cnt.value)}
+
+    def reset_profile(self):
+        self._check(self._lib.snu_reset_profile(self._h))
+        return self
 
     def stats(self):
         s = _Stats()

@@ -1,6 +1,7 @@
 // C-ABI of snusolver_b200 (declared in include/snusolver_b200.h).
 #include "../../include/snusolver_b200.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -26,6 +27,8 @@ struct snu_handle {
   snu_stats stats;
   double* dB = nullptr;  // staging for host solves
   size_t dcap = 0;
+  void* stream = nullptr;    // user stream (applied at construct)
+  unsigned prof_mask = 0;    // profiling families (applied at construct)
 };
 
 namespace {
@@ -184,7 +187,10 @@ SNU_API snu_status snu_construct(snu_handle* h, int n, int nnz,
   eo.mem_budget = h->opts.mem_budget;
   h->eng = snu::make_engine(eo, err);
   if (!h->eng) return fail(h, SNU_ECUDA, "CUDA engine unavailable: " + err);
-  int rc = h->eng->setup(h->S, h->FP, rowptr, colidx);
+  int rc = h->eng->set_stream(h->stream);
+  if (rc) return from_engine(h, rc);
+  h->eng->set_profiling(h->prof_mask);
+  rc = h->eng->setup(h->S, h->FP, rowptr, colidx);
   if (rc) return from_engine(h, rc);
   rc = h->eng->set_values(vals);
   if (rc) return from_engine(h, rc);
@@ -284,6 +290,43 @@ SNU_API snu_status snu_solve(snu_handle* h, const double* B, double* X,
 SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st) {
   if (!h || !st) return fail(nullptr, SNU_EINVAL, "null argument");
   *st = h->stats;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_set_stream(snu_handle* h, void* stream) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  h->stream = stream;
+  if (h->eng) return from_engine(h, h->eng->set_stream(stream));
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_set_profiling(snu_handle* h, unsigned mask) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  h->prof_mask = mask;
+  if (h->eng) h->eng->set_profiling(mask);
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_get_profile(const snu_handle* h, snu_kernel_stat* out,
+                                   int max, int* count) {
+  if (!h || (!out && max > 0)) return fail(nullptr, SNU_EINVAL, "null argument");
+  snu::KernelStat ks[snu::KF_COUNT];
+  if (h->eng) h->eng->profile(ks);
+  int m = std::min<int>(max, snu::KF_COUNT);
+  for (int f = 0; f < m; f++) {
+    out[f].name = snu::kernel_family_name(f);
+    out[f].launches = ks[f].launches;
+    out[f].seconds = ks[f].seconds;
+    out[f].flops = ks[f].flops;
+    out[f].bytes = ks[f].bytes;
+  }
+  if (count) *count = snu::KF_COUNT;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_reset_profile(snu_handle* h) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->eng) h->eng->reset_profile();
   return SNU_OK;
 }
 

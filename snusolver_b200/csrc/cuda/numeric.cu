@@ -44,6 +44,8 @@ struct GemmBatch {
   GemmProb* probs = nullptr;
   GemmTile* tiles = nullptr;
   int ntiles = 0;
+  double flops = 0;  // sum of 2 m n k
+  double elems = 0;  // algorithmic elements moved: A + B read, C read+write
 };
 
 struct Step {
@@ -53,6 +55,8 @@ struct Step {
   PanelTask* panel = nullptr;
   int npanel = 0;
   GemmBatch trail;
+  double diag_flops = 0, diag_elems = 0;    // diagonal-block LU
+  double panel_flops = 0, panel_elems = 0;  // L / U panel solves
 };
 
 struct LevelSched {
@@ -68,6 +72,8 @@ struct LevelSched {
   int nlistq = 0;
   std::vector<Step> steps;
   GemmBatch f22;
+  std::vector<double> ea_elems;  // per child rank: update entries added
+  double solve_elems = 0;        // sum of front dims (per right-hand side)
 };
 
 struct SolveSched {
@@ -85,13 +91,30 @@ class CudaEngine : public Engine {
 
   int init() {
     CK(cudaSetDevice(opt_.device));
-    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+    stream_ = own_stream_;
     CK(cudaEventCreate(&ev0_));
     CK(cudaEventCreate(&ev1_));
+    CK(cudaEventCreate(&sev0_));
+    CK(cudaEventCreate(&sev1_));
     return ENG_OK;
   }
 
   const std::string& error() const override { return err_; }
+
+  int set_stream(void* st) override {
+    CK(cudaSetDevice(opt_.device));
+    CK(cudaStreamSynchronize(stream_));
+    stream_ = st ? (cudaStream_t)st : own_stream_;
+    return ENG_OK;
+  }
+  void set_profiling(unsigned mask) override { prof_mask_ = mask; }
+  void profile(KernelStat* out) const override {
+    for (int f = 0; f < KF_COUNT; f++) out[f] = kstat_[f];
+  }
+  void reset_profile() override {
+    for (int f = 0; f < KF_COUNT; f++) kstat_[f] = KernelStat();
+  }
   int64_t device_bytes() const override { return bytes_; }
   int tiny_pivots() const override { return tiny_; }
 
@@ -176,6 +199,7 @@ class CudaEngine : public Engine {
     CK(cudaMemcpyAsync(flags, d_flags_, sizeof flags, cudaMemcpyDeviceToHost,
                        stream_));
     CK(cudaStreamSynchronize(stream_));
+    prof_collect();
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
     if (seconds) *seconds = ms * 1e-3;
@@ -206,7 +230,7 @@ class CudaEngine : public Engine {
     int rc;
     if ((rc = ensure_solve(nrhs))) return rc;
     bnorm_.clear();
-    CK(cudaEventRecord(ev0_, st));
+    CK(cudaEventRecord(sev0_, st));
     SolveReport r;
     if (precision == 0) {
       if ((rc = tree_solve<double>(d_F64_, d_W64_, dB, ldb, dX, ldb, nrhs, st)))
@@ -216,10 +240,11 @@ class CudaEngine : public Engine {
     } else {
       if ((rc = refine(dB, ldb, dX, ldb, nrhs, st, &r))) return rc;
     }
-    CK(cudaEventRecord(ev1_, st));
-    CK(cudaEventSynchronize(ev1_));
+    CK(cudaEventRecord(sev1_, st));
+    CK(cudaEventSynchronize(sev1_));
+    prof_collect();
     float ms = 0;
-    CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    CK(cudaEventElapsedTime(&ms, sev0_, sev1_));
     r.seconds = ms * 1e-3;
     if (rep) *rep = r;
     return ENG_OK;
@@ -301,6 +326,44 @@ class CudaEngine : public Engine {
   }
 
  private:
+  // --------------------------------------------------------- profiling
+  int prof_begin(int fam, cudaStream_t st) {
+    if (!((prof_mask_ >> fam) & 1u)) return -1;
+    if (pev_used_ + 2 > (int)pev_.size()) {
+      for (int k = 0; k < 64; k++) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return -1;
+        pev_.push_back(e);
+      }
+    }
+    int i = pev_used_;
+    pev_used_ += 2;
+    cudaEventRecord(pev_[i], st);
+    return i;
+  }
+  void prof_end(int i, int fam, cudaStream_t st, double flops, double bytes) {
+    if (i < 0) return;
+    cudaEventRecord(pev_[i + 1], st);
+    pend_.push_back({fam, i, flops, bytes});
+  }
+  // call after the stream that carried the records has been synchronized
+  void prof_collect() {
+    for (const ProfRec& r : pend_) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, pev_[r.ev], pev_[r.ev + 1]) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      KernelStat& k = kstat_[r.fam];
+      k.launches++;
+      k.seconds += ms * 1e-3;
+      k.flops += r.flops;
+      k.bytes += r.bytes;
+    }
+    pend_.clear();
+    pev_used_ = 0;
+  }
+
   // ------------------------------------------------------------ memory
   template <typename T>
   int alloc(T*& p, size_t n) {
@@ -337,9 +400,14 @@ class CudaEngine : public Engine {
     bytes_ = 0;
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
-    if (stream_) cudaStreamDestroy(stream_);
+    if (sev0_) cudaEventDestroy(sev0_);
+    if (sev1_) cudaEventDestroy(sev1_);
+    sev0_ = sev1_ = nullptr;
+    for (cudaEvent_t e : pev_) cudaEventDestroy(e);
+    pev_.clear();
+    if (own_stream_) cudaStreamDestroy(own_stream_);
     ev0_ = ev1_ = nullptr;
-    stream_ = nullptr;
+    stream_ = own_stream_ = nullptr;
   }
 
   int arena_to_host(std::vector<double>& F, int64_t off = 0, int64_t cnt = -1) {
@@ -359,6 +427,10 @@ class CudaEngine : public Engine {
         for (int a = 0; a < tm; a++) tiles.push_back({(int)k, a, b});
     }
     gb.ntiles = (int)tiles.size();
+    for (const GemmProb& g : probs) {
+      gb.flops += 2.0 * g.m * (double)g.n * g.k;
+      gb.elems += (double)g.m * g.k + (double)g.k * g.n + 2.0 * g.m * g.n;
+    }
     if (tiles.empty()) return ENG_OK;
     int rc;
     if ((rc = upload(gb.probs, probs))) return rc;
@@ -395,6 +467,9 @@ class CudaEngine : public Engine {
       L.nea.assign(mc, 0);
       L.ea_children.assign(mc, nullptr);
       L.nea_children.assign(mc, 0);
+      L.ea_elems.assign(mc, 0.0);
+      for (int f = L.f0; f < L.f1; f++)
+        L.solve_elems += fp.fronts[f].p + fp.fronts[f].q;
       for (int r = 0; r < mc; r++) {
         int b0 = fp.ea_ptr[(size_t)l * mc + r], b1 = fp.ea_ptr[(size_t)l * mc + r + 1];
         std::vector<EaTask> tasks;
@@ -403,6 +478,7 @@ class CudaEngine : public Engine {
           int c = fp.ea_child[k];
           kids.push_back(c);
           for (int j = 0; j < fp.fronts[c].q; j++) tasks.push_back({c, j});
+          L.ea_elems[r] += (double)fp.fronts[c].q * fp.fronts[c].q;
         }
         L.nea[r] = (int)tasks.size();
         L.nea_children[r] = (int)kids.size();
@@ -430,6 +506,10 @@ class CudaEngine : public Engine {
             pt.push_back({f, 0, c});
             pt.push_back({f, 1, c});
           }
+          S.diag_flops += 2.0 / 3.0 * kb * (double)kb * kb;
+          S.diag_elems += 2.0 * kb * kb;
+          S.panel_flops += 2.0 * rem * (double)kb * kb;
+          S.panel_elems += 4.0 * rem * (double)kb;
           int64_t o = fi.offset, ld = fi.ld;
           if (dim - k1 > 0 && fi.p - k1 > 0)
             gp.push_back({dim - k1, fi.p - k1, kb, fi.ld, fi.ld, fi.ld,
@@ -518,23 +598,27 @@ class CudaEngine : public Engine {
   // --------------------------------------------------------- launches
   template <typename T>
   int launch_gemm(const GemmBatch& gb, const T* A, const T* B, T* C, int mode,
-                  cudaStream_t st) {
+                  cudaStream_t st, int fam) {
     if (gb.ntiles == 0) return ENG_OK;
+    int pi = prof_begin(fam, st);
     k_gemm<T, GBM, GBN, 16, 4, 4><<<gb.ntiles, 256, 0, st>>>(
         gb.tiles, gb.probs, A, B, C, mode);
     CKL();
+    prof_end(pi, fam, st, gb.flops, gb.elems * sizeof(T));
     return ENG_OK;
   }
 
   template <typename T>
   int run_factor(T* F) {
     cudaStream_t st = stream_;
+    const double es = sizeof(T);
     int rc;
     for (int l = 0; l < nlevels_; l++) {
       LevelSched& L = lv_[l];
+      int64_t na = L.asm1 - L.asm0;
+      int pi = prof_begin(KF_ASSEMBLE, st);
       if (L.mem1 > L.mem0)
         CK(cudaMemsetAsync(F + L.mem0, 0, sizeof(T) * (L.mem1 - L.mem0), st));
-      int64_t na = L.asm1 - L.asm0;
       if (na > 0) {
         int blocks = (int)std::min<int64_t>((na + 255) / 256, 148 * 16);
         k_assemble<T><<<blocks, 256, 0, st>>>(d_asm_pos_ + L.asm0,
@@ -542,22 +626,32 @@ class CudaEngine : public Engine {
                                               na);
         CKL();
       }
+      prof_end(pi, KF_ASSEMBLE, st, 0,
+               es * (L.mem1 - L.mem0) + (20.0 + es) * na);
       for (size_t r = 0; r < L.ea.size(); r++) {
         if (!L.nea[r]) continue;
+        pi = prof_begin(KF_EXTEND_ADD, st);
         k_extend_add<T><<<L.nea[r], 128, 0, st>>>(L.ea[r], d_fr_, d_rel_, F);
         CKL();
+        prof_end(pi, KF_EXTEND_ADD, st, L.ea_elems[r],
+                 L.ea_elems[r] * (3 * es + 4));
       }
       for (Step& S : L.steps) {
+        pi = prof_begin(KF_DIAG_LU, st);
         k_diag_lu<T><<<S.nactive, 256, 0, st>>>(S.active, d_fr_, F, S.k0,
                                                 opt_.pivot_eps, d_flags_);
         CKL();
+        prof_end(pi, KF_DIAG_LU, st, S.diag_flops, S.diag_elems * es);
         if (S.npanel) {
+          pi = prof_begin(KF_PANEL_TRSM, st);
           k_panel_trsm<T><<<S.npanel, 128, 0, st>>>(S.panel, d_fr_, F, S.k0);
           CKL();
+          prof_end(pi, KF_PANEL_TRSM, st, S.panel_flops, S.panel_elems * es);
         }
-        if ((rc = launch_gemm<T>(S.trail, F, F, F, 0, st))) return rc;
+        if ((rc = launch_gemm<T>(S.trail, F, F, F, 0, st, KF_GEMM_TRAIL)))
+          return rc;
       }
-      if ((rc = launch_gemm<T>(L.f22, F, F, F, 0, st))) return rc;
+      if ((rc = launch_gemm<T>(L.f22, F, F, F, 0, st, KF_GEMM_SCHUR))) return rc;
     }
     return ENG_OK;
   }
@@ -566,11 +660,13 @@ class CudaEngine : public Engine {
   int tree_solve(const T* F, T* W, const double* B, int ldb, double* X,
                  int ldx, int nrhs, cudaStream_t st) {
     SolveSched& S = solve_sched_[nrhs];
-    int rc;
+    const double es = sizeof(T);
+    int rc, pi;
     for (int l = 0; l < nlevels_; l++) {
       LevelSched& L = lv_[l];
       int nf = L.f1 - L.f0;
       if (!nf) continue;
+      pi = prof_begin(KF_SOLVE_MISC, st);
       k_solve_init<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_, B,
                                                    ldb, nrhs, W);
       CKL();
@@ -580,12 +676,16 @@ class CudaEngine : public Engine {
             L.ea_children[r], d_fr_, d_rel_, nrhs, W);
         CKL();
       }
+      prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
       for (size_t s = 0; s < L.steps.size(); s++) {
         Step& St = L.steps[s];
+        pi = prof_begin(KF_SOLVE_DIAG, st);
         k_solve_diag<T><<<St.nactive, 256, 0, st>>>(St.active, d_fr_, F,
                                                     St.k0, nrhs, 0, W);
         CKL();
-        if ((rc = launch_gemm<T>(S.fwd[l][s], F, W, W, 0, st))) return rc;
+        prof_end(pi, KF_SOLVE_DIAG, st, St.diag_flops * 0, St.diag_elems * es);
+        if ((rc = launch_gemm<T>(S.fwd[l][s], F, W, W, 0, st, KF_SOLVE_GEMM)))
+          return rc;
       }
     }
     for (int l = nlevels_ - 1; l >= 0; l--) {
@@ -593,21 +693,29 @@ class CudaEngine : public Engine {
       int nf = L.f1 - L.f0;
       if (!nf) continue;
       if (L.nlistq) {
+        pi = prof_begin(KF_SOLVE_MISC, st);
         k_solve_gather_q<T><<<dim3(8, L.nlistq), 256, 0, st>>>(
             L.listq, d_fr_, d_gidx_, X, ldx, nrhs, W);
         CKL();
-        if ((rc = launch_gemm<T>(S.bq[l], F, W, W, 0, st))) return rc;
+        prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
+        if ((rc = launch_gemm<T>(S.bq[l], F, W, W, 0, st, KF_SOLVE_GEMM)))
+          return rc;
       }
       for (int s = (int)L.steps.size() - 1; s >= 0; s--) {
         Step& St = L.steps[s];
+        pi = prof_begin(KF_SOLVE_DIAG, st);
         k_solve_diag<T><<<St.nactive, 256, 0, st>>>(St.active, d_fr_, F,
                                                     St.k0, nrhs, 1, W);
         CKL();
-        if ((rc = launch_gemm<T>(S.bwd[l][s], F, W, W, 0, st))) return rc;
+        prof_end(pi, KF_SOLVE_DIAG, st, 0, St.diag_elems * es);
+        if ((rc = launch_gemm<T>(S.bwd[l][s], F, W, W, 0, st, KF_SOLVE_GEMM)))
+          return rc;
       }
+      pi = prof_begin(KF_SOLVE_MISC, st);
       k_solve_scatter_p<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_,
                                                         W, nrhs, X, ldx);
       CKL();
+      prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
     }
     return ENG_OK;
   }
@@ -636,10 +744,13 @@ class CudaEngine : public Engine {
     if (bnorm_.empty()) {
       if ((rc = colmax(B, ldb, nrhs, st, bnorm_))) return rc;
     }
+    int pi = prof_begin(KF_RESIDUAL, st);
     k_residual<<<(n_ + 255) / 256, 256, 0, st>>>(n_, d_rowptr_, d_colidx_,
                                                  d_vals_, B, ldb, X, ldx,
                                                  nrhs, d_R_, n_);
     CKL();
+    prof_end(pi, KF_RESIDUAL, st, 2.0 * nnz_ * nrhs,
+             12.0 * nnz_ + 4.0 * (n_ + 1) + 24.0 * n_ * nrhs);
     std::vector<double> rn, xn;
     if ((rc = colmax(d_R_, n_, nrhs, st, rn))) return rc;
     if ((rc = colmax(X, ldx, nrhs, st, xn))) return rc;
@@ -680,8 +791,10 @@ class CudaEngine : public Engine {
         if ((rc = tree_solve<double>(d_F64_, d_W64_, d_R_, n_, d_D_, n_, nrhs,
                                      st)))
           return rc;
+        int pi = prof_begin(KF_RESIDUAL, st);
         k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
         CKL();
+        prof_end(pi, KF_RESIDUAL, st, (double)total, 24.0 * total);
         if ((rc = residual_norms(B, ldb, X, ldx, nrhs, st, &be))) return rc;
         rep->fp64_fallback = 1;
         break;
@@ -692,8 +805,10 @@ class CudaEngine : public Engine {
       // d = solve32(r); x += d
       if ((rc = tree_solve<float>(d_F32_, d_W32_, d_R_, n_, d_D_, n_, nrhs, st)))
         return rc;
+      int pi = prof_begin(KF_RESIDUAL, st);
       k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
       CKL();
+      prof_end(pi, KF_RESIDUAL, st, (double)total, 24.0 * total);
       it++;
     }
     rep->ir_iters = it;
@@ -703,8 +818,18 @@ class CudaEngine : public Engine {
 
   EngineOptions opt_;
   std::string err_;
-  cudaStream_t stream_ = nullptr;
-  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
+  // per-launch profiling
+  struct ProfRec {
+    int fam, ev;
+    double flops, bytes;
+  };
+  unsigned prof_mask_ = 0;
+  std::vector<cudaEvent_t> pev_;
+  int pev_used_ = 0;
+  std::vector<ProfRec> pend_;
+  KernelStat kstat_[KF_COUNT];
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, sev0_ = nullptr, sev1_ = nullptr;
   std::vector<void*> ptrs_;
   std::vector<int64_t> sizes_;
   int64_t bytes_ = 0;
@@ -734,6 +859,13 @@ class CudaEngine : public Engine {
 };
 
 }  // namespace
+
+const char* kernel_family_name(int f) {
+  static const char* names[KF_COUNT] = {
+      "assemble", "extend_add", "diag_lu", "panel_trsm", "gemm_trail",
+      "gemm_schur", "solve_diag", "solve_gemm", "solve_misc", "residual"};
+  return (f >= 0 && f < KF_COUNT) ? names[f] : "?";
+}
 
 std::unique_ptr<Engine> make_engine(const EngineOptions& opt, std::string& err) {
   std::unique_ptr<CudaEngine> e(new CudaEngine(opt));

@@ -36,9 +36,37 @@ struct SolveReport {
   double seconds = 0;
 };
 
+// Kernel families timed by the optional per-launch CUDA-event profiling.
+enum KernelFamily {
+  KF_ASSEMBLE = 0,   // original values into the fronts (+ front zeroing)
+  KF_EXTEND_ADD,     // children's update matrices into the parents
+  KF_DIAG_LU,        // diagonal-block LU of a panel step
+  KF_PANEL_TRSM,     // L / U panel solves of a panel step
+  KF_GEMM_TRAIL,     // rank-NB trailing updates inside the pivot block
+  KF_GEMM_SCHUR,     // F22 -= F21 F12 Schur-complement update of a front
+  KF_SOLVE_DIAG,     // triangular tile solves of the forward / back sweeps
+  KF_SOLVE_GEMM,     // GEMM updates of the sweeps
+  KF_SOLVE_MISC,     // gathers, scatters and extend-adds of the sweeps
+  KF_RESIDUAL,       // FP64 residual, norms and solution updates
+  KF_COUNT
+};
+const char* kernel_family_name(int f);
+
+struct KernelStat {
+  int64_t launches = 0;
+  double seconds = 0, flops = 0, bytes = 0;
+};
+
 class Engine {
  public:
   virtual ~Engine() {}
+  // Profiling: families whose bit is set in mask get CUDA events around each
+  // launch; totals accumulate until reset.
+  virtual void set_profiling(unsigned mask) = 0;
+  virtual void profile(KernelStat* out) const = 0;  // KF_COUNT entries
+  virtual void reset_profile() = 0;
+  // Stream for all work of the handle (nullptr: the engine's own stream).
+  virtual int set_stream(void* stream) = 0;
   // Uploads the plan and the CSR pattern (kept for the FP64 residual).
   virtual int setup(const Structure& s, const FrontPlan& fp, const int* rowptr,
                     const int* colidx) = 0;
