@@ -20,6 +20,8 @@ struct FrontDev {
   int64_t idx_off;  // into gidx
   int64_t rel_off;  // into rel
   int64_t w_off;    // solve work offset (elements per right-hand side)
+  int64_t y_off;    // pivot-part solve offset (elements per right-hand side)
+  int64_t inv_off;  // diagonal-tile inverses: 2 NB x NB tiles per panel step
 };
 
 struct GemmProb {
@@ -38,6 +40,10 @@ struct EaTask {
 
 struct PanelTask {
   int front, kind, chunk;  // kind 0: rows of the L panel; 1: columns of U
+};
+
+struct SweepTask {
+  int front, chunk, kchunk;
 };
 
 // ---------------------------------------------------------------- assembly
@@ -71,94 +77,6 @@ __global__ void k_extend_add(const EaTask* __restrict__ tasks,
   const T* src = F + c.off + (int64_t)(c.p + t.j) * c.ld + c.p;
   T* dst = F + pf.off + (int64_t)r[t.j] * pf.ld;
   for (int i = threadIdx.x; i < c.q; i += blockDim.x) dst[r[i]] += src[i];
-}
-
-// ------------------------------------------------- blocked partial LU steps
-
-// LU without pivoting of the kb x kb diagonal block at (k0, k0) of every
-// active front, in shared memory.  Leaf fronts apply the reference's static
-// pivot (|p| < eps -> +-eps, kernel_sparse.cu:742-749); separator fronts do
-// not guard, like cusolverDnDgetrf without ipiv (kernel_cuda.cu:67).
-// flags[0] counts replaced pivots, flags[1] is set on a zero or non-finite
-// pivot.
-template <typename T>
-__global__ void __launch_bounds__(256)
-    k_diag_lu(const int* __restrict__ active, const FrontDev* __restrict__ fr,
-              T* __restrict__ F, int k0, double eps, int* flags) {
-  __shared__ T D[NB * NB];
-  const FrontDev f = fr[active[blockIdx.x]];
-  const int kb = min(NB, f.p - k0);
-  T* base = F + f.off + k0 + (int64_t)k0 * f.ld;
-  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-    int i = e % kb, j = e / kb;
-    D[i + j * NB] = base[i + (int64_t)j * f.ld];
-  }
-  __syncthreads();
-  const T teps = (T)eps;
-  for (int kk = 0; kk < kb; kk++) {
-    if (threadIdx.x == 0) {
-      T piv = D[kk + kk * NB];
-      if (f.guard && piv < teps && piv > -teps) {
-        piv = piv < (T)0 ? -teps : teps;
-        D[kk + kk * NB] = piv;
-        atomicAdd(flags, 1);
-      }
-      if (!(piv != (T)0) || !isfinite((double)piv)) flags[1] = 1;
-    }
-    __syncthreads();
-    const T piv = D[kk + kk * NB];
-    for (int i = kk + 1 + threadIdx.x; i < kb; i += blockDim.x)
-      D[i + kk * NB] /= piv;
-    __syncthreads();
-    const int m = kb - kk - 1;
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      int i = kk + 1 + e % m, j = kk + 1 + e / m;
-      D[i + j * NB] -= D[i + kk * NB] * D[kk + j * NB];
-    }
-    __syncthreads();
-  }
-  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-    int i = e % kb, j = e / kb;
-    base[i + (int64_t)j * f.ld] = D[i + j * NB];
-  }
-}
-
-// Panel solves after the diagonal block: rows below it become
-// L = A U_D^-1 (trsm right/upper/non-unit, kernel_cuda.cu:98-121) and
-// columns right of it become U = L_D^-1 A (trsm left/lower/unit,
-// kernel_cuda.cu:74-97).  One thread per row or column.
-template <typename T>
-__global__ void __launch_bounds__(128)
-    k_panel_trsm(const PanelTask* __restrict__ tasks,
-                 const FrontDev* __restrict__ fr, T* __restrict__ F, int k0) {
-  __shared__ T D[NB * NB];
-  const PanelTask t = tasks[blockIdx.x];
-  const FrontDev f = fr[t.front];
-  const int kb = min(NB, f.p - k0);
-  const int dim = f.p + f.q;
-  const T* dsrc = F + f.off + k0 + (int64_t)k0 * f.ld;
-  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-    int i = e % kb, j = e / kb;
-    D[i + j * NB] = dsrc[i + (int64_t)j * f.ld];
-  }
-  __syncthreads();
-  const int idx = k0 + kb + t.chunk * blockDim.x + threadIdx.x;
-  if (idx >= dim) return;
-  if (t.kind == 0) {
-    T* row = F + f.off + idx + (int64_t)k0 * f.ld;
-    for (int j = 0; j < kb; j++) {
-      T s = row[(int64_t)j * f.ld];
-      for (int i = 0; i < j; i++) s -= row[(int64_t)i * f.ld] * D[i + j * NB];
-      row[(int64_t)j * f.ld] = s / D[j + j * NB];
-    }
-  } else {
-    T* col = F + f.off + k0 + (int64_t)idx * f.ld;
-    for (int i = 1; i < kb; i++) {
-      T s = col[i];
-      for (int j = 0; j < i; j++) s -= D[i + j * NB] * col[j];
-      col[i] = s;
-    }
-  }
 }
 
 // ------------------------------------------------------------ batched GEMM
@@ -260,87 +178,6 @@ __global__ void k_solve_ea(const int* __restrict__ list,
   for (int e = threadIdx.x; e < c.q * nrhs; e += blockDim.x) {
     int i = e % c.q, k = e / c.q;
     dst[r[i] + (int64_t)k * dimp] += src[c.p + i + (int64_t)k * dimc];
-  }
-}
-
-// Solve of one kb x kb diagonal tile for every right-hand side: unit lower
-// (forward, upper = 0) or non-unit upper (backward, upper = 1).  One warp
-// per right-hand side, column-oriented so each step is one warp-wide axpy.
-template <typename T>
-__global__ void __launch_bounds__(256)
-    k_solve_diag(const int* __restrict__ active,
-                 const FrontDev* __restrict__ fr, const T* __restrict__ F,
-                 int k0, int nrhs, int upper, T* __restrict__ W) {
-  __shared__ T D[TB * TB];
-  __shared__ T x[8][TB];
-  const FrontDev f = fr[active[blockIdx.x]];
-  const int kb = min(TB, f.p - k0);
-  const int dim = f.p + f.q;
-  const T* src = F + f.off + k0 + (int64_t)k0 * f.ld;
-  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-    int i = e % kb, j = e / kb;
-    D[i + j * TB] = src[i + (int64_t)j * f.ld];
-  }
-  __syncthreads();
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  T* Wf = W + f.w_off * nrhs;
-  for (int r = warp; r < nrhs; r += blockDim.x / 32) {
-    T* w = Wf + (int64_t)r * dim + k0;
-    for (int i = lane; i < kb; i += 32) x[warp][i] = w[i];
-    __syncwarp();
-    if (!upper) {
-      for (int j = 0; j < kb; j++) {
-        T y = x[warp][j];
-        for (int i = j + 1 + lane; i < kb; i += 32) x[warp][i] -= D[i + j * TB] * y;
-        __syncwarp();
-      }
-    } else {
-      for (int j = kb - 1; j >= 0; j--) {
-        T y = x[warp][j] / D[j + j * TB];
-        __syncwarp();
-        if (lane == 0) x[warp][j] = y;
-        for (int i = lane; i < j; i += 32) x[warp][i] -= D[i + j * TB] * y;
-        __syncwarp();
-      }
-    }
-    for (int i = lane; i < kb; i += 32) w[i] = x[warp][i];
-    __syncwarp();
-  }
-}
-
-// Backward sweep helpers: X_Q of every front is gathered into the Q rows of
-// its work vector; after the sweep X_P is scattered to the solution.
-template <typename T>
-__global__ void k_solve_gather_q(const int* __restrict__ list,
-                                 const FrontDev* __restrict__ fr,
-                                 const int* __restrict__ gidx,
-                                 const double* __restrict__ X, int ldx,
-                                 int nrhs, T* __restrict__ W) {
-  const FrontDev f = fr[list[blockIdx.y]];
-  const int dim = f.p + f.q;
-  T* w = W + f.w_off * nrhs;
-  const int* g = gidx + f.idx_off;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < f.q * nrhs;
-       e += gridDim.x * blockDim.x) {
-    int t = e % f.q, r = e / f.q;
-    w[f.p + t + (int64_t)r * dim] = (T)X[g[f.p + t] + (int64_t)r * ldx];
-  }
-}
-
-template <typename T>
-__global__ void k_solve_scatter_p(const int* __restrict__ list,
-                                  const FrontDev* __restrict__ fr,
-                                  const int* __restrict__ gidx,
-                                  const T* __restrict__ W, int nrhs,
-                                  double* __restrict__ X, int ldx) {
-  const FrontDev f = fr[list[blockIdx.y]];
-  const int dim = f.p + f.q;
-  const T* w = W + f.w_off * nrhs;
-  const int* g = gidx + f.idx_off;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < f.p * nrhs;
-       e += gridDim.x * blockDim.x) {
-    int t = e % f.p, r = e / f.p;
-    X[g[t] + (int64_t)r * ldx] = (double)w[t + (int64_t)r * dim];
   }
 }
 

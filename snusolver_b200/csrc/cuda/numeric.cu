@@ -11,6 +11,8 @@
 
 #include "../engine.h"
 #include "kernels.cuh"
+#include "panel.cuh"
+#include "sweep.cuh"
 
 namespace snu {
 
@@ -74,13 +76,15 @@ struct LevelSched {
   GemmBatch f22;
   std::vector<double> ea_elems;  // per child rank: update entries added
   double solve_elems = 0;        // sum of front dims (per right-hand side)
+  // solve sweeps: per tile step the (front, row chunk) tasks
+  std::vector<SweepTask*> fwd, bwd;
+  std::vector<int> nfwd, nbwd;
+  std::vector<double> fwd_elems, bwd_elems;  // factor entries read per step
+  SweepTask* gq = nullptr;  // (front, 64-row chunk, 256-column chunk) of F12
+  int ngq = 0;
+  double gq_elems = 0;
 };
 
-struct SolveSched {
-  // per level: forward step GEMMs, backward F12 GEMM, backward step GEMMs
-  std::vector<std::vector<GemmBatch>> fwd, bwd;
-  std::vector<GemmBatch> bq;
-};
 
 constexpr int GBM = 64, GBN = 64;
 
@@ -97,6 +101,18 @@ class CudaEngine : public Engine {
     CK(cudaEventCreate(&ev1_));
     CK(cudaEventCreate(&sev0_));
     CK(cudaEventCreate(&sev1_));
+    CK(cudaFuncSetAttribute(k_diag_lu_inv<double>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)diag_smem<double>()));
+    CK(cudaFuncSetAttribute(k_diag_lu_inv<float>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)diag_smem<float>()));
+    CK(cudaFuncSetAttribute(k_panel_apply<double>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)apply_smem<double>()));
+    CK(cudaFuncSetAttribute(k_panel_apply<float>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)apply_smem<float>()));
     return ENG_OK;
   }
 
@@ -129,7 +145,7 @@ class CudaEngine : public Engine {
     arena_ = fp.arena;
     // fronts
     frh_.resize(nfronts_);
-    int64_t woff = 0;
+    int64_t woff = 0, yoff = 0, ioff = 0;
     wtot_ = 0;
     for (int f = 0; f < nfronts_; f++) {
       const FrontInfo& fi = fp.fronts[f];
@@ -145,9 +161,15 @@ class CudaEngine : public Engine {
       d.rel_off = fi.rel_offset;
       d.w_off = woff;
       woff += fi.p + fi.q;
+      d.y_off = yoff;
+      yoff += fi.p;
+      d.inv_off = ioff;
+      ioff += (int64_t)((fi.p + NB - 1) / NB) * 2 * NB * NB;
       frh_[f] = d;
     }
     wtot_ = woff;
+    ytot_ = yoff;
+    invtot_ = ioff;
     int rc;
     if ((rc = upload(d_fr_, frh_))) return rc;
     if ((rc = upload(d_gidx_, fp.gidx))) return rc;
@@ -187,12 +209,15 @@ class CudaEngine : public Engine {
     int rc;
     if (precision == 0) {
       if (!d_F64_ && (rc = alloc(d_F64_, (size_t)arena_))) return rc;
+      if (!d_I64_ && (rc = alloc(d_I64_, (size_t)invtot_))) return rc;
     } else {
       if (!d_F32_ && (rc = alloc(d_F32_, (size_t)arena_))) return rc;
+      if (!d_I32_ && (rc = alloc(d_I32_, (size_t)invtot_))) return rc;
     }
     CK(cudaMemsetAsync(d_flags_, 0, 4 * sizeof(int), stream_));
     CK(cudaEventRecord(ev0_, stream_));
-    rc = precision == 0 ? run_factor<double>(d_F64_) : run_factor<float>(d_F32_);
+    rc = precision == 0 ? run_factor<double>(d_F64_, d_I64_)
+                        : run_factor<float>(d_F32_, d_I32_);
     if (rc) return rc;
     CK(cudaEventRecord(ev1_, stream_));
     int flags[4];
@@ -233,7 +258,7 @@ class CudaEngine : public Engine {
     CK(cudaEventRecord(sev0_, st));
     SolveReport r;
     if (precision == 0) {
-      if ((rc = tree_solve<double>(d_F64_, d_W64_, dB, ldb, dX, ldb, nrhs, st)))
+      if ((rc = tree_solve<double>(d_F64_, d_I64_, d_W64_, d_Y64_, dB, ldb, dX, ldb, nrhs, st)))
         return rc;
       if ((rc = residual_norms(dB, ldb, dX, ldb, nrhs, st, &r.backward_error)))
         return rc;
@@ -501,7 +526,7 @@ class CudaEngine : public Engine {
           act.push_back(f);
           int kb = std::min(NB, fi.p - S.k0), k1 = S.k0 + kb;
           int dim = fi.p + fi.q, rem = dim - k1;
-          int chunks = (rem + 127) / 128;
+          int chunks = (rem + NB - 1) / NB;
           for (int c = 0; c < chunks; c++) {
             pt.push_back({f, 0, c});
             pt.push_back({f, 1, c});
@@ -535,57 +560,59 @@ class CudaEngine : public Engine {
                        o + fi.p * ld, o + fi.p + fi.p * ld});
       }
       if ((rc = gemm_batch(f22, L.f22))) return rc;
+      // solve sweeps
+      L.fwd.assign(nsteps, nullptr);
+      L.bwd.assign(nsteps, nullptr);
+      L.nfwd.assign(nsteps, 0);
+      L.nbwd.assign(nsteps, 0);
+      L.fwd_elems.assign(nsteps, 0.0);
+      L.bwd_elems.assign(nsteps, 0.0);
+      for (int s = 0; s < nsteps; s++) {
+        int k0 = s * NB;
+        std::vector<SweepTask> tf, tb;
+        for (int f = L.f0; f < L.f1; f++) {
+          const FrontInfo& fi = fp.fronts[f];
+          if (fi.p <= k0) continue;
+          int kb = std::min(NB, fi.p - k0), k1 = k0 + kb, dim = fi.p + fi.q;
+          int cf = std::max(1, (dim - k1 + SWEEP_ROWS - 1) / SWEEP_ROWS);
+          int cb = std::max(1, (k0 + SWEEP_ROWS - 1) / SWEEP_ROWS);
+          for (int c = 0; c < cf; c++) tf.push_back({f, c, 0});
+          for (int c = 0; c < cb; c++) tb.push_back({f, c, 0});
+          L.fwd_elems[s] += (double)(dim - k0) * kb;
+          L.bwd_elems[s] += (double)(k1) * kb;
+        }
+        L.nfwd[s] = (int)tf.size();
+        L.nbwd[s] = (int)tb.size();
+        if (!tf.empty() && (rc = upload(L.fwd[s], tf))) return rc;
+        if (!tb.empty() && (rc = upload(L.bwd[s], tb))) return rc;
+      }
+      std::vector<SweepTask> gq;
+      for (int f = L.f0; f < L.f1; f++) {
+        const FrontInfo& fi = fp.fronts[f];
+        if (fi.p == 0 || fi.q == 0) continue;
+        int rcn = (fi.p + GEMV_ROWS - 1) / GEMV_ROWS;
+        int kcn = (fi.q + GEMV_K - 1) / GEMV_K;
+        for (int a = 0; a < rcn; a++)
+          for (int b = 0; b < kcn; b++) gq.push_back({f, a, b});
+        L.gq_elems += (double)fi.p * fi.q;
+      }
+      L.ngq = (int)gq.size();
+      if (!gq.empty() && (rc = upload(L.gq, gq))) return rc;
     }
     return ENG_OK;
   }
 
   int ensure_solve(int nrhs) {
-    auto it = solve_sched_.find(nrhs);
-    if (it != solve_sched_.end()) return ENG_OK;
-    const FrontPlan& fp = *fp_;
-    SolveSched S;
-    S.fwd.resize(nlevels_);
-    S.bwd.resize(nlevels_);
-    S.bq.resize(nlevels_);
     int rc;
-    for (int l = 0; l < nlevels_; l++) {
-      LevelSched& L = lv_[l];
-      S.fwd[l].resize(L.steps.size());
-      S.bwd[l].resize(L.steps.size());
-      for (size_t s = 0; s < L.steps.size(); s++) {
-        int k0 = (int)s * TB;
-        std::vector<GemmProb> fw, bw;
-        for (int f = L.f0; f < L.f1; f++) {
-          const FrontInfo& fi = fp.fronts[f];
-          if (fi.p <= k0) continue;
-          int kb = std::min(TB, fi.p - k0), k1 = k0 + kb, dim = fi.p + fi.q;
-          int64_t w = frh_[f].w_off * nrhs, o = fi.offset, ld = fi.ld;
-          if (dim - k1 > 0)
-            fw.push_back({dim - k1, nrhs, kb, fi.ld, dim, dim, o + k1 + k0 * ld,
-                          w + k0, w + k1});
-          if (k0 > 0)
-            bw.push_back({k0, nrhs, kb, fi.ld, dim, dim, o + k0 * ld, w + k0, w});
-        }
-        if ((rc = gemm_batch(fw, S.fwd[l][s]))) return rc;
-        if ((rc = gemm_batch(bw, S.bwd[l][s]))) return rc;
-      }
-      std::vector<GemmProb> bq;
-      for (int f = L.f0; f < L.f1; f++) {
-        const FrontInfo& fi = fp.fronts[f];
-        if (fi.p == 0 || fi.q == 0) continue;
-        int dim = fi.p + fi.q;
-        int64_t w = frh_[f].w_off * nrhs, o = fi.offset, ld = fi.ld;
-        bq.push_back({fi.p, nrhs, fi.q, fi.ld, dim, dim, o + fi.p * ld,
-                      w + fi.p, w});
-      }
-      if ((rc = gemm_batch(bq, S.bq[l]))) return rc;
-    }
-    solve_sched_[nrhs] = std::move(S);
-    // work buffers sized for the largest nrhs seen
     if ((size_t)(wtot_ * nrhs) > wcap_) {
       wcap_ = (size_t)(wtot_ * nrhs);
       if ((rc = alloc(d_W64_, wcap_))) return rc;
       if ((rc = alloc(d_W32_, wcap_))) return rc;
+    }
+    if ((size_t)(ytot_ * nrhs) > ycap_) {
+      ycap_ = (size_t)(ytot_ * nrhs);
+      if ((rc = alloc(d_Y64_, ycap_))) return rc;
+      if ((rc = alloc(d_Y32_, ycap_))) return rc;
     }
     if ((size_t)n_ * nrhs > rcap_) {
       rcap_ = (size_t)n_ * nrhs;
@@ -609,7 +636,7 @@ class CudaEngine : public Engine {
   }
 
   template <typename T>
-  int run_factor(T* F) {
+  int run_factor(T* F, T* I) {
     cudaStream_t st = stream_;
     const double es = sizeof(T);
     int rc;
@@ -638,13 +665,14 @@ class CudaEngine : public Engine {
       }
       for (Step& S : L.steps) {
         pi = prof_begin(KF_DIAG_LU, st);
-        k_diag_lu<T><<<S.nactive, 256, 0, st>>>(S.active, d_fr_, F, S.k0,
-                                                opt_.pivot_eps, d_flags_);
+        k_diag_lu_inv<T><<<S.nactive, 256, diag_smem<T>(), st>>>(
+            S.active, d_fr_, F, I, S.k0, S.k0 / NB, opt_.pivot_eps, d_flags_);
         CKL();
         prof_end(pi, KF_DIAG_LU, st, S.diag_flops, S.diag_elems * es);
         if (S.npanel) {
           pi = prof_begin(KF_PANEL_TRSM, st);
-          k_panel_trsm<T><<<S.npanel, 128, 0, st>>>(S.panel, d_fr_, F, S.k0);
+          k_panel_apply<T><<<S.npanel, 256, apply_smem<T>(), st>>>(
+              S.panel, d_fr_, F, I, S.k0, S.k0 / NB);
           CKL();
           prof_end(pi, KF_PANEL_TRSM, st, S.panel_flops, S.panel_elems * es);
         }
@@ -657,11 +685,10 @@ class CudaEngine : public Engine {
   }
 
   template <typename T>
-  int tree_solve(const T* F, T* W, const double* B, int ldb, double* X,
-                 int ldx, int nrhs, cudaStream_t st) {
-    SolveSched& S = solve_sched_[nrhs];
+  int tree_solve(const T* F, const T* I, T* W, T* Y, const double* B, int ldb,
+                 double* X, int ldx, int nrhs, cudaStream_t st) {
     const double es = sizeof(T);
-    int rc, pi;
+    int pi;
     for (int l = 0; l < nlevels_; l++) {
       LevelSched& L = lv_[l];
       int nf = L.f1 - L.f0;
@@ -677,43 +704,44 @@ class CudaEngine : public Engine {
         CKL();
       }
       prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
-      for (size_t s = 0; s < L.steps.size(); s++) {
-        Step& St = L.steps[s];
+      for (size_t s = 0; s < L.fwd.size(); s++) {
+        if (!L.nfwd[s]) continue;
         pi = prof_begin(KF_SOLVE_DIAG, st);
-        k_solve_diag<T><<<St.nactive, 256, 0, st>>>(St.active, d_fr_, F,
-                                                    St.k0, nrhs, 0, W);
+        k_fwd_step<T><<<L.nfwd[s], 256, 0, st>>>(L.fwd[s], d_fr_, F, I,
+                                                 (int)s * NB, (int)s, nrhs, W, Y);
         CKL();
-        prof_end(pi, KF_SOLVE_DIAG, st, St.diag_flops * 0, St.diag_elems * es);
-        if ((rc = launch_gemm<T>(S.fwd[l][s], F, W, W, 0, st, KF_SOLVE_GEMM)))
-          return rc;
+        prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.fwd_elems[s] * nrhs,
+                 L.fwd_elems[s] * es);
       }
     }
     for (int l = nlevels_ - 1; l >= 0; l--) {
       LevelSched& L = lv_[l];
       int nf = L.f1 - L.f0;
       if (!nf) continue;
-      if (L.nlistq) {
-        pi = prof_begin(KF_SOLVE_MISC, st);
-        k_solve_gather_q<T><<<dim3(8, L.nlistq), 256, 0, st>>>(
-            L.listq, d_fr_, d_gidx_, X, ldx, nrhs, W);
+      pi = prof_begin(KF_SOLVE_MISC, st);
+      k_bwd_init<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_, X,
+                                                 ldx, nrhs, Y, W);
+      CKL();
+      prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
+      if (L.ngq) {
+        pi = prof_begin(KF_SOLVE_GEMM, st);
+        k_gemv_q<T><<<L.ngq, 256, 0, st>>>(L.gq, d_fr_, F, nrhs, W);
         CKL();
-        prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
-        if ((rc = launch_gemm<T>(S.bq[l], F, W, W, 0, st, KF_SOLVE_GEMM)))
-          return rc;
+        prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
+                 L.gq_elems * es);
       }
-      for (int s = (int)L.steps.size() - 1; s >= 0; s--) {
-        Step& St = L.steps[s];
+      for (int s = (int)L.bwd.size() - 1; s >= 0; s--) {
+        if (!L.nbwd[s]) continue;
         pi = prof_begin(KF_SOLVE_DIAG, st);
-        k_solve_diag<T><<<St.nactive, 256, 0, st>>>(St.active, d_fr_, F,
-                                                    St.k0, nrhs, 1, W);
+        k_bwd_step<T><<<L.nbwd[s], 256, 0, st>>>(L.bwd[s], d_fr_, F, I,
+                                                 s * NB, s, nrhs, W, Y);
         CKL();
-        prof_end(pi, KF_SOLVE_DIAG, st, 0, St.diag_elems * es);
-        if ((rc = launch_gemm<T>(S.bwd[l][s], F, W, W, 0, st, KF_SOLVE_GEMM)))
-          return rc;
+        prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.bwd_elems[s] * nrhs,
+                 L.bwd_elems[s] * es);
       }
       pi = prof_begin(KF_SOLVE_MISC, st);
-      k_solve_scatter_p<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_,
-                                                        W, nrhs, X, ldx);
+      k_scatter_y<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_, Y,
+                                                  nrhs, X, ldx);
       CKL();
       prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
     }
@@ -773,7 +801,7 @@ class CudaEngine : public Engine {
     int total = n_ * nrhs;
     int blocks = (total + 255) / 256;
     // x0 = solve32(b)
-    if ((rc = tree_solve<float>(d_F32_, d_W32_, B, ldb, X, ldx, nrhs, st)))
+    if ((rc = tree_solve<float>(d_F32_, d_I32_, d_W32_, d_Y32_, B, ldb, X, ldx, nrhs, st)))
       return rc;
     double be = 0, prev = INFINITY;
     int it = 0, stagnant = 0;
@@ -788,8 +816,8 @@ class CudaEngine : public Engine {
           int frc = factorize(0, &sec);
           if (frc) return frc;
         }
-        if ((rc = tree_solve<double>(d_F64_, d_W64_, d_R_, n_, d_D_, n_, nrhs,
-                                     st)))
+        if ((rc = tree_solve<double>(d_F64_, d_I64_, d_W64_, d_Y64_, d_R_, n_, d_D_, n_,
+                                     nrhs, st)))
           return rc;
         int pi = prof_begin(KF_RESIDUAL, st);
         k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
@@ -803,7 +831,7 @@ class CudaEngine : public Engine {
       else stagnant = 0;
       prev = be;
       // d = solve32(r); x += d
-      if ((rc = tree_solve<float>(d_F32_, d_W32_, d_R_, n_, d_D_, n_, nrhs, st)))
+      if ((rc = tree_solve<float>(d_F32_, d_I32_, d_W32_, d_Y32_, d_R_, n_, d_D_, n_, nrhs, st)))
         return rc;
       int pi = prof_begin(KF_RESIDUAL, st);
       k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
@@ -836,7 +864,12 @@ class CudaEngine : public Engine {
   const FrontPlan* fp_ = nullptr;
   int n_ = 0, nnz_ = 0, nfronts_ = 0, nlevels_ = 0;
   int64_t arena_ = 0, wtot_ = 0;
-  size_t wcap_ = 0, rcap_ = 0;
+  size_t wcap_ = 0, rcap_ = 0, ycap_ = 0;
+  int64_t ytot_ = 0, invtot_ = 0;
+  double* d_I64_ = nullptr;  // diagonal-tile inverses (FP64 factors)
+  float* d_I32_ = nullptr;   // diagonal-tile inverses (FP32 factors)
+  double* d_Y64_ = nullptr;
+  float* d_Y32_ = nullptr;
   std::vector<FrontDev> frh_;
   FrontDev* d_fr_ = nullptr;
   int *d_gidx_ = nullptr, *d_rel_ = nullptr, *d_asm_val_ = nullptr;
@@ -855,7 +888,6 @@ class CudaEngine : public Engine {
   std::vector<double> bnorm_;
   std::vector<int> rowptr_h_;
   std::vector<LevelSched> lv_;
-  std::map<int, SolveSched> solve_sched_;
 };
 
 }  // namespace
