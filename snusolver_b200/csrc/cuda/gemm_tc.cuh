@@ -1,0 +1,316 @@
+// Tensor-core (tcgen05, kind::tf32) batched GEMM for the FP32 path:
+// C -= A B with C column-major in the front arena.
+//
+// FP32 accuracy from TF32 tensor cores: every operand x is split into
+// hi = tf32(x) and lo = tf32(x - hi), and A B is formed as
+// A_hi B_hi + A_hi B_lo + A_lo B_hi (the lo*lo term is below FP32 rounding).
+// A pack kernel writes the three products as one GEMM of depth 3*kpad:
+// A' = [A_hi | A_hi | A_lo] and B' = [B_hi ; B_lo ; B_hi], both K-major
+// (row-major in K), kpad = k rounded up to 32.  The GEMM kernel then runs a
+// plain TF32 GEMM: TMA loads 128 x 32 (A') and BN x 32 (B') fp32 tiles with
+// 128-byte swizzle into a STAGES-deep shared-memory ring, one thread issues
+// tcgen05.mma (M=128, N=BN, K=8) into a TMEM accumulator, and the four warps
+// read the accumulator back with tcgen05.ld and subtract it from C.
+//
+// Every wait on an mbarrier is bounded; on timeout the kernel records the
+// failure in err[0], lets its in-flight work drain (bounded), frees its TMEM
+// and returns.
+#pragma once
+#include <cuda.h>
+#include <stdint.h>
+
+namespace snu {
+
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_STAGES = 6;
+constexpr long TC_SPIN_LIMIT = 1L << 24;
+
+struct TcProb {
+  int m, n, k, kpad;
+  int64_t a, b, c;  // element offsets of A, B, C in the front arena
+  int lda, ldb, ldc;
+  int64_t apack, bpack;  // element offsets of A', B' in the pack workspace
+};
+
+struct TcTile {
+  int prob, tm, tn;
+};
+
+// ------------------------------------------------------------------ pack
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// A' (m rows x 3*kpad) from A (m x k, column-major): 32 x 32 blocks through
+// shared memory so both the column-major reads and the row-major writes are
+// coalesced.  grid: (kpad/32, ceil(m/32), problems); block 32 x 8.
+__global__ void k_tc_pack_a(const TcProb* __restrict__ probs,
+                            const float* __restrict__ F, float* __restrict__ P) {
+  __shared__ float t[32][33];
+  const TcProb pr = probs[blockIdx.z];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  if (r0 >= pr.m || c0 >= pr.kpad) return;
+  const float* A = F + pr.a;
+  for (int cc = threadIdx.y; cc < 32; cc += 8) {
+    int r = r0 + threadIdx.x, c = c0 + cc;
+    t[cc][threadIdx.x] = (r < pr.m && c < pr.k) ? A[r + (int64_t)c * pr.lda] : 0.f;
+  }
+  __syncthreads();
+  float* out = P + pr.apack;
+  const int64_t kk = 3 * (int64_t)pr.kpad;
+  for (int rr = threadIdx.y; rr < 32; rr += 8) {
+    int r = r0 + rr, c = c0 + threadIdx.x;
+    if (r >= pr.m) continue;
+    float v = t[threadIdx.x][rr];
+    float hi = tf32_rna(v), lo = tf32_rna(v - hi);
+    float* row = out + r * kk;
+    row[c] = hi;
+    row[pr.kpad + c] = hi;
+    row[2 * pr.kpad + c] = lo;
+  }
+}
+
+// B' (n rows x 3*kpad) from B (k x n, column-major): column c of B is row c
+// of B', already contiguous.  grid: (ceil(n/8), problems); block 256.
+__global__ void k_tc_pack_b(const TcProb* __restrict__ probs,
+                            const float* __restrict__ F, float* __restrict__ P) {
+  const TcProb pr = probs[blockIdx.y];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * 8 + warp;
+  if (c >= pr.n) return;
+  const float* B = F + pr.b + (int64_t)c * pr.ldb;
+  float* row = P + pr.bpack + (int64_t)c * 3 * pr.kpad;
+  for (int kk = lane; kk < pr.kpad; kk += 32) {
+    float v = kk < pr.k ? B[kk] : 0.f;
+    float hi = tf32_rna(v), lo = tf32_rna(v - hi);
+    row[kk] = hi;
+    row[pr.kpad + kk] = lo;
+    row[2 * pr.kpad + kk] = hi;
+  }
+}
+
+// ------------------------------------------------------------ primitives
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile(
+      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+          smem_addr(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+// Bounded parity wait; returns false (and sets err) on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          int* err) {
+  const uint32_t a = smem_addr(bar);
+  for (long it = 0; it < TC_SPIN_LIMIT; it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  atomicExch(err, 1);
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map,
+                                            int c0, int c1, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::"
+      "bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_addr(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, rows of 128
+// bytes, 8-row groups 1024 bytes apart (SBO), version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;                  // LBO (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;        // SBO
+  d |= (uint64_t)1 << 46;                  // descriptor version
+  d |= (uint64_t)2 << 61;                  // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor: D f32, A/B tf32, both K-major, M = 128, N = BN.
+__host__ __device__ constexpr uint32_t tc_idesc(int bn) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(bn >> 3) << 17) |
+         ((uint32_t)(TC_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc,
+                                       uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+          tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+      "[%0];" ::"r"(smem_addr(bar))
+      : "memory");
+}
+
+constexpr size_t tc_smem_bytes() {
+  return 1024 /* alignment slack */ +
+         (size_t)TC_STAGES * (TC_BM + TC_BN) * TC_BK * sizeof(float);
+}
+
+// ----------------------------------------------------------------- GEMM
+
+__global__ void __launch_bounds__(128, 1)
+    k_gemm_tc(const TcTile* __restrict__ tiles, const TcProb* __restrict__ probs,
+              const CUtensorMap* __restrict__ amaps,
+              const CUtensorMap* __restrict__ bmaps, float* __restrict__ F,
+              int* err) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES], acc_bar;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int failed_s;
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  float* As = (float*)smem;                                   // [STAGES][BM*BK]
+  float* Bs = As + (size_t)TC_STAGES * TC_BM * TC_BK;         // [STAGES][BN*BK]
+  const TcTile tl = tiles[blockIdx.x];
+  const TcProb pr = probs[tl.prob];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nk = 3 * pr.kpad / TC_BK;
+
+  if (threadIdx.x == 0) {
+    failed_s = 0;
+    for (int s = 0; s < TC_STAGES; s++) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&acc_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile(
+        "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+            smem_addr(&tmem_base_s)),
+        "r"(TC_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_s;
+
+  int issued = 0;  // loads issued by the producer thread
+  if (warp == 0 && lane == 0) {
+    // producer: TMA ring
+    const CUtensorMap* am = amaps + tl.prob;
+    const CUtensorMap* bm = bmaps + tl.prob;
+    for (int kb = 0; kb < nk; kb++) {
+      const int s = kb % TC_STAGES;
+      if (kb >= TC_STAGES &&
+          !mbar_wait(&empty_bar[s], ((kb / TC_STAGES) - 1) & 1, err)) {
+        failed_s = 1;
+        break;
+      }
+      mbar_expect_tx(&full_bar[s], (TC_BM + TC_BN) * TC_BK * sizeof(float));
+      tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * TC_BK, tl.tm * TC_BM,
+                  &full_bar[s]);
+      tma_load_2d(Bs + (size_t)s * TC_BN * TC_BK, bm, kb * TC_BK, tl.tn * TC_BN,
+                  &full_bar[s]);
+      issued = kb + 1;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    const uint32_t idesc = tc_idesc(TC_BN);
+    for (int kb = 0; kb < nk; kb++) {
+      const int s = kb % TC_STAGES;
+      if (!mbar_wait(&full_bar[s], (kb / TC_STAGES) & 1, err)) {
+        failed_s = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_addr(As + (size_t)s * TC_BM * TC_BK);
+      const uint32_t b0 = smem_addr(Bs + (size_t)s * TC_BN * TC_BK);
+#pragma unroll
+      for (int kk = 0; kk < TC_BK / 8; kk++)
+        tc_mma(tmem, umma_desc(a0 + kk * 32), umma_desc(b0 + kk * 32), idesc,
+               (kb > 0 || kk > 0) ? 1u : 0u);
+      tc_commit(&empty_bar[s]);
+    }
+    tc_commit(&acc_bar);  // also after an early exit: drains issued MMAs
+  }
+  __syncthreads();  // every role has finished issuing
+
+  // epilogue: TMEM lanes 32w..32w+31 hold rows tm*128 + 32w + lane
+  const bool ok =
+      __syncthreads_and(mbar_wait(&acc_bar, 0, err) && !failed_s) != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok && nk > 0) {
+    const int row = tl.tm * TC_BM + warp * 32 + lane;
+    float* Cc = F + pr.c;
+    for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+      uint32_t v[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, "
+          "[%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]),
+            "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]),
+            "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+            "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+            "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+            "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+            "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < pr.m) {
+        // all 32 loads of the chunk first, then the stores (no load waits
+        // behind a store to a possibly aliasing address)
+        const int colbase = tl.tn * TC_BN + c0;
+        float* cp = Cc + row + (int64_t)colbase * pr.ldc;
+        const int ncol = min(32, pr.n - colbase);
+        float cv[32];
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+          cv[j] = j < ncol ? cp[(int64_t)j * pr.ldc] : 0.f;
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+          if (j < ncol) cp[(int64_t)j * pr.ldc] = cv[j] - __uint_as_float(v[j]);
+      }
+    }
+  }
+  // drain: after a failure the producer's last loads may still be in flight
+  if (!ok && warp == 0 && lane == 0)
+    for (int kb = issued > TC_STAGES ? issued - TC_STAGES : 0; kb < issued; kb++)
+      mbar_wait(&full_bar[kb % TC_STAGES], (kb / TC_STAGES) & 1, err);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 2)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
+                     tmem),
+                 "r"(TC_BN));
+}
+
+}  // namespace snu

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <vector>
@@ -13,6 +14,7 @@
 #include "kernels.cuh"
 #include "panel.cuh"
 #include "sweep.cuh"
+#include "gemm_tc.cuh"
 
 namespace snu {
 
@@ -43,12 +45,29 @@ struct DevVec {
 };
 
 struct GemmBatch {
-  GemmProb* probs = nullptr;
+  GemmProb* probs = nullptr;  // all problems (FP64 path, SIMT)
   GemmTile* tiles = nullptr;
   int ntiles = 0;
   double flops = 0;  // sum of 2 m n k
   double elems = 0;  // algorithmic elements moved: A + B read, C read+write
+  // FP32 path: problems large enough for the tensor cores, and the rest
+  std::vector<TcProb> tc_host;
+  TcProb* tcp = nullptr;
+  TcTile* tct = nullptr;
+  CUtensorMap* amaps = nullptr;
+  CUtensorMap* bmaps = nullptr;
+  int ntcp = 0, ntct = 0, tc_maxm = 0, tc_maxn = 0, tc_maxkpad = 0;
+  GemmProb* rprobs = nullptr;  // SIMT remainder of the FP32 path
+  GemmTile* rtiles = nullptr;
+  int nrtiles = 0;
 };
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType,
+                                  cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
 
 struct Step {
   int k0 = 0;
@@ -88,6 +107,18 @@ struct LevelSched {
 
 constexpr int GBM = 64, GBN = 64;
 
+#define SNU_LAUNCH_(K, T, R, CFG, ARGS) K<T, R><<<SNU_UNPACK CFG>>> ARGS
+#define SNU_UNPACK(...) __VA_ARGS__
+// Launch a sweep kernel specialized for the right-hand-side group width.
+#define SNU_RG_DISPATCH(nrhs, K, T, CFG, ARGS)        \
+  do {                                                \
+    if ((nrhs) <= 1) SNU_LAUNCH_(K, T, 1, CFG, ARGS);  \
+    else if ((nrhs) <= 2) SNU_LAUNCH_(K, T, 2, CFG, ARGS); \
+    else if ((nrhs) <= 4) SNU_LAUNCH_(K, T, 4, CFG, ARGS); \
+    else if ((nrhs) <= 8) SNU_LAUNCH_(K, T, 8, CFG, ARGS); \
+    else SNU_LAUNCH_(K, T, 16, CFG, ARGS);             \
+  } while (0)
+
 class CudaEngine : public Engine {
  public:
   explicit CudaEngine(const EngineOptions& o) : opt_(o) {}
@@ -107,6 +138,19 @@ class CudaEngine : public Engine {
     CK(cudaFuncSetAttribute(k_diag_lu_inv<float>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)diag_smem<float>()));
+    CK(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tc_smem_bytes()));
+    {
+      const char* e = getenv("SNU_TC_GEMM");
+      use_tc_ = !(e && e[0] == '0');
+    }
+    {
+      int rc2;
+      if ((rc2 = sweep_attr<double, 1>()) || (rc2 = sweep_attr<double, 2>()) ||
+          (rc2 = sweep_attr<double, 4>()) || (rc2 = sweep_attr<double, 8>()) ||
+          (rc2 = sweep_attr<double, 16>()))
+        return rc2;
+    }
     CK(cudaFuncSetAttribute(k_panel_apply<double>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)apply_smem<double>()));
@@ -184,6 +228,7 @@ class CudaEngine : public Engine {
     if ((rc = alloc(d_flags_, 4))) return rc;
     if ((rc = alloc(d_norms_, 3 * 64))) return rc;
     if ((rc = build_schedule())) return rc;
+    if ((rc = finalize_tc())) return rc;
     have64_ = have32_ = false;
     return ENG_OK;
   }
@@ -233,6 +278,10 @@ class CudaEngine : public Engine {
       have64_ = true;
     else
       have32_ = true;
+    if (flags[2]) {
+      err_ = "tensor-core GEMM pipeline wait timed out";
+      return ENG_ETIMEOUT;
+    }
     if (flags[1]) {
       err_ = "zero or non-finite pivot in the factorization";
       return ENG_ESINGULAR;
@@ -351,6 +400,17 @@ class CudaEngine : public Engine {
   }
 
  private:
+  template <typename T, int R>
+  int sweep_attr() {
+    CK(cudaFuncSetAttribute(k_fwd_step<T, R>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sweep_smem<T>()));
+    CK(cudaFuncSetAttribute(k_bwd_step<T, R>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sweep_smem<T>()));
+    return ENG_OK;
+  }
+
   // --------------------------------------------------------- profiling
   int prof_begin(int fam, cudaStream_t st) {
     if (!((prof_mask_ >> fam) & 1u)) return -1;
@@ -444,13 +504,23 @@ class CudaEngine : public Engine {
   }
 
   // ---------------------------------------------------------- schedule
-  int gemm_batch(const std::vector<GemmProb>& probs, GemmBatch& gb) {
-    std::vector<GemmTile> tiles;
+  static void tiles_of(const std::vector<GemmProb>& probs,
+                       std::vector<GemmTile>& tiles) {
     for (size_t k = 0; k < probs.size(); k++) {
       int tm = (probs[k].m + GBM - 1) / GBM, tn = (probs[k].n + GBN - 1) / GBN;
       for (int b = 0; b < tn; b++)
         for (int a = 0; a < tm; a++) tiles.push_back({(int)k, a, b});
     }
+  }
+
+  // Tensor-core eligibility of a problem on the FP32 path.
+  static bool tc_eligible(const GemmProb& g) {
+    return g.m >= TC_BM && g.n >= TC_BN && g.k >= 16;
+  }
+
+  int gemm_batch(const std::vector<GemmProb>& probs, GemmBatch& gb) {
+    std::vector<GemmTile> tiles;
+    tiles_of(probs, tiles);
     gb.ntiles = (int)tiles.size();
     for (const GemmProb& g : probs) {
       gb.flops += 2.0 * g.m * (double)g.n * g.k;
@@ -460,6 +530,93 @@ class CudaEngine : public Engine {
     int rc;
     if ((rc = upload(gb.probs, probs))) return rc;
     if ((rc = upload(gb.tiles, tiles))) return rc;
+    // FP32 split
+    std::vector<GemmProb> rest;
+    int64_t apos = 0;
+    for (const GemmProb& g : probs) {
+      if (!tc_eligible(g)) {
+        rest.push_back(g);
+        continue;
+      }
+      TcProb t;
+      t.m = g.m, t.n = g.n, t.k = g.k, t.kpad = (g.k + TC_BK - 1) / TC_BK * TC_BK;
+      t.a = g.a, t.b = g.b, t.c = g.c;
+      t.lda = g.lda, t.ldb = g.ldb, t.ldc = g.ldc;
+      t.apack = apos;
+      apos += (int64_t)g.m * 3 * t.kpad;
+      apos = (apos + 63) / 64 * 64;
+      t.bpack = apos;
+      apos += (int64_t)g.n * 3 * t.kpad;
+      apos = (apos + 63) / 64 * 64;
+      gb.tc_host.push_back(t);
+      gb.tc_maxm = std::max(gb.tc_maxm, g.m);
+      gb.tc_maxn = std::max(gb.tc_maxn, g.n);
+      gb.tc_maxkpad = std::max(gb.tc_maxkpad, t.kpad);
+    }
+    pack_need_ = std::max(pack_need_, apos);
+    if (!gb.tc_host.empty()) tc_batches_.push_back(&gb);
+    std::vector<GemmTile> rt;
+    tiles_of(rest, rt);
+    gb.nrtiles = (int)rt.size();
+    if (!rt.empty()) {
+      if ((rc = upload(gb.rprobs, rest))) return rc;
+      if ((rc = upload(gb.rtiles, rt))) return rc;
+    }
+    return ENG_OK;
+  }
+
+  // After the schedule: one pack workspace for the largest tensor-core batch
+  // and a TMA map for every packed operand (the workspace address is fixed).
+  int finalize_tc() {
+    int rc;
+    if (tc_batches_.empty()) return ENG_OK;
+    if ((rc = alloc(d_pack_, (size_t)pack_need_))) return rc;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault,
+                               &q));
+    if (!fn || q != cudaDriverEntryPointSuccess) {
+      err_ = "cuTensorMapEncodeTiled unavailable";
+      return ENG_ECUDA;
+    }
+    EncodeTiledFn enc = (EncodeTiledFn)fn;
+    for (GemmBatch* gb : tc_batches_) {
+      std::vector<CUtensorMap> am(gb->tc_host.size()), bm(gb->tc_host.size());
+      std::vector<TcTile> tiles;
+      for (size_t k = 0; k < gb->tc_host.size(); k++) {
+        const TcProb& t = gb->tc_host[k];
+        const cuuint64_t kk = 3 * (cuuint64_t)t.kpad;
+        cuuint64_t dimA[2] = {kk, (cuuint64_t)t.m}, dimB[2] = {kk, (cuuint64_t)t.n};
+        cuuint64_t stride[1] = {kk * sizeof(float)};
+        cuuint32_t boxA[2] = {TC_BK, TC_BM}, boxB[2] = {TC_BK, TC_BN};
+        cuuint32_t es[2] = {1, 1};
+        CUresult r1 = enc(&am[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                          d_pack_ + t.apack, dimA, stride, boxA, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        CUresult r2 = enc(&bm[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                          d_pack_ + t.bpack, dimB, stride, boxB, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) {
+          err_ = "tensor map encoding failed";
+          return ENG_ECUDA;
+        }
+        int tm = (t.m + TC_BM - 1) / TC_BM, tn = (t.n + TC_BN - 1) / TC_BN;
+        for (int b = 0; b < tn; b++)
+          for (int a = 0; a < tm; a++) tiles.push_back({(int)k, a, b});
+      }
+      gb->ntcp = (int)gb->tc_host.size();
+      gb->ntct = (int)tiles.size();
+      if ((rc = upload(gb->tcp, gb->tc_host))) return rc;
+      if ((rc = upload(gb->tct, tiles))) return rc;
+      if ((rc = upload(gb->amaps, am))) return rc;
+      if ((rc = upload(gb->bmaps, bm))) return rc;
+    }
     return ENG_OK;
   }
 
@@ -635,6 +792,33 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
+  // Factorization GEMMs (C -= A B inside the arena).  FP32: tensor-core
+  // problems through pack + tcgen05, the remainder on the SIMT kernel.
+  int factor_gemm(const GemmBatch& gb, double* F, cudaStream_t st, int fam) {
+    return launch_gemm<double>(gb, F, F, F, 0, st, fam);
+  }
+  int factor_gemm(const GemmBatch& gb, float* F, cudaStream_t st, int fam) {
+    if (gb.ntiles == 0) return ENG_OK;
+    if (!use_tc_ || gb.ntcp == 0) return launch_gemm<float>(gb, F, F, F, 0, st, fam);
+    int pi = prof_begin(fam, st);
+    dim3 ga(gb.tc_maxkpad / 32, (gb.tc_maxm + 31) / 32, gb.ntcp);
+    k_tc_pack_a<<<ga, dim3(32, 8), 0, st>>>(gb.tcp, F, d_pack_);
+    CKL();
+    dim3 gbp((gb.tc_maxn + 7) / 8, gb.ntcp);
+    k_tc_pack_b<<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
+    CKL();
+    k_gemm_tc<<<gb.ntct, 128, tc_smem_bytes(), st>>>(gb.tct, gb.tcp, gb.amaps,
+                                                    gb.bmaps, F, d_flags_ + 2);
+    CKL();
+    if (gb.nrtiles) {
+      k_gemm<float, GBM, GBN, 16, 4, 4><<<gb.nrtiles, 256, 0, st>>>(
+          gb.rtiles, gb.rprobs, F, F, F, 0);
+      CKL();
+    }
+    prof_end(pi, fam, st, gb.flops, gb.elems * sizeof(float));
+    return ENG_OK;
+  }
+
   template <typename T>
   int run_factor(T* F, T* I) {
     cudaStream_t st = stream_;
@@ -676,10 +860,9 @@ class CudaEngine : public Engine {
           CKL();
           prof_end(pi, KF_PANEL_TRSM, st, S.panel_flops, S.panel_elems * es);
         }
-        if ((rc = launch_gemm<T>(S.trail, F, F, F, 0, st, KF_GEMM_TRAIL)))
-          return rc;
+        if ((rc = factor_gemm(S.trail, F, st, KF_GEMM_TRAIL))) return rc;
       }
-      if ((rc = launch_gemm<T>(L.f22, F, F, F, 0, st, KF_GEMM_SCHUR))) return rc;
+      if ((rc = factor_gemm(L.f22, F, st, KF_GEMM_SCHUR))) return rc;
     }
     return ENG_OK;
   }
@@ -707,8 +890,9 @@ class CudaEngine : public Engine {
       for (size_t s = 0; s < L.fwd.size(); s++) {
         if (!L.nfwd[s]) continue;
         pi = prof_begin(KF_SOLVE_DIAG, st);
-        k_fwd_step<T><<<L.nfwd[s], 256, 0, st>>>(L.fwd[s], d_fr_, F, I,
-                                                 (int)s * NB, (int)s, nrhs, W, Y);
+        SNU_RG_DISPATCH(nrhs, k_fwd_step, T,
+                        (L.nfwd[s], 256, sweep_smem<T>(), st),
+                        (L.fwd[s], d_fr_, F, I, (int)s * NB, (int)s, nrhs, W, Y));
         CKL();
         prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.fwd_elems[s] * nrhs,
                  L.fwd_elems[s] * es);
@@ -725,7 +909,8 @@ class CudaEngine : public Engine {
       prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
       if (L.ngq) {
         pi = prof_begin(KF_SOLVE_GEMM, st);
-        k_gemv_q<T><<<L.ngq, 256, 0, st>>>(L.gq, d_fr_, F, nrhs, W);
+        SNU_RG_DISPATCH(nrhs, k_gemv_q, T, (L.ngq, 256, 0, st),
+                        (L.gq, d_fr_, F, nrhs, W));
         CKL();
         prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
                  L.gq_elems * es);
@@ -733,8 +918,9 @@ class CudaEngine : public Engine {
       for (int s = (int)L.bwd.size() - 1; s >= 0; s--) {
         if (!L.nbwd[s]) continue;
         pi = prof_begin(KF_SOLVE_DIAG, st);
-        k_bwd_step<T><<<L.nbwd[s], 256, 0, st>>>(L.bwd[s], d_fr_, F, I,
-                                                 s * NB, s, nrhs, W, Y);
+        SNU_RG_DISPATCH(nrhs, k_bwd_step, T,
+                        (L.nbwd[s], 256, sweep_smem<T>(), st),
+                        (L.bwd[s], d_fr_, F, I, s * NB, s, nrhs, W, Y));
         CKL();
         prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.bwd_elems[s] * nrhs,
                  L.bwd_elems[s] * es);
@@ -866,6 +1052,11 @@ class CudaEngine : public Engine {
   int64_t arena_ = 0, wtot_ = 0;
   size_t wcap_ = 0, rcap_ = 0, ycap_ = 0;
   int64_t ytot_ = 0, invtot_ = 0;
+  // tensor-core GEMM workspace (packed split operands) and its batches
+  float* d_pack_ = nullptr;
+  int64_t pack_need_ = 0;
+  std::vector<GemmBatch*> tc_batches_;
+  bool use_tc_ = true;
   double* d_I64_ = nullptr;  // diagonal-tile inverses (FP64 factors)
   float* d_I32_ = nullptr;   // diagonal-tile inverses (FP32 factors)
   double* d_Y64_ = nullptr;

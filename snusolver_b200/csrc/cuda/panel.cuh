@@ -12,10 +12,15 @@ namespace snu {
 // Shared-memory tile, column-major with one element of padding per column.
 constexpr int TLD = NB + 1;
 
-// Dynamic shared memory of k_diag_lu_inv: D, Linv, Uinv.
+// Correctly rounded reciprocal (CUDA intrinsics): multipliers are formed as
+// x * (1/p) instead of x / p, one reciprocal per pivot.
+__device__ __forceinline__ float recip_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double recip_rn(double x) { return __drcp_rn(x); }
+
+// Dynamic shared memory of k_diag_lu_inv: the factored tile.
 template <typename T>
 constexpr size_t diag_smem() {
-  return 3 * (size_t)NB * TLD * sizeof(T);
+  return (size_t)NB * TLD * sizeof(T);
 }
 
 // LU without pivoting of the diagonal tile at (k0, k0) of every active front
@@ -25,6 +30,13 @@ constexpr size_t diag_smem() {
 // separator fronts do not guard, like cusolverDnDgetrf without a pivot
 // array (kernel_cuda.cu:45-73).  flags[0] counts replaced pivots, flags[1]
 // records a zero or non-finite pivot.
+//
+// Each of the 256 threads keeps a 4 x 4 strided block of the tile in
+// registers (rows tx + 16a, columns ty + 16b).  Step k reads the pivot row
+// and column from a double-buffered shared copy that their owners refresh
+// right after their own update, so every elimination step (and every
+// inverse step) costs one barrier.  A tile smaller than NB is padded with
+// the identity, which leaves its factors and inverses unchanged.
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_diag_lu_inv(const int* __restrict__ active,
@@ -32,71 +44,185 @@ __global__ void __launch_bounds__(256)
                   T* __restrict__ INV, int k0, int step, double eps,
                   int* flags) {
   extern __shared__ unsigned char smem_raw[];
-  T* D = reinterpret_cast<T*>(smem_raw);
-  T* XL = D + NB * TLD;
-  T* XU = XL + NB * TLD;
+  T* LU = reinterpret_cast<T*>(smem_raw);
+  __shared__ T rowb[2][NB], colb[2][NB];
   const FrontDev f = fr[active[blockIdx.x]];
   const int kb = min(NB, f.p - k0);
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   T* base = F + f.off + k0 + (int64_t)k0 * f.ld;
-  for (int j = ty; j < kb; j += 16)
-    for (int i = tx; i < kb; i += 16) D[i + j * TLD] = base[i + (int64_t)j * f.ld];
-  for (int j = ty; j < NB; j += 16)
-    for (int i = tx; i < NB; i += 16) {
-      T v = (i == j) ? (T)1 : (T)0;
-      XL[i + j * TLD] = v;
-      XU[i + j * TLD] = v;
+  T a[4][4];
+#pragma unroll
+  for (int ia = 0; ia < 4; ia++)
+#pragma unroll
+    for (int jb = 0; jb < 4; jb++) {
+      int i = tx + 16 * ia, j = ty + 16 * jb;
+      a[ia][jb] = (i < kb && j < kb) ? base[i + (int64_t)j * f.ld]
+                                     : (i == j ? (T)1 : (T)0);
     }
+  // publish row 0 and column 0
+  if (tx == 0)
+#pragma unroll
+    for (int jb = 0; jb < 4; jb++) rowb[0][ty + 16 * jb] = a[0][jb];
+  if (ty == 0)
+#pragma unroll
+    for (int ia = 0; ia < 4; ia++) colb[0][tx + 16 * ia] = a[ia][0];
   __syncthreads();
   const T teps = (T)eps;
-  for (int kk = 0; kk < kb; kk++) {
-    T piv = D[kk + kk * TLD];
+  for (int k = 0; k < NB; k++) {
+    const int cb = k & 1, nb = cb ^ 1;
+    T piv = rowb[cb][k];
     bool guarded = false;
-    if (f.guard && piv < teps && piv > -teps) {
+    if (k < kb && f.guard && piv < teps && piv > -teps) {
       piv = piv < (T)0 ? -teps : teps;
       guarded = true;
     }
-    if (tid < kb && tid > kk) D[tid + kk * TLD] /= piv;
-    __syncthreads();
-    if (tid == 0) {
-      if (guarded) {
-        D[kk + kk * TLD] = piv;
-        atomicAdd(flags, 1);
-      }
+    const T rp = recip_rn(piv);
+    T li[4], rj[4];
+#pragma unroll
+    for (int ia = 0; ia < 4; ia++) {
+      const int i = tx + 16 * ia;
+      li[ia] = i > k ? colb[cb][i] * rp : (T)0;
+    }
+#pragma unroll
+    for (int jb = 0; jb < 4; jb++) {
+      const int j = ty + 16 * jb;
+      rj[jb] = j > k ? rowb[cb][j] : (T)0;
+    }
+#pragma unroll
+    for (int ia = 0; ia < 4; ia++)
+#pragma unroll
+      for (int jb = 0; jb < 4; jb++) a[ia][jb] -= li[ia] * rj[jb];
+    // column k keeps the multipliers, (k, k) the (guarded) pivot
+#pragma unroll
+    for (int jb = 0; jb < 4; jb++)
+      if (ty + 16 * jb == k)
+#pragma unroll
+        for (int ia = 0; ia < 4; ia++) {
+          const int i = tx + 16 * ia;
+          if (i > k) a[ia][jb] = li[ia];
+          if (i == k) a[ia][jb] = piv;
+        }
+    if (k < kb && tx == (k & 15) && ty == (k & 15)) {
+      if (guarded) atomicAdd(flags, 1);
       if (!(piv != (T)0) || !isfinite((double)piv)) flags[1] = 1;
     }
-    for (int j = kk + 1 + ty; j < kb; j += 16) {
-      const T u = D[kk + j * TLD];
-      for (int i = kk + 1 + tx; i < kb; i += 16)
-        D[i + j * TLD] -= D[i + kk * TLD] * u;
+    if (k + 1 < NB) {
+      const int r = k + 1;
+#pragma unroll
+      for (int ia = 0; ia < 4; ia++)
+        if (tx + 16 * ia == r)
+#pragma unroll
+          for (int jb = 0; jb < 4; jb++) rowb[nb][ty + 16 * jb] = a[ia][jb];
+#pragma unroll
+      for (int jb = 0; jb < 4; jb++)
+        if (ty + 16 * jb == r)
+#pragma unroll
+          for (int ia = 0; ia < 4; ia++) colb[nb][tx + 16 * ia] = a[ia][jb];
     }
     __syncthreads();
   }
-  // Linv: L X = I, row k of X is final once rows < k have been applied.
-  // Uinv: U X = I, processed from the bottom: row k is divided by U[k,k]
-  // and then eliminated from the rows above.  Both in the same loop.
-  for (int k = 0; k < kb; k++) {
-    const int ku = kb - 1 - k;
-    if (tid < NB) XU[ku + tid * TLD] /= D[ku + ku * TLD];
-    __syncthreads();
-    for (int j = ty; j <= k; j += 16) {
-      const T x = XL[k + j * TLD];
-      for (int i = k + 1 + tx; i < kb; i += 16) XL[i + j * TLD] -= D[i + k * TLD] * x;
+  // factored tile to the front and to shared memory (columns of L and U
+  // for the inverses)
+#pragma unroll
+  for (int ia = 0; ia < 4; ia++)
+#pragma unroll
+    for (int jb = 0; jb < 4; jb++) {
+      const int i = tx + 16 * ia, j = ty + 16 * jb;
+      LU[i + j * TLD] = a[ia][jb];
+      if (i < kb && j < kb) base[i + (int64_t)j * f.ld] = a[ia][jb];
     }
-    for (int j = ku + ty; j < kb; j += 16) {
-      const T x = XU[ku + j * TLD];
-      for (int i = tx; i < ku; i += 16) XU[i + j * TLD] -= D[i + ku * TLD] * x;
-    }
-    __syncthreads();
-  }
-  for (int j = ty; j < kb; j += 16)
-    for (int i = tx; i < kb; i += 16) base[i + (int64_t)j * f.ld] = D[i + j * TLD];
+  __syncthreads();
   T* inv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
-  for (int j = ty; j < NB; j += 16)
-    for (int i = tx; i < NB; i += 16) {
-      inv[i + j * NB] = XL[i + j * TLD];
-      inv[NB * NB + i + j * NB] = XU[i + j * TLD];
+  // Linv: rows top-down, X[i,:] -= L[i,k] X[k,:] once row k is final.
+  {
+    T x[4][4];
+#pragma unroll
+    for (int ia = 0; ia < 4; ia++)
+#pragma unroll
+      for (int jb = 0; jb < 4; jb++)
+        x[ia][jb] = (tx + 16 * ia == ty + 16 * jb) ? (T)1 : (T)0;
+    if (tx == 0)
+#pragma unroll
+      for (int jb = 0; jb < 4; jb++) rowb[0][ty + 16 * jb] = x[0][jb];
+    __syncthreads();
+    for (int k = 0; k < NB; k++) {
+      const int cb = k & 1, nb = cb ^ 1;
+      T rv[4];
+#pragma unroll
+      for (int jb = 0; jb < 4; jb++) rv[jb] = rowb[cb][ty + 16 * jb];
+#pragma unroll
+      for (int ia = 0; ia < 4; ia++) {
+        const int i = tx + 16 * ia;
+        const T lk = i > k ? LU[i + k * TLD] : (T)0;
+#pragma unroll
+        for (int jb = 0; jb < 4; jb++) x[ia][jb] -= lk * rv[jb];
+      }
+      const int r = k + 1;
+#pragma unroll
+      for (int ia = 0; ia < 4; ia++)
+        if (tx + 16 * ia == r)
+#pragma unroll
+          for (int jb = 0; jb < 4; jb++) rowb[nb][ty + 16 * jb] = x[ia][jb];
+      __syncthreads();
     }
+#pragma unroll
+    for (int ia = 0; ia < 4; ia++)
+#pragma unroll
+      for (int jb = 0; jb < 4; jb++)
+        inv[tx + 16 * ia + (ty + 16 * jb) * NB] = x[ia][jb];
+  }
+  // Uinv: rows bottom-up, Y[ku,:] /= U[ku,ku], then Y[i,:] -= U[i,ku] Y[ku,:].
+  {
+    T y[4][4];
+#pragma unroll
+    for (int ia = 0; ia < 4; ia++)
+#pragma unroll
+      for (int jb = 0; jb < 4; jb++)
+        y[ia][jb] = (tx + 16 * ia == ty + 16 * jb) ? (T)1 : (T)0;
+    {
+      const T rd = recip_rn(LU[(NB - 1) + (NB - 1) * TLD]);
+#pragma unroll
+      for (int ia = 0; ia < 4; ia++)
+        if (tx + 16 * ia == NB - 1)
+#pragma unroll
+          for (int jb = 0; jb < 4; jb++) {
+            y[ia][jb] *= rd;
+            colb[0][ty + 16 * jb] = y[ia][jb];
+          }
+    }
+    __syncthreads();
+    for (int k = 0; k < NB; k++) {
+      const int cb = k & 1, nb = cb ^ 1, ku = NB - 1 - k;
+      T cv[4];
+#pragma unroll
+      for (int jb = 0; jb < 4; jb++) cv[jb] = colb[cb][ty + 16 * jb];
+#pragma unroll
+      for (int ia = 0; ia < 4; ia++) {
+        const int i = tx + 16 * ia;
+        const T uk = i < ku ? LU[i + ku * TLD] : (T)0;
+#pragma unroll
+        for (int jb = 0; jb < 4; jb++) y[ia][jb] -= uk * cv[jb];
+      }
+      const int ru = ku - 1;
+      if (ru >= 0 && tx == (ru & 15)) {
+        const T rd = recip_rn(LU[ru + ru * TLD]);
+#pragma unroll
+        for (int ia = 0; ia < 4; ia++)
+          if (tx + 16 * ia == ru)
+#pragma unroll
+            for (int jb = 0; jb < 4; jb++) {
+              y[ia][jb] *= rd;
+              colb[nb][ty + 16 * jb] = y[ia][jb];
+            }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int ia = 0; ia < 4; ia++)
+#pragma unroll
+      for (int jb = 0; jb < 4; jb++)
+        inv[NB * NB + tx + 16 * ia + (ty + 16 * jb) * NB] = y[ia][jb];
+  }
 }
 
 // Dynamic shared memory of k_panel_apply: the panel tile and the inverse.

@@ -15,55 +15,67 @@ namespace snu {
 constexpr int SWEEP_ROWS = 256;  // rows updated per CTA
 constexpr int RG = 16;           // right-hand sides per register group
 
+// Dynamic shared memory of the sweep steps: the staged tile inverse.
+template <typename T>
+constexpr size_t sweep_smem() {
+  return (size_t)NB * (NB + 1) * sizeof(T);
+}
+
 // Forward step at tile (k0, kb): y = Linv * W[k0:k1]; Y[k0:k1] = y (chunk
 // 0); W[r] -= L[r, k0:k1] y for the CTA's rows r >= k1.
-template <typename T>
+template <typename T, int R>
 __global__ void __launch_bounds__(256)
     k_fwd_step(const SweepTask* __restrict__ tasks,
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                const T* __restrict__ INV, int k0, int step, int nrhs,
                T* __restrict__ W, T* __restrict__ Y) {
-  __shared__ T ws[NB][RG];
-  __shared__ T ys[NB][RG];
+  extern __shared__ unsigned char smem_raw[];
+  T* X = reinterpret_cast<T*>(smem_raw);  // Linv, leading dimension NB + 1
+  __shared__ T ws[NB][R];
+  __shared__ T ys[NB][R];
   const SweepTask t = tasks[blockIdx.x];
   const FrontDev f = fr[t.front];
   const int kb = min(NB, f.p - k0), k1 = k0 + kb, dim = f.p + f.q;
   const T* linv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x)
+    X[(e % NB) + (e / NB) * (NB + 1)] = linv[e];
   T* Wf = W + f.w_off * nrhs;
   T* Yf = Y + f.y_off * nrhs;
   const int tid = threadIdx.x;
   const int row = k1 + t.chunk * SWEEP_ROWS + tid;
   const T* lrow = F + f.off + row + (int64_t)k0 * f.ld;
-  for (int r0 = 0; r0 < nrhs; r0 += RG) {
-    const int nr = min(RG, nrhs - r0);
-    for (int e = tid; e < NB * RG; e += blockDim.x) {
+  for (int r0 = 0; r0 < nrhs; r0 += R) {
+    const int nr = min(R, nrhs - r0);
+    for (int e = tid; e < NB * R; e += blockDim.x) {
       int i = e % NB, r = e / NB;
       ws[i][r] = (i < kb && r < nr) ? Wf[k0 + i + (int64_t)(r0 + r) * dim] : (T)0;
     }
     __syncthreads();
-    for (int e = tid; e < NB * RG; e += blockDim.x) {
+    for (int e = tid; e < NB * R; e += blockDim.x) {
       int i = e % NB, r = e / NB;
       T s = (T)0;
       if (i < kb && r < nr)
-        for (int m = 0; m <= i; m++) s += linv[i + m * NB] * ws[m][r];
+        for (int m = 0; m <= i; m++) s += X[i + m * (NB + 1)] * ws[m][r];
       ys[i][r] = s;
     }
     __syncthreads();
     if (t.chunk == 0)
-      for (int e = tid; e < NB * RG; e += blockDim.x) {
+      for (int e = tid; e < NB * R; e += blockDim.x) {
         int i = e % NB, r = e / NB;
         if (i < kb && r < nr) Yf[k0 + i + (int64_t)(r0 + r) * f.p] = ys[i][r];
       }
     if (row < dim) {
-      T acc[RG];
+      T acc[R];
 #pragma unroll
-      for (int r = 0; r < RG; r++) acc[r] = (T)0;
+      for (int r = 0; r < R; r++) acc[r] = (T)0;
       for (int m = 0; m < kb; m++) {
         const T l = lrow[(int64_t)m * f.ld];
 #pragma unroll
-        for (int r = 0; r < RG; r++) acc[r] += l * ys[m][r];
+        for (int r = 0; r < R; r++) acc[r] += l * ys[m][r];
       }
-      for (int r = 0; r < nr; r++) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        if (r < nr) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
     }
     __syncthreads();
   }
@@ -71,53 +83,59 @@ __global__ void __launch_bounds__(256)
 
 // Backward step at tile (k0, kb): x = Uinv * W[k0:k1]; Y[k0:k1] = x (chunk
 // 0); W[r] -= U[r, k0:k1] x for the CTA's rows r < k0.
-template <typename T>
+template <typename T, int R>
 __global__ void __launch_bounds__(256)
     k_bwd_step(const SweepTask* __restrict__ tasks,
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                const T* __restrict__ INV, int k0, int step, int nrhs,
                T* __restrict__ W, T* __restrict__ Y) {
-  __shared__ T ws[NB][RG];
-  __shared__ T xs[NB][RG];
+  extern __shared__ unsigned char smem_raw[];
+  T* X = reinterpret_cast<T*>(smem_raw);  // Uinv, leading dimension NB + 1
+  __shared__ T ws[NB][R];
+  __shared__ T xs[NB][R];
   const SweepTask t = tasks[blockIdx.x];
   const FrontDev f = fr[t.front];
   const int kb = min(NB, f.p - k0), dim = f.p + f.q;
   const T* uinv = INV + f.inv_off + (int64_t)step * 2 * NB * NB + NB * NB;
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x)
+    X[(e % NB) + (e / NB) * (NB + 1)] = uinv[e];
   T* Wf = W + f.w_off * nrhs;
   T* Yf = Y + f.y_off * nrhs;
   const int tid = threadIdx.x;
   const int row = t.chunk * SWEEP_ROWS + tid;
   const T* urow = F + f.off + row + (int64_t)k0 * f.ld;
-  for (int r0 = 0; r0 < nrhs; r0 += RG) {
-    const int nr = min(RG, nrhs - r0);
-    for (int e = tid; e < NB * RG; e += blockDim.x) {
+  for (int r0 = 0; r0 < nrhs; r0 += R) {
+    const int nr = min(R, nrhs - r0);
+    for (int e = tid; e < NB * R; e += blockDim.x) {
       int i = e % NB, r = e / NB;
       ws[i][r] = (i < kb && r < nr) ? Wf[k0 + i + (int64_t)(r0 + r) * dim] : (T)0;
     }
     __syncthreads();
-    for (int e = tid; e < NB * RG; e += blockDim.x) {
+    for (int e = tid; e < NB * R; e += blockDim.x) {
       int i = e % NB, r = e / NB;
       T s = (T)0;
       if (i < kb && r < nr)
-        for (int m = i; m < kb; m++) s += uinv[i + m * NB] * ws[m][r];
+        for (int m = i; m < kb; m++) s += X[i + m * (NB + 1)] * ws[m][r];
       xs[i][r] = s;
     }
     __syncthreads();
     if (t.chunk == 0)
-      for (int e = tid; e < NB * RG; e += blockDim.x) {
+      for (int e = tid; e < NB * R; e += blockDim.x) {
         int i = e % NB, r = e / NB;
         if (i < kb && r < nr) Yf[k0 + i + (int64_t)(r0 + r) * f.p] = xs[i][r];
       }
     if (row < k0) {
-      T acc[RG];
+      T acc[R];
 #pragma unroll
-      for (int r = 0; r < RG; r++) acc[r] = (T)0;
+      for (int r = 0; r < R; r++) acc[r] = (T)0;
       for (int m = 0; m < kb; m++) {
         const T u = urow[(int64_t)m * f.ld];
 #pragma unroll
-        for (int r = 0; r < RG; r++) acc[r] += u * xs[m][r];
+        for (int r = 0; r < R; r++) acc[r] += u * xs[m][r];
       }
-      for (int r = 0; r < nr; r++) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        if (r < nr) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
     }
     __syncthreads();
   }
@@ -149,12 +167,12 @@ constexpr int GEMV_ROWS = 64, GEMV_K = 256;
 
 // W[0:p] -= F12 W[p:dim] for a (64-row, 256-column) block of F12 per CTA;
 // column blocks of one front add into W with atomics.
-template <typename T>
+template <typename T, int R>
 __global__ void __launch_bounds__(256)
     k_gemv_q(const SweepTask* __restrict__ tasks,
              const FrontDev* __restrict__ fr, const T* __restrict__ F,
              int nrhs, T* __restrict__ W) {
-  __shared__ T red[4][GEMV_ROWS][RG + 1];
+  __shared__ T red[4][GEMV_ROWS][R + 1];
   const SweepTask t = tasks[blockIdx.x];
   const FrontDev f = fr[t.front];
   const int dim = f.p + f.q;
@@ -162,21 +180,21 @@ __global__ void __launch_bounds__(256)
   const int kc0 = t.kchunk * GEMV_K, kc1 = min(f.q, kc0 + GEMV_K);
   T* Wf = W + f.w_off * nrhs;
   const T* a = F + f.off + i + (int64_t)f.p * f.ld;
-  for (int r0 = 0; r0 < nrhs; r0 += RG) {
-    const int nr = min(RG, nrhs - r0);
-    T acc[RG];
+  for (int r0 = 0; r0 < nrhs; r0 += R) {
+    const int nr = min(R, nrhs - r0);
+    T acc[R];
 #pragma unroll
-    for (int r = 0; r < RG; r++) acc[r] = (T)0;
+    for (int r = 0; r < R; r++) acc[r] = (T)0;
     if (i < f.p) {
       for (int k = kc0 + g; k < kc1; k += 4) {
         const T av = a[(int64_t)k * f.ld];
 #pragma unroll
-        for (int r = 0; r < RG; r++)
+        for (int r = 0; r < R; r++)
           if (r < nr) acc[r] += av * Wf[f.p + k + (int64_t)(r0 + r) * dim];
       }
     }
 #pragma unroll
-    for (int r = 0; r < RG; r++) red[g][threadIdx.x & 63][r] = acc[r];
+    for (int r = 0; r < R; r++) red[g][threadIdx.x & 63][r] = acc[r];
     __syncthreads();
     if (g == 0 && i < f.p) {
       for (int r = 0; r < nr; r++) {

@@ -185,4 +185,8 @@ def config(name):
         n = len(rp) - 1
         B = np.asfortranarray(rng.uniform(-1.0, 1.0, size=(16, n)).T)
         return rp, ci, v, B
+    if name.startswith("convdiff") and name[8:].isdigit():
+        m = int(name[8:])
+        rp, ci, v = convdiff3d(m)
+        return rp, ci, v, rhs(len(rp) - 1, 4, seed=2)
     raise KeyError(name)

@@ -160,10 +160,26 @@ def test_fp32_ir_reaches_tolerance(gpu):
     x = s.solve(B[:, 0])
     st = s.stats()
     assert st["backward_error"] <= 1e-10
+    # FP32 factors accurate to FP32 level: refinement converges in a few
+    # steps and never needs the FP64 fallback
+    assert st["fp64_fallback"] == 0 and st["ir_iters"] <= 3, st
     assert rel_resid(rp, ci, v, x, B[:, 0]) <= 1e-10
     ref = snu.Solver(nleaves=8).construct(rp, ci, v).factorize().solve(B[:, 0])
     fwd = np.abs(x - ref).max() / np.abs(ref).max()
     assert fwd <= 1e-8, fwd
+
+
+def test_fp32_ir_3d(gpu):
+    # 3D fronts are large enough for the tensor-core GEMM path
+    rp, ci, v = generators.convdiff3d(24)
+    n = len(rp) - 1
+    B = generators.rhs(n, 2, seed=9)
+    s = snu.Solver(nleaves=8, precision=snu.FP32_IR).construct(rp, ci, v)
+    X = s.factorize().solve(B)
+    st = s.stats()
+    assert st["fp64_fallback"] == 0 and st["ir_iters"] <= 3, st
+    for r in range(2):
+        assert rel_resid(rp, ci, v, X[:, r], B[:, r]) <= 1e-10
 
 
 def test_solve_device_pointers(gpu):
