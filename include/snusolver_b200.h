@@ -117,6 +117,25 @@ SNU_API snu_status snu_solve_device(snu_handle* h, const double* dB,
                                     void* stream);
 SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st);
 
+/* No counterpart in the reference.  snu_solve_device for callers that must
+   not allocate device memory: code running while a stream is being captured
+   into a CUDA graph, or a process whose memory manager owns the whole device
+   and forbids cudaMalloc (cudaMalloc may also synchronize the device, which
+   a latency-bound caller cannot accept).  Same arguments and results as
+   snu_solve_device, on a handle that has already been factorized; dX must
+   not alias dB.  The work vectors live in one static device array of 32 MiB
+   that every GPU loading this library holds until exit; a matrix / nrhs whose
+   work vectors do not fit is refused with SNU_EINVAL (snu_last_error gives
+   the size needed).  All calls share that array, so calls whose GPU work
+   overlaps (other streams, other threads, other handles) race.  The first
+   call on a device looks up the array's device address; make that first
+   call before capturing a stream.  The call returns after the solve has
+   finished on the stream.  With SNU_FP32_IR, refinement that would need the
+   FP64 fallback (which allocates) returns SNU_ENOTCONV instead. */
+SNU_API snu_status snu_solve_device_noalloc(snu_handle* h, const double* dB,
+                                            double* dX, int nrhs, int ldb,
+                                            void* stream);
+
 /* ---- execution control and measurement (no reference counterpart) ---- */
 /* All device work of the handle goes to this cudaStream_t (NULL: the
    handle's own stream).  Takes effect now, or at snu_construct. */

@@ -254,6 +254,25 @@ SNU_API snu_status snu_solve_device(snu_handle* h, const double* dB,
   return SNU_OK;
 }
 
+SNU_API snu_status snu_solve_device_noalloc(snu_handle* h, const double* dB,
+                                            double* dX, int nrhs, int ldb,
+                                            void* stream) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 3) return fail(h, SNU_ESTATE, "solve before factorize");
+  if (!dB || !dX || nrhs <= 0 || ldb < h->S.n)
+    return fail(h, SNU_EINVAL, "bad right-hand side arguments");
+  if (dB == dX) return fail(h, SNU_EINVAL, "dX must not alias dB");
+  snu::SolveReport rep;
+  int prec = h->opts.precision == SNU_FP64 ? 0 : 1;
+  int rc = h->eng->solve_noalloc(dB, dX, nrhs, ldb, stream, prec, &rep);
+  if (rc && rc != snu::ENG_ENOTCONV) return from_engine(h, rc);
+  h->stats.solve_s = rep.seconds;
+  h->stats.ir_iters = rep.ir_iters;
+  h->stats.backward_error = rep.backward_error;
+  if (rc == snu::ENG_ENOTCONV) return from_engine(h, rc);
+  return SNU_OK;
+}
+
 SNU_API snu_status snu_solve(snu_handle* h, const double* B, double* X,
                              int nrhs, int ldb) {
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");

@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "../engine.h"
@@ -17,6 +18,37 @@
 #include "gemm_tc.cuh"
 
 namespace snu {
+
+// Work space of snu_solve_device_noalloc: a fixed device array that every GPU
+// loading this library holds until the process exits, so callers that may
+// not allocate device memory can still solve.  All such calls share it; its
+// contents are whatever the last call left (every call rewrites all of the
+// part it reads before reading it).  Calls that overlap on the GPU race.
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)32 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch on the current device; looked up once
+// per device (the host-side symbol is not a device address).
+static int noalloc_scratch(int device, unsigned char** out, std::string& err) {
+  static std::mutex mu;
+  static unsigned char* addr[256] = {};
+  if (device < 0 || device >= 256) {
+    err = "device ordinal out of range";
+    return 1;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+      return 1;
+    }
+    addr[device] = (unsigned char*)p;
+  }
+  *out = addr[device];
+  return 0;
+}
 
 namespace {
 
@@ -977,6 +1009,111 @@ class CudaEngine : public Engine {
     }
     *out = worst;
     return ENG_OK;
+  }
+
+  // ---------------------------------------------- no-allocation solve
+  // The solve of solve() with W, Y (and R, D for refinement) carved from
+  // g_noalloc_scratch.  Nothing is allocated: work vectors that do not fit
+  // are refused, and FP32 refinement that would need the FP64 fallback
+  // (which allocates FP64 factors) stops with ENG_ENOTCONV instead.
+  int solve_noalloc(const double* dB, double* dX, int nrhs, int ldb,
+                    void* stream, int precision, SolveReport* rep) override {
+    CK(cudaSetDevice(opt_.device));
+    if (nrhs <= 0 || ldb < n_) {
+      err_ = "bad nrhs or ldb";
+      return ENG_EINVAL;
+    }
+    if ((precision == 0 && !have64_) || (precision == 1 && !have32_)) {
+      err_ = "solve before factorize";
+      return ENG_ESTATE;
+    }
+    const size_t es = precision == 0 ? sizeof(double) : sizeof(float);
+    auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t bw = up((size_t)wtot_ * nrhs * es), by = up((size_t)ytot_ * nrhs * es);
+    const size_t br = up((size_t)n_ * nrhs * sizeof(double));
+    const size_t need = bw + by + (precision == 0 ? br : 2 * br);
+    if (need > NOALLOC_SCRATCH_BYTES) {
+      err_ = "the no-allocation solve needs " + std::to_string(need) +
+             " bytes of work space for this matrix and nrhs; its static "
+             "device array holds " + std::to_string(NOALLOC_SCRATCH_BYTES);
+      return ENG_EINVAL;
+    }
+    unsigned char* base = nullptr;
+    std::string e2;
+    if (noalloc_scratch(opt_.device, &base, e2)) {
+      err_ = e2;
+      return ENG_ECUDA;
+    }
+    unsigned char* pW = base;
+    unsigned char* pY = base + bw;
+    double* R = (double*)(base + bw + by);
+    double* D = (double*)(base + bw + by + br);
+    cudaStream_t st = stream ? (cudaStream_t)stream : stream_;
+    const unsigned saved_mask = prof_mask_;
+    prof_mask_ = 0;  // no profiling events on this path
+    SolveReport r;
+    int rc = ENG_OK;
+    std::vector<double> bn, rn, xn;
+    auto berr = [&](const double* X) -> int {
+      int q;
+      k_residual<<<(n_ + 255) / 256, 256, 0, st>>>(n_, d_rowptr_, d_colidx_,
+                                                   d_vals_, dB, ldb, X, ldb,
+                                                   nrhs, R, n_);
+      CKL();
+      if ((q = colmax(R, n_, nrhs, st, rn))) return q;
+      if ((q = colmax(X, ldb, nrhs, st, xn))) return q;
+      double worst = 0;
+      for (size_t c = 0; c < rn.size(); c++) {
+        double den = anorm_ * xn[c] + bn[c];
+        double be = den > 0 ? rn[c] / den : rn[c];
+        if (!(be == be)) be = INFINITY;
+        worst = std::max(worst, be);
+      }
+      r.backward_error = worst;
+      return ENG_OK;
+    };
+    do {
+      if ((rc = colmax(dB, ldb, nrhs, st, bn))) break;
+      if (precision == 0) {
+        if ((rc = tree_solve<double>(d_F64_, d_I64_, (double*)pW, (double*)pY,
+                                     dB, ldb, dX, ldb, nrhs, st)))
+          break;
+        rc = berr(dX);
+        break;
+      }
+      float* W = (float*)pW;
+      float* Y = (float*)pY;
+      if ((rc = tree_solve<float>(d_F32_, d_I32_, W, Y, dB, ldb, dX, ldb, nrhs,
+                                  st)))
+        break;
+      double prev = INFINITY;
+      int it = 0, stagnant = 0;
+      const int blocks = (n_ * nrhs + 255) / 256;
+      for (;;) {
+        if ((rc = berr(dX))) break;
+        if (r.backward_error <= opt_.ir_tol) break;
+        if (it >= opt_.ir_max_iter || stagnant >= 2) {
+          rc = ENG_ENOTCONV;
+          err_ = "refinement stalled; the no-allocation solve has no FP64 "
+                 "fallback";
+          break;
+        }
+        stagnant = r.backward_error > 0.5 * prev ? stagnant + 1 : 0;
+        prev = r.backward_error;
+        if ((rc = tree_solve<float>(d_F32_, d_I32_, W, Y, R, n_, D, n_, nrhs,
+                                    st)))
+          break;
+        k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, D, n_, dX, ldb);
+        CKL();
+        it++;
+      }
+      r.ir_iters = it;
+    } while (0);
+    prof_mask_ = saved_mask;
+    if (rc && rc != ENG_ENOTCONV) return rc;
+    CK(cudaStreamSynchronize(st));
+    if (rep) *rep = r;
+    return rc;
   }
 
   // FP32 factors + FP64 residual refinement; FP64 factorization on

@@ -83,6 +83,10 @@ class Engine {
   // and a dense separator block LU[{i, j}].
   virtual int leaf_factor(const Structure& s, int rank, double* out) = 0;
   virtual int dense_block(const Structure& s, int i, int j, double* out) = 0;
+  // The same solve with its work vectors in a fixed static device array
+  // instead of memory the handle allocates (snu_solve_device_noalloc).
+  virtual int solve_noalloc(const double* dB, double* dX, int nrhs, int ldb,
+                            void* stream, int precision, SolveReport* rep) = 0;
   virtual int64_t device_bytes() const = 0;
   virtual int tiny_pivots() const = 0;
   virtual const std::string& error() const = 0;
