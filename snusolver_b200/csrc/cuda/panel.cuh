@@ -17,11 +17,13 @@ constexpr int TLD = NB + 1;
 __device__ __forceinline__ float recip_rn(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double recip_rn(double x) { return __drcp_rn(x); }
 
-// Dynamic shared memory of k_diag_lu_inv: the factored tile.
+// Dynamic shared memory of k_diag_lu_inv: the tile and its two inverses.
 template <typename T>
 constexpr size_t diag_smem() {
-  return (size_t)NB * TLD * sizeof(T);
+  return 3 * (size_t)NB * TLD * sizeof(T);
 }
+
+constexpr int SB = 16;  // sub-block of the blocked tile factorization
 
 // LU without pivoting of the diagonal tile at (k0, k0) of every active front
 // and the inverses of its triangles, written to INV + inv_off + step*2*NB*NB
@@ -31,12 +33,14 @@ constexpr size_t diag_smem() {
 // array (kernel_cuda.cu:45-73).  flags[0] counts replaced pivots, flags[1]
 // records a zero or non-finite pivot.
 //
-// Each of the 256 threads keeps a 4 x 4 strided block of the tile in
-// registers (rows tx + 16a, columns ty + 16b).  Step k reads the pivot row
-// and column from a double-buffered shared copy that their owners refresh
-// right after their own update, so every elimination step (and every
-// inverse step) costs one barrier.  A tile smaller than NB is padded with
-// the identity, which leaves its factors and inverses unchanged.
+// Blocked in SB x SB sub-blocks: one warp factors each diagonal sub-block in
+// registers (row k broadcast by shuffles), the rows below and columns right
+// of it inside the tile are finished by substitution (one thread per row /
+// column), and the rest of the tile takes a rank-SB update.  The inverses
+// start from the SB x SB diagonal-block inverses (eight warps at once) and
+// fill the off-diagonal blocks by distance from the diagonal.  A tile
+// smaller than NB is padded with the identity, which leaves its factors and
+// inverses unchanged.
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_diag_lu_inv(const int* __restrict__ active,
@@ -44,184 +48,193 @@ __global__ void __launch_bounds__(256)
                   T* __restrict__ INV, int k0, int step, double eps,
                   int* flags) {
   extern __shared__ unsigned char smem_raw[];
-  T* LU = reinterpret_cast<T*>(smem_raw);
-  __shared__ T rowb[2][NB], colb[2][NB];
+  T* D = reinterpret_cast<T*>(smem_raw);
+  T* XL = D + NB * TLD;
+  T* XU = XL + NB * TLD;
+  __shared__ T rdiag[NB];  // 1 / U[i][i]
+  __shared__ T Tb[6][SB][SB + 1];
   const FrontDev f = fr[active[blockIdx.x]];
   const int kb = min(NB, f.p - k0);
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   T* base = F + f.off + k0 + (int64_t)k0 * f.ld;
-  T a[4][4];
-#pragma unroll
-  for (int ia = 0; ia < 4; ia++)
-#pragma unroll
-    for (int jb = 0; jb < 4; jb++) {
-      int i = tx + 16 * ia, j = ty + 16 * jb;
-      a[ia][jb] = (i < kb && j < kb) ? base[i + (int64_t)j * f.ld]
-                                     : (i == j ? (T)1 : (T)0);
-    }
-  // publish row 0 and column 0
-  if (tx == 0)
-#pragma unroll
-    for (int jb = 0; jb < 4; jb++) rowb[0][ty + 16 * jb] = a[0][jb];
-  if (ty == 0)
-#pragma unroll
-    for (int ia = 0; ia < 4; ia++) colb[0][tx + 16 * ia] = a[ia][0];
+  for (int e = tid; e < NB * NB; e += 256) {
+    const int i = e & (NB - 1), j = e / NB;
+    D[i + j * TLD] = (i < kb && j < kb) ? base[i + (int64_t)j * f.ld]
+                                        : (i == j ? (T)1 : (T)0);
+    XL[i + j * TLD] = (T)0;
+    XU[i + j * TLD] = (T)0;
+  }
   __syncthreads();
   const T teps = (T)eps;
-  for (int k = 0; k < NB; k++) {
-    const int cb = k & 1, nb = cb ^ 1;
-    T piv = rowb[cb][k];
-    bool guarded = false;
-    if (k < kb && f.guard && piv < teps && piv > -teps) {
-      piv = piv < (T)0 ? -teps : teps;
-      guarded = true;
-    }
-    const T rp = recip_rn(piv);
-    T li[4], rj[4];
+  for (int b = 0; b < NB / SB; b++) {
+    const int s0 = b * SB;
+    // (1) diagonal sub-block by warp 0; lane l (< SB) owns row s0 + l
+    if (warp == 0) {
+      const int r = s0 + (lane & (SB - 1));
+      T v[SB];
 #pragma unroll
-    for (int ia = 0; ia < 4; ia++) {
-      const int i = tx + 16 * ia;
-      li[ia] = i > k ? colb[cb][i] * rp : (T)0;
-    }
+      for (int j = 0; j < SB; j++) v[j] = D[r + (s0 + j) * TLD];
 #pragma unroll
-    for (int jb = 0; jb < 4; jb++) {
-      const int j = ty + 16 * jb;
-      rj[jb] = j > k ? rowb[cb][j] : (T)0;
-    }
+      for (int k = 0; k < SB; k++) {
+        T rowk[SB];
 #pragma unroll
-    for (int ia = 0; ia < 4; ia++)
-#pragma unroll
-      for (int jb = 0; jb < 4; jb++) a[ia][jb] -= li[ia] * rj[jb];
-    // column k keeps the multipliers, (k, k) the (guarded) pivot
-#pragma unroll
-    for (int jb = 0; jb < 4; jb++)
-      if (ty + 16 * jb == k)
-#pragma unroll
-        for (int ia = 0; ia < 4; ia++) {
-          const int i = tx + 16 * ia;
-          if (i > k) a[ia][jb] = li[ia];
-          if (i == k) a[ia][jb] = piv;
+        for (int j = k; j < SB; j++) rowk[j] = __shfl_sync(0xffffffffu, v[j], k);
+        T piv = rowk[k];
+        bool guarded = false;
+        if (f.guard && s0 + k < kb && piv < teps && piv > -teps) {
+          piv = piv < (T)0 ? -teps : teps;
+          guarded = true;
         }
-    if (k < kb && tx == (k & 15) && ty == (k & 15)) {
-      if (guarded) atomicAdd(flags, 1);
-      if (!(piv != (T)0) || !isfinite((double)piv)) flags[1] = 1;
-    }
-    if (k + 1 < NB) {
-      const int r = k + 1;
+        const T rp = recip_rn(piv);
+        if (lane == k) v[k] = piv;
+        if (lane > k && lane < SB) {
+          const T l = v[k] * rp;
+          v[k] = l;
 #pragma unroll
-      for (int ia = 0; ia < 4; ia++)
-        if (tx + 16 * ia == r)
-#pragma unroll
-          for (int jb = 0; jb < 4; jb++) rowb[nb][ty + 16 * jb] = a[ia][jb];
-#pragma unroll
-      for (int jb = 0; jb < 4; jb++)
-        if (ty + 16 * jb == r)
-#pragma unroll
-          for (int ia = 0; ia < 4; ia++) colb[nb][tx + 16 * ia] = a[ia][jb];
-    }
-    __syncthreads();
-  }
-  // factored tile to the front and to shared memory (columns of L and U
-  // for the inverses)
-#pragma unroll
-  for (int ia = 0; ia < 4; ia++)
-#pragma unroll
-    for (int jb = 0; jb < 4; jb++) {
-      const int i = tx + 16 * ia, j = ty + 16 * jb;
-      LU[i + j * TLD] = a[ia][jb];
-      if (i < kb && j < kb) base[i + (int64_t)j * f.ld] = a[ia][jb];
-    }
-  __syncthreads();
-  T* inv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
-  // Linv: rows top-down, X[i,:] -= L[i,k] X[k,:] once row k is final.
-  {
-    T x[4][4];
-#pragma unroll
-    for (int ia = 0; ia < 4; ia++)
-#pragma unroll
-      for (int jb = 0; jb < 4; jb++)
-        x[ia][jb] = (tx + 16 * ia == ty + 16 * jb) ? (T)1 : (T)0;
-    if (tx == 0)
-#pragma unroll
-      for (int jb = 0; jb < 4; jb++) rowb[0][ty + 16 * jb] = x[0][jb];
-    __syncthreads();
-    for (int k = 0; k < NB; k++) {
-      const int cb = k & 1, nb = cb ^ 1;
-      T rv[4];
-#pragma unroll
-      for (int jb = 0; jb < 4; jb++) rv[jb] = rowb[cb][ty + 16 * jb];
-#pragma unroll
-      for (int ia = 0; ia < 4; ia++) {
-        const int i = tx + 16 * ia;
-        const T lk = i > k ? LU[i + k * TLD] : (T)0;
-#pragma unroll
-        for (int jb = 0; jb < 4; jb++) x[ia][jb] -= lk * rv[jb];
-      }
-      const int r = k + 1;
-#pragma unroll
-      for (int ia = 0; ia < 4; ia++)
-        if (tx + 16 * ia == r)
-#pragma unroll
-          for (int jb = 0; jb < 4; jb++) rowb[nb][ty + 16 * jb] = x[ia][jb];
-      __syncthreads();
-    }
-#pragma unroll
-    for (int ia = 0; ia < 4; ia++)
-#pragma unroll
-      for (int jb = 0; jb < 4; jb++)
-        inv[tx + 16 * ia + (ty + 16 * jb) * NB] = x[ia][jb];
-  }
-  // Uinv: rows bottom-up, Y[ku,:] /= U[ku,ku], then Y[i,:] -= U[i,ku] Y[ku,:].
-  {
-    T y[4][4];
-#pragma unroll
-    for (int ia = 0; ia < 4; ia++)
-#pragma unroll
-      for (int jb = 0; jb < 4; jb++)
-        y[ia][jb] = (tx + 16 * ia == ty + 16 * jb) ? (T)1 : (T)0;
-    {
-      const T rd = recip_rn(LU[(NB - 1) + (NB - 1) * TLD]);
-#pragma unroll
-      for (int ia = 0; ia < 4; ia++)
-        if (tx + 16 * ia == NB - 1)
-#pragma unroll
-          for (int jb = 0; jb < 4; jb++) {
-            y[ia][jb] *= rd;
-            colb[0][ty + 16 * jb] = y[ia][jb];
+          for (int j = k + 1; j < SB; j++) v[j] -= l * rowk[j];
+        }
+        if (lane == 0) {
+          rdiag[s0 + k] = rp;
+          if (s0 + k < kb) {
+            if (guarded) atomicAdd(flags, 1);
+            if (!(piv != (T)0) || !isfinite((double)piv)) flags[1] = 1;
           }
+        }
+      }
+      if (lane < SB)
+#pragma unroll
+        for (int j = 0; j < SB; j++) D[r + (s0 + j) * TLD] = v[j];
     }
     __syncthreads();
-    for (int k = 0; k < NB; k++) {
-      const int cb = k & 1, nb = cb ^ 1, ku = NB - 1 - k;
-      T cv[4];
+    const int rem = NB - s0 - SB;
+    if (rem > 0) {
+      // (2) rows below: x Ubb = a; columns right: Lbb y = a (unit lower)
+      if (tid < rem) {
+        const int i = s0 + SB + tid;
+        T x[SB];
 #pragma unroll
-      for (int jb = 0; jb < 4; jb++) cv[jb] = colb[cb][ty + 16 * jb];
+        for (int j = 0; j < SB; j++) {
+          T a = D[i + (s0 + j) * TLD];
 #pragma unroll
-      for (int ia = 0; ia < 4; ia++) {
-        const int i = tx + 16 * ia;
-        const T uk = i < ku ? LU[i + ku * TLD] : (T)0;
+          for (int m = 0; m < j; m++) a -= x[m] * D[s0 + m + (s0 + j) * TLD];
+          x[j] = a * rdiag[s0 + j];
+        }
 #pragma unroll
-        for (int jb = 0; jb < 4; jb++) y[ia][jb] -= uk * cv[jb];
+        for (int j = 0; j < SB; j++) D[i + (s0 + j) * TLD] = x[j];
+      } else if (tid >= 128 && tid < 128 + rem) {
+        const int c = s0 + SB + (tid - 128);
+        T y[SB];
+#pragma unroll
+        for (int i = 0; i < SB; i++) {
+          T a = D[s0 + i + c * TLD];
+#pragma unroll
+          for (int m = 0; m < i; m++) a -= D[s0 + i + (s0 + m) * TLD] * y[m];
+          y[i] = a;
+        }
+#pragma unroll
+        for (int i = 0; i < SB; i++) D[s0 + i + c * TLD] = y[i];
       }
-      const int ru = ku - 1;
-      if (ru >= 0 && tx == (ru & 15)) {
-        const T rd = recip_rn(LU[ru + ru * TLD]);
+      __syncthreads();
+      // (3) rank-SB update of the rest of the tile
+      const int tx = tid & 15, ty = tid >> 4;
+      for (int jj = ty; jj < rem; jj += 16) {
+        const int j = s0 + SB + jj;
+        T u[SB];
 #pragma unroll
-        for (int ia = 0; ia < 4; ia++)
-          if (tx + 16 * ia == ru)
+        for (int t = 0; t < SB; t++) u[t] = D[s0 + t + j * TLD];
+        for (int ii = tx; ii < rem; ii += 16) {
+          const int i = s0 + SB + ii;
+          T acc = D[i + j * TLD];
 #pragma unroll
-            for (int jb = 0; jb < 4; jb++) {
-              y[ia][jb] *= rd;
-              colb[nb][ty + 16 * jb] = y[ia][jb];
-            }
+          for (int t = 0; t < SB; t++) acc -= D[i + (s0 + t) * TLD] * u[t];
+          D[i + j * TLD] = acc;
+        }
       }
       __syncthreads();
     }
+  }
+  // factored tile back to the front
+  for (int e = tid; e < NB * NB; e += 256) {
+    const int i = e & (NB - 1), j = e / NB;
+    if (i < kb && j < kb) base[i + (int64_t)j * f.ld] = D[i + j * TLD];
+  }
+  // inverses, stage A: SB x SB diagonal blocks; warps 0-3 Linv, 4-7 Uinv;
+  // lane j (< SB) computes column j of its block
+  {
+    const int s0 = (warp & 3) * SB, j = lane;
+    if (j < SB) {
+      T x[SB];
+      if (warp < 4) {
 #pragma unroll
-    for (int ia = 0; ia < 4; ia++)
+        for (int i = 0; i < SB; i++) {
+          T a = (i == j) ? (T)1 : (T)0;
 #pragma unroll
-      for (int jb = 0; jb < 4; jb++)
-        inv[NB * NB + tx + 16 * ia + (ty + 16 * jb) * NB] = y[ia][jb];
+          for (int m = 0; m < i; m++) a -= D[s0 + i + (s0 + m) * TLD] * x[m];
+          x[i] = a;
+        }
+#pragma unroll
+        for (int i = 0; i < SB; i++) XL[s0 + i + (s0 + j) * TLD] = x[i];
+      } else {
+#pragma unroll
+        for (int ii = SB - 1; ii >= 0; ii--) {
+          T a = (ii == j) ? (T)1 : (T)0;
+#pragma unroll
+          for (int m = ii + 1; m < SB; m++) a -= D[s0 + ii + (s0 + m) * TLD] * x[m];
+          x[ii] = a * rdiag[s0 + ii];
+        }
+#pragma unroll
+        for (int i = 0; i < SB; i++) XU[s0 + i + (s0 + j) * TLD] = x[i];
+      }
+    }
+  }
+  __syncthreads();
+  // stage B: off-diagonal blocks by distance d from the diagonal
+  //   Linv(b2,b1) = -Linv(b2,b2) * sum_{m=b1}^{b2-1} L(b2,m) Linv(m,b1)
+  //   Uinv(b1,b2) = -Uinv(b1,b1) * sum_{m=b1+1}^{b2} U(b1,m) Uinv(m,b2)
+  const int ei = tid & 15, ej = tid >> 4;
+  for (int d = 1; d < NB / SB; d++) {
+    const int nt = NB / SB - d;  // blocks at distance d, per triangle
+    for (int t = 0; t < 2 * nt; t++) {
+      const bool low = t < nt;
+      const int b1 = low ? t : t - nt, b2 = b1 + d;
+      T acc = (T)0;
+      if (low) {
+        const int r = b2 * SB + ei, c = b1 * SB + ej;
+        for (int m = b1 * SB; m < b2 * SB; m++)
+          acc += D[r + m * TLD] * XL[m + c * TLD];
+      } else {
+        const int r = b1 * SB + ei, c = b2 * SB + ej;
+        for (int m = (b1 + 1) * SB; m < (b2 + 1) * SB; m++)
+          acc += D[r + m * TLD] * XU[m + c * TLD];
+      }
+      Tb[t][ei][ej] = acc;
+    }
+    __syncthreads();
+    for (int t = 0; t < 2 * nt; t++) {
+      const bool low = t < nt;
+      const int b1 = low ? t : t - nt, b2 = b1 + d;
+      T acc = (T)0;
+      if (low) {
+        const int r = b2 * SB + ei;
+#pragma unroll
+        for (int m = 0; m < SB; m++)
+          acc -= XL[r + (b2 * SB + m) * TLD] * Tb[t][m][ej];
+        XL[r + (b1 * SB + ej) * TLD] = acc;
+      } else {
+        const int r = b1 * SB + ei;
+#pragma unroll
+        for (int m = 0; m < SB; m++)
+          acc -= XU[r + (b1 * SB + m) * TLD] * Tb[t][m][ej];
+        XU[r + (b2 * SB + ej) * TLD] = acc;
+      }
+    }
+    __syncthreads();
+  }
+  T* inv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
+  for (int e = tid; e < NB * NB; e += 256) {
+    const int i = e & (NB - 1), j = e / NB;
+    inv[e] = XL[i + j * TLD];
+    inv[NB * NB + e] = XU[i + j * TLD];
   }
 }
 

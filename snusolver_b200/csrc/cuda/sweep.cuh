@@ -54,9 +54,9 @@ __global__ void __launch_bounds__(256)
     for (int e = tid; e < NB * R; e += blockDim.x) {
       int i = e % NB, r = e / NB;
       T s = (T)0;
-      if (i < kb && r < nr)
-        for (int m = 0; m <= i; m++) s += X[i + m * (NB + 1)] * ws[m][r];
-      ys[i][r] = s;
+#pragma unroll 16
+      for (int m = 0; m < NB; m++) s += X[i + m * (NB + 1)] * ws[m][r];
+      ys[i][r] = (i < kb && r < nr) ? s : (T)0;
     }
     __syncthreads();
     if (t.chunk == 0)
@@ -68,10 +68,15 @@ __global__ void __launch_bounds__(256)
       T acc[R];
 #pragma unroll
       for (int r = 0; r < R; r++) acc[r] = (T)0;
-      for (int m = 0; m < kb; m++) {
-        const T l = lrow[(int64_t)m * f.ld];
+      for (int m0 = 0; m0 < kb; m0 += 16) {
+        T lv[16];
 #pragma unroll
-        for (int r = 0; r < R; r++) acc[r] += l * ys[m][r];
+        for (int u = 0; u < 16; u++)
+          lv[u] = m0 + u < kb ? lrow[(int64_t)(m0 + u) * f.ld] : (T)0;
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+#pragma unroll
+          for (int r = 0; r < R; r++) acc[r] += lv[u] * ys[m0 + u][r];
       }
 #pragma unroll
       for (int r = 0; r < R; r++)
@@ -114,9 +119,9 @@ __global__ void __launch_bounds__(256)
     for (int e = tid; e < NB * R; e += blockDim.x) {
       int i = e % NB, r = e / NB;
       T s = (T)0;
-      if (i < kb && r < nr)
-        for (int m = i; m < kb; m++) s += X[i + m * (NB + 1)] * ws[m][r];
-      xs[i][r] = s;
+#pragma unroll 16
+      for (int m = 0; m < NB; m++) s += X[i + m * (NB + 1)] * ws[m][r];
+      xs[i][r] = (i < kb && r < nr) ? s : (T)0;
     }
     __syncthreads();
     if (t.chunk == 0)
@@ -128,10 +133,15 @@ __global__ void __launch_bounds__(256)
       T acc[R];
 #pragma unroll
       for (int r = 0; r < R; r++) acc[r] = (T)0;
-      for (int m = 0; m < kb; m++) {
-        const T u = urow[(int64_t)m * f.ld];
+      for (int m0 = 0; m0 < kb; m0 += 16) {
+        T uv[16];
 #pragma unroll
-        for (int r = 0; r < R; r++) acc[r] += u * xs[m][r];
+        for (int u = 0; u < 16; u++)
+          uv[u] = m0 + u < kb ? urow[(int64_t)(m0 + u) * f.ld] : (T)0;
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+#pragma unroll
+          for (int r = 0; r < R; r++) acc[r] += uv[u] * xs[m0 + u][r];
       }
 #pragma unroll
       for (int r = 0; r < R; r++)
@@ -186,11 +196,22 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int r = 0; r < R; r++) acc[r] = (T)0;
     if (i < f.p) {
-      for (int k = kc0 + g; k < kc1; k += 4) {
-        const T av = a[(int64_t)k * f.ld];
+      constexpr int UB = R <= 4 ? 8 : (R <= 8 ? 4 : 2);  // loads in flight
+      for (int k0 = kc0 + g; k0 < kc1; k0 += 4 * UB) {
+        T av[UB], wv[UB][R];
 #pragma unroll
-        for (int r = 0; r < R; r++)
-          if (r < nr) acc[r] += av * Wf[f.p + k + (int64_t)(r0 + r) * dim];
+        for (int u = 0; u < UB; u++) {
+          const int k = k0 + 4 * u;
+          av[u] = k < kc1 ? a[(int64_t)k * f.ld] : (T)0;
+#pragma unroll
+          for (int r = 0; r < R; r++)
+            wv[u][r] = (k < kc1 && r < nr) ? Wf[f.p + k + (int64_t)(r0 + r) * dim]
+                                           : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < UB; u++)
+#pragma unroll
+          for (int r = 0; r < R; r++) acc[r] += av[u] * wv[u][r];
       }
     }
 #pragma unroll
