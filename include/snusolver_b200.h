@@ -155,6 +155,19 @@ SNU_API snu_status snu_get_profile(const snu_handle* h, snu_kernel_stat* out,
                                    int max, int* count);
 SNU_API snu_status snu_reset_profile(snu_handle* h);
 
+/* Launch trace: with SNU_PROFILE_TRACE also set in the profiling mask, every
+   timed launch is kept in order (up to 1M records; snu_reset_profile clears
+   them).  level is the elimination-tree level the launch worked on (-1 for
+   work over the whole matrix). */
+#define SNU_PROFILE_TRACE 0x80000000u
+typedef struct snu_launch_rec {
+  int family;         /* index into the snu_get_profile list */
+  int level;
+  double seconds, flops, bytes;
+} snu_launch_rec;
+SNU_API snu_status snu_get_trace(const snu_handle* h, snu_launch_rec* out,
+                                 int max, int* count);
+
 /* ---- parity read-back in the reference's layouts (host arrays) ---- */
 /* order[n] (order[old] = new) and sizes[2*nleaves-1]. */
 SNU_API snu_status snu_get_ordering(const snu_handle* h, int* order,

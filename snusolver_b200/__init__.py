@@ -69,6 +69,12 @@ class _KStat(C.Structure):
                 ("bytes", C.c_double)]
 
 
+class _LaunchRec(C.Structure):
+    _fields_ = [("family", C.c_int), ("level", C.c_int),
+                ("seconds", C.c_double), ("flops", C.c_double),
+                ("bytes", C.c_double)]
+
+
 KERNEL_FAMILIES = ("assemble", "extend_add", "diag_lu", "panel_trsm",
                    "gemm_trail", "gemm_schur", "solve_diag", "solve_gemm",
                    "solve_misc", "residual")
@@ -102,6 +108,8 @@ _EXPORTS = {
     "snu_free": (None, [C.c_void_p]),
     "snu_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "snu_set_profiling": (C.c_int, [C.c_void_p, C.c_uint]),
+    "snu_get_trace": (C.c_int, [C.c_void_p, C.POINTER(_LaunchRec), C.c_int,
+                                C.POINTER(C.c_int)]),
     "snu_get_profile": (C.c_int, [C.c_void_p, C.POINTER(_KStat), C.c_int,
                                   C.POINTER(C.c_int)]),
     "snu_reset_profile": (C.c_int, [C.c_void_p]),
@@ -234,9 +242,10 @@ class Solver:
         self._check(self._lib.snu_set_stream(self._h, C.c_void_p(stream or None)))
         return self
 
-    def set_profiling(self, families=()):
-        """Per-launch CUDA-event timing for the named kernel families."""
-        mask = 0
+    def set_profiling(self, families=(), trace=False):
+        """Per-launch CUDA-event timing for the named kernel families;
+        ``trace`` also keeps every launch's record (see :meth:`trace`)."""
+        mask = 0x80000000 if trace else 0
         for f in families:
             mask |= 1 << KERNEL_FAMILIES.index(f)
         self._check(self._lib.snu_set_profiling(self._h, mask))
@@ -251,6 +260,17 @@ class Solver:
                                            flops=arr[i].flops,
                                            bytes=arr[i].bytes)
                 for i in range(cnt.value)}
+
+    def trace(self):
+        """Per-launch records (family, level, seconds, flops, bytes), in
+        launch order; recorded while profiling runs with ``trace=True``."""
+        cnt = C.c_int()
+        self._check(self._lib.snu_get_trace(self._h, None, 0, C.byref(cnt)))
+        arr = (_LaunchRec * max(cnt.value, 1))()
+        self._check(self._lib.snu_get_trace(self._h, arr, cnt.value,
+                                            C.byref(cnt)))
+        return [(KERNEL_FAMILIES[r.family], r.level, r.seconds, r.flops,
+                 r.bytes) for r in arr[:cnt.value]]
 
     def reset_profile(self):
         self._check(self._lib.snu_reset_profile(self._h))

@@ -343,6 +343,20 @@ SNU_API snu_status snu_get_profile(const snu_handle* h, snu_kernel_stat* out,
   return SNU_OK;
 }
 
+SNU_API snu_status snu_get_trace(const snu_handle* h, snu_launch_rec* out,
+                                 int max, int* count) {
+  if (!h || (!out && max > 0)) return fail(nullptr, SNU_EINVAL, "null argument");
+  int n = 0;
+  if (h->eng) {
+    const std::vector<snu::LaunchRec>& t = h->eng->trace();
+    n = (int)t.size();
+    for (int i = 0; i < std::min(max, n); i++)
+      out[i] = {t[i].family, t[i].level, t[i].seconds, t[i].flops, t[i].bytes};
+  }
+  if (count) *count = n;
+  return SNU_OK;
+}
+
 SNU_API snu_status snu_reset_profile(snu_handle* h) {
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
   if (h->eng) h->eng->reset_profile();

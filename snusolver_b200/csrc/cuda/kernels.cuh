@@ -163,7 +163,8 @@ __global__ void k_solve_init(const int* __restrict__ list,
 }
 
 // Update vectors of children (their Q rows after the forward sweep) are
-// added into the parent's work vector, in child-rank order.
+// added into the parent's work vector; all children of a level in one
+// launch, siblings meeting on a parent row add with atomics.
 template <typename T>
 __global__ void k_solve_ea(const int* __restrict__ list,
                            const FrontDev* __restrict__ fr,
@@ -177,7 +178,7 @@ __global__ void k_solve_ea(const int* __restrict__ list,
   const int* r = rel + c.rel_off;
   for (int e = threadIdx.x; e < c.q * nrhs; e += blockDim.x) {
     int i = e % c.q, k = e / c.q;
-    dst[r[i] + (int64_t)k * dimp] += src[c.p + i + (int64_t)k * dimc];
+    atomicAdd(dst + r[i] + (int64_t)k * dimp, src[c.p + i + (int64_t)k * dimc]);
   }
 }
 

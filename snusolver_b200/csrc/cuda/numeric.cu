@@ -118,8 +118,8 @@ struct LevelSched {
   int64_t asm0 = 0, asm1 = 0;
   std::vector<EaTask*> ea;  // per child rank
   std::vector<int> nea;
-  std::vector<int*> ea_children;  // per child rank (solve)
-  std::vector<int> nea_children;
+  int* ea_kids = nullptr;  // children of the level's fronts (solve)
+  int nea_kids = 0;
   int* list = nullptr;  // fronts of the level
   int* listq = nullptr; // fronts of the level with q > 0
   int nlistq = 0;
@@ -127,13 +127,18 @@ struct LevelSched {
   GemmBatch f22;
   std::vector<double> ea_elems;  // per child rank: update entries added
   double solve_elems = 0;        // sum of front dims (per right-hand side)
-  // solve sweeps: per tile step the (front, row chunk) tasks
-  std::vector<SweepTask*> fwd, bwd;
-  std::vector<int> nfwd, nbwd;
-  std::vector<double> fwd_elems, bwd_elems;  // factor entries read per step
-  SweepTask* gq = nullptr;  // (front, 64-row chunk, 256-column chunk) of F12
-  int ngq = 0;
-  double gq_elems = 0;
+  // solve sweeps: pivot-block (front, 128-row chunk) tasks, forward in
+  // ascending and backward in descending chunk order
+  SweepTask* wf = nullptr;
+  SweepTask* wb = nullptr;
+  int nwf = 0, nwb = 0;
+  double diag_elems = 0;  // factor entries of one triangle of the pivot blocks
+  // off-diagonal products: (front, 64-row chunk, 256-column chunk) of L21
+  // (forward) and of U12 (backward)
+  SweepTask* gl = nullptr;
+  SweepTask* gq = nullptr;
+  int ngl = 0, ngq = 0;
+  double gq_elems = 0;  // p * q summed over the level
 };
 
 
@@ -180,7 +185,9 @@ class CudaEngine : public Engine {
       int rc2;
       if ((rc2 = sweep_attr<double, 1>()) || (rc2 = sweep_attr<double, 2>()) ||
           (rc2 = sweep_attr<double, 4>()) || (rc2 = sweep_attr<double, 8>()) ||
-          (rc2 = sweep_attr<double, 16>()))
+          (rc2 = sweep_attr<double, 16>()) || (rc2 = sweep_attr<float, 1>()) ||
+          (rc2 = sweep_attr<float, 2>()) || (rc2 = sweep_attr<float, 4>()) ||
+          (rc2 = sweep_attr<float, 8>()) || (rc2 = sweep_attr<float, 16>()))
         return rc2;
     }
     CK(cudaFuncSetAttribute(k_panel_apply<double>,
@@ -206,7 +213,9 @@ class CudaEngine : public Engine {
   }
   void reset_profile() override {
     for (int f = 0; f < KF_COUNT; f++) kstat_[f] = KernelStat();
+    trace_.clear();
   }
+  const std::vector<LaunchRec>& trace() const override { return trace_; }
   int64_t device_bytes() const override { return bytes_; }
   int tiny_pivots() const override { return tiny_; }
 
@@ -247,6 +256,18 @@ class CudaEngine : public Engine {
     ytot_ = yoff;
     invtot_ = ioff;
     int rc;
+    {
+      // one flag per pivot tile of every front, for each sweep direction
+      std::vector<int64_t> fo(std::max(nfronts_, 1), 0);
+      int64_t acc = 0;
+      for (int f = 0; f < nfronts_; f++) {
+        fo[f] = acc;
+        acc += (fp.fronts[f].p + NB - 1) / NB;
+      }
+      ntileflags_ = std::max<int64_t>(acc, 1);
+      if ((rc = upload(d_flag_off_, fo))) return rc;
+      if ((rc = alloc(d_tflags_, (size_t)(2 * ntileflags_)))) return rc;
+    }
     if ((rc = upload(d_fr_, frh_))) return rc;
     if ((rc = upload(d_gidx_, fp.gidx))) return rc;
     if ((rc = upload(d_rel_, fp.rel))) return rc;
@@ -257,7 +278,7 @@ class CudaEngine : public Engine {
     if ((rc = upload(d_rowptr_, rp))) return rc;
     if ((rc = upload(d_colidx_, ci))) return rc;
     if ((rc = alloc(d_vals_, (size_t)std::max(1, nnz_)))) return rc;
-    if ((rc = alloc(d_flags_, 4))) return rc;
+    if ((rc = alloc(d_flags_, 8))) return rc;
     if ((rc = alloc(d_norms_, 3 * 64))) return rc;
     if ((rc = build_schedule())) return rc;
     if ((rc = finalize_tc())) return rc;
@@ -336,6 +357,7 @@ class CudaEngine : public Engine {
     int rc;
     if ((rc = ensure_solve(nrhs))) return rc;
     bnorm_.clear();
+    CK(cudaMemsetAsync(d_flags_ + 4, 0, sizeof(int), st));
     CK(cudaEventRecord(sev0_, st));
     SolveReport r;
     if (precision == 0) {
@@ -347,12 +369,24 @@ class CudaEngine : public Engine {
       if ((rc = refine(dB, ldb, dX, ldb, nrhs, st, &r))) return rc;
     }
     CK(cudaEventRecord(sev1_, st));
-    CK(cudaEventSynchronize(sev1_));
+    if ((rc = sweep_status(st))) return rc;
     prof_collect();
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, sev0_, sev1_));
     r.seconds = ms * 1e-3;
     if (rep) *rep = r;
+    return ENG_OK;
+  }
+
+  // Reads the pivot-block sweep timeout flag (synchronizes the stream).
+  int sweep_status(cudaStream_t st) {
+    int f = 0;
+    CK(cudaMemcpyAsync(&f, d_flags_ + 4, sizeof f, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (f) {
+      err_ = "solve sweep wait for a pivot tile timed out";
+      return ENG_ETIMEOUT;
+    }
     return ENG_OK;
   }
 
@@ -434,13 +468,53 @@ class CudaEngine : public Engine {
  private:
   template <typename T, int R>
   int sweep_attr() {
-    CK(cudaFuncSetAttribute(k_fwd_step<T, R>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)sweep_smem<T>()));
-    CK(cudaFuncSetAttribute(k_bwd_step<T, R>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)sweep_smem<T>()));
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
+    for (auto k : {k_fwd_diag<T, R>, k_bwd_diag<T, R>}) {
+      CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sweep_smem<T>()));
+      int nb = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, DIAG_ROWS,
+                                                       sweep_smem<T>()));
+      if (nb < 1) {
+        err_ = "pivot-block sweep kernel does not fit on an SM";
+        return ENG_ECUDA;
+      }
+      coop_cap_[(const void*)k] = nb * sms;
+    }
     return ENG_OK;
+  }
+
+  // One cooperative launch of the pivot-block sweep of a level: the grid is
+  // at most what the device holds at once, blocks stride over the tasks.
+  template <typename T, int R>
+  int diag_launch(bool fwd, const SweepTask* tasks, int ntasks, const T* F,
+                  const T* I, int nrhs, T* W, T* Y, cudaStream_t st) {
+    auto k = fwd ? k_fwd_diag<T, R> : k_bwd_diag<T, R>;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(std::min(ntasks, coop_cap_[(const void*)k]));
+    cfg.blockDim = dim3(DIAG_ROWS);
+    cfg.dynamicSmemBytes = sweep_smem<T>();
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int* fl = d_tflags_ + (fwd ? 0 : ntileflags_);
+    CK(cudaLaunchKernelEx(&cfg, k, tasks, ntasks, (const FrontDev*)d_fr_, F, I,
+                          (const int64_t*)d_flag_off_, nrhs, W, Y, fl,
+                          d_flags_ + 4));
+    return ENG_OK;
+  }
+  template <typename T>
+  int diag_sweep(bool fwd, const SweepTask* tasks, int ntasks, const T* F,
+                 const T* I, int nrhs, T* W, T* Y, cudaStream_t st) {
+    if (nrhs <= 1) return diag_launch<T, 1>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
+    if (nrhs <= 2) return diag_launch<T, 2>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
+    if (nrhs <= 4) return diag_launch<T, 4>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
+    if (nrhs <= 8) return diag_launch<T, 8>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
+    return diag_launch<T, 16>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
   }
 
   // --------------------------------------------------------- profiling
@@ -461,7 +535,7 @@ class CudaEngine : public Engine {
   void prof_end(int i, int fam, cudaStream_t st, double flops, double bytes) {
     if (i < 0) return;
     cudaEventRecord(pev_[i + 1], st);
-    pend_.push_back({fam, i, flops, bytes});
+    pend_.push_back({fam, i, cur_level_, flops, bytes});
   }
   // call after the stream that carried the records has been synchronized
   void prof_collect() {
@@ -476,6 +550,8 @@ class CudaEngine : public Engine {
       k.seconds += ms * 1e-3;
       k.flops += r.flops;
       k.bytes += r.bytes;
+      if ((prof_mask_ >> 31) && trace_.size() < (1u << 20))
+        trace_.push_back({r.fam, r.level, ms * 1e-3, r.flops, r.bytes});
     }
     pend_.clear();
     pev_used_ = 0;
@@ -679,15 +755,13 @@ class CudaEngine : public Engine {
       if ((rc = upload(L.listq, listq))) return rc;
       L.ea.assign(mc, nullptr);
       L.nea.assign(mc, 0);
-      L.ea_children.assign(mc, nullptr);
-      L.nea_children.assign(mc, 0);
       L.ea_elems.assign(mc, 0.0);
       for (int f = L.f0; f < L.f1; f++)
         L.solve_elems += fp.fronts[f].p + fp.fronts[f].q;
+      std::vector<int> kids;
       for (int r = 0; r < mc; r++) {
         int b0 = fp.ea_ptr[(size_t)l * mc + r], b1 = fp.ea_ptr[(size_t)l * mc + r + 1];
         std::vector<EaTask> tasks;
-        std::vector<int> kids;
         for (int k = b0; k < b1; k++) {
           int c = fp.ea_child[k];
           kids.push_back(c);
@@ -695,10 +769,10 @@ class CudaEngine : public Engine {
           L.ea_elems[r] += (double)fp.fronts[c].q * fp.fronts[c].q;
         }
         L.nea[r] = (int)tasks.size();
-        L.nea_children[r] = (int)kids.size();
         if (!tasks.empty() && (rc = upload(L.ea[r], tasks))) return rc;
-        if (!kids.empty() && (rc = upload(L.ea_children[r], kids))) return rc;
       }
+      L.nea_kids = (int)kids.size();
+      if (!kids.empty() && (rc = upload(L.ea_kids, kids))) return rc;
       int maxp = 0;
       for (int f = L.f0; f < L.f1; f++) maxp = std::max(maxp, fp.fronts[f].p);
       int nsteps = (maxp + NB - 1) / NB;
@@ -749,42 +823,35 @@ class CudaEngine : public Engine {
                        o + fi.p * ld, o + fi.p + fi.p * ld});
       }
       if ((rc = gemm_batch(f22, L.f22))) return rc;
-      // solve sweeps
-      L.fwd.assign(nsteps, nullptr);
-      L.bwd.assign(nsteps, nullptr);
-      L.nfwd.assign(nsteps, 0);
-      L.nbwd.assign(nsteps, 0);
-      L.fwd_elems.assign(nsteps, 0.0);
-      L.bwd_elems.assign(nsteps, 0.0);
-      for (int s = 0; s < nsteps; s++) {
-        int k0 = s * NB;
-        std::vector<SweepTask> tf, tb;
-        for (int f = L.f0; f < L.f1; f++) {
-          const FrontInfo& fi = fp.fronts[f];
-          if (fi.p <= k0) continue;
-          int kb = std::min(NB, fi.p - k0), k1 = k0 + kb, dim = fi.p + fi.q;
-          int cf = std::max(1, (dim - k1 + SWEEP_ROWS - 1) / SWEEP_ROWS);
-          int cb = std::max(1, (k0 + SWEEP_ROWS - 1) / SWEEP_ROWS);
-          for (int c = 0; c < cf; c++) tf.push_back({f, c, 0});
-          for (int c = 0; c < cb; c++) tb.push_back({f, c, 0});
-          L.fwd_elems[s] += (double)(dim - k0) * kb;
-          L.bwd_elems[s] += (double)(k1) * kb;
-        }
-        L.nfwd[s] = (int)tf.size();
-        L.nbwd[s] = (int)tb.size();
-        if (!tf.empty() && (rc = upload(L.fwd[s], tf))) return rc;
-        if (!tb.empty() && (rc = upload(L.bwd[s], tb))) return rc;
-      }
-      std::vector<SweepTask> gq;
-      for (int f = L.f0; f < L.f1; f++) {
+      // solve sweeps; fronts with the longest tile chains first
+      std::vector<int> byp;
+      for (int f = L.f0; f < L.f1; f++)
+        if (fp.fronts[f].p > 0) byp.push_back(f);
+      std::stable_sort(byp.begin(), byp.end(), [&](int x, int y) {
+        return fp.fronts[x].p > fp.fronts[y].p;
+      });
+      std::vector<SweepTask> wf, wb, gl, gq;
+      for (int f : byp) {
         const FrontInfo& fi = fp.fronts[f];
-        if (fi.p == 0 || fi.q == 0) continue;
-        int rcn = (fi.p + GEMV_ROWS - 1) / GEMV_ROWS;
-        int kcn = (fi.q + GEMV_K - 1) / GEMV_K;
-        for (int a = 0; a < rcn; a++)
-          for (int b = 0; b < kcn; b++) gq.push_back({f, a, b});
+        int nc = (fi.p + DIAG_ROWS - 1) / DIAG_ROWS;
+        for (int c = 0; c < nc; c++) wf.push_back({f, c, 0});
+        for (int c = nc - 1; c >= 0; c--) wb.push_back({f, c, 0});
+        L.diag_elems += 0.5 * fi.p * (fi.p + 1.0);
+        if (fi.q == 0) continue;
+        for (int a = 0; a < (fi.q + GEMV_ROWS - 1) / GEMV_ROWS; a++)
+          for (int b = 0; b < (fi.p + GEMV_K - 1) / GEMV_K; b++)
+            gl.push_back({f, a, b});
+        for (int a = 0; a < (fi.p + GEMV_ROWS - 1) / GEMV_ROWS; a++)
+          for (int b = 0; b < (fi.q + GEMV_K - 1) / GEMV_K; b++)
+            gq.push_back({f, a, b});
         L.gq_elems += (double)fi.p * fi.q;
       }
+      L.nwf = (int)wf.size();
+      L.nwb = (int)wb.size();
+      L.ngl = (int)gl.size();
+      if (!wf.empty() && (rc = upload(L.wf, wf))) return rc;
+      if (!wb.empty() && (rc = upload(L.wb, wb))) return rc;
+      if (!gl.empty() && (rc = upload(L.gl, gl))) return rc;
       L.ngq = (int)gq.size();
       if (!gq.empty() && (rc = upload(L.gq, gq))) return rc;
     }
@@ -858,6 +925,7 @@ class CudaEngine : public Engine {
     int rc;
     for (int l = 0; l < nlevels_; l++) {
       LevelSched& L = lv_[l];
+      cur_level_ = l;
       int64_t na = L.asm1 - L.asm0;
       int pi = prof_begin(KF_ASSEMBLE, st);
       if (L.mem1 > L.mem0)
@@ -896,6 +964,7 @@ class CudaEngine : public Engine {
       }
       if ((rc = factor_gemm(L.f22, F, st, KF_GEMM_SCHUR))) return rc;
     }
+    cur_level_ = -1;
     return ENG_OK;
   }
 
@@ -903,35 +972,42 @@ class CudaEngine : public Engine {
   int tree_solve(const T* F, const T* I, T* W, T* Y, const double* B, int ldb,
                  double* X, int ldx, int nrhs, cudaStream_t st) {
     const double es = sizeof(T);
-    int pi;
+    int pi, rc;
+    CK(cudaMemsetAsync(d_tflags_, 0, sizeof(int) * 2 * ntileflags_, st));
     for (int l = 0; l < nlevels_; l++) {
       LevelSched& L = lv_[l];
+      cur_level_ = l;
       int nf = L.f1 - L.f0;
       if (!nf) continue;
       pi = prof_begin(KF_SOLVE_MISC, st);
       k_solve_init<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_, B,
                                                    ldb, nrhs, W);
       CKL();
-      for (size_t r = 0; r < L.ea_children.size(); r++) {
-        if (!L.nea_children[r]) continue;
-        k_solve_ea<T><<<L.nea_children[r], 256, 0, st>>>(
-            L.ea_children[r], d_fr_, d_rel_, nrhs, W);
+      if (L.nea_kids) {
+        k_solve_ea<T><<<L.nea_kids, 256, 0, st>>>(L.ea_kids, d_fr_, d_rel_,
+                                                  nrhs, W);
         CKL();
       }
       prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
-      for (size_t s = 0; s < L.fwd.size(); s++) {
-        if (!L.nfwd[s]) continue;
+      if (L.nwf) {
         pi = prof_begin(KF_SOLVE_DIAG, st);
-        SNU_RG_DISPATCH(nrhs, k_fwd_step, T,
-                        (L.nfwd[s], 256, sweep_smem<T>(), st),
-                        (L.fwd[s], d_fr_, F, I, (int)s * NB, (int)s, nrhs, W, Y));
+        if ((rc = diag_sweep<T>(true, L.wf, L.nwf, F, I, nrhs, W, Y, st)))
+          return rc;
+        prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.diag_elems * nrhs,
+                 L.diag_elems * es);
+      }
+      if (L.ngl) {
+        pi = prof_begin(KF_SOLVE_GEMM, st);
+        SNU_RG_DISPATCH(nrhs, k_gemv_l21, T, (L.ngl, 256, 0, st),
+                        (L.gl, d_fr_, F, nrhs, W, Y));
         CKL();
-        prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.fwd_elems[s] * nrhs,
-                 L.fwd_elems[s] * es);
+        prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
+                 L.gq_elems * es);
       }
     }
     for (int l = nlevels_ - 1; l >= 0; l--) {
       LevelSched& L = lv_[l];
+      cur_level_ = l;
       int nf = L.f1 - L.f0;
       if (!nf) continue;
       pi = prof_begin(KF_SOLVE_MISC, st);
@@ -941,21 +1017,18 @@ class CudaEngine : public Engine {
       prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
       if (L.ngq) {
         pi = prof_begin(KF_SOLVE_GEMM, st);
-        SNU_RG_DISPATCH(nrhs, k_gemv_q, T, (L.ngq, 256, 0, st),
-                        (L.gq, d_fr_, F, nrhs, W));
+        SNU_RG_DISPATCH(nrhs, k_gemv_u12, T, (L.ngq, 256, 0, st),
+                        (L.gq, d_fr_, F, nrhs, W, Y));
         CKL();
         prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
                  L.gq_elems * es);
       }
-      for (int s = (int)L.bwd.size() - 1; s >= 0; s--) {
-        if (!L.nbwd[s]) continue;
+      if (L.nwb) {
         pi = prof_begin(KF_SOLVE_DIAG, st);
-        SNU_RG_DISPATCH(nrhs, k_bwd_step, T,
-                        (L.nbwd[s], 256, sweep_smem<T>(), st),
-                        (L.bwd[s], d_fr_, F, I, s * NB, s, nrhs, W, Y));
-        CKL();
-        prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.bwd_elems[s] * nrhs,
-                 L.bwd_elems[s] * es);
+        if ((rc = diag_sweep<T>(false, L.wb, L.nwb, F, I, nrhs, W, Y, st)))
+          return rc;
+        prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.diag_elems * nrhs,
+                 L.diag_elems * es);
       }
       pi = prof_begin(KF_SOLVE_MISC, st);
       k_scatter_y<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_, Y,
@@ -963,6 +1036,7 @@ class CudaEngine : public Engine {
       CKL();
       prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
     }
+    cur_level_ = -1;
     return ENG_OK;
   }
 
@@ -1072,6 +1146,7 @@ class CudaEngine : public Engine {
       r.backward_error = worst;
       return ENG_OK;
     };
+    CK(cudaMemsetAsync(d_flags_ + 4, 0, sizeof(int), st));
     do {
       if ((rc = colmax(dB, ldb, nrhs, st, bn))) break;
       if (precision == 0) {
@@ -1111,7 +1186,8 @@ class CudaEngine : public Engine {
     } while (0);
     prof_mask_ = saved_mask;
     if (rc && rc != ENG_ENOTCONV) return rc;
-    CK(cudaStreamSynchronize(st));
+    int wrc = sweep_status(st);
+    if (wrc) return wrc;
     if (rep) *rep = r;
     return rc;
   }
@@ -1172,9 +1248,11 @@ class CudaEngine : public Engine {
   cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
   // per-launch profiling
   struct ProfRec {
-    int fam, ev;
+    int fam, ev, level;
     double flops, bytes;
   };
+  std::vector<LaunchRec> trace_;
+  int cur_level_ = -1;  // tree level of the launches being issued
   unsigned prof_mask_ = 0;
   std::vector<cudaEvent_t> pev_;
   int pev_used_ = 0;
@@ -1189,6 +1267,12 @@ class CudaEngine : public Engine {
   int64_t arena_ = 0, wtot_ = 0;
   size_t wcap_ = 0, rcap_ = 0, ycap_ = 0;
   int64_t ytot_ = 0, invtot_ = 0;
+  // pivot-block sweep flags (forward, then backward) and per-front offsets
+  int64_t* d_flag_off_ = nullptr;
+  int* d_tflags_ = nullptr;
+  int64_t ntileflags_ = 0;
+  // co-resident grid size of each pivot-block sweep kernel
+  std::map<const void*, int> coop_cap_;
   // tensor-core GEMM workspace (packed split operands) and its batches
   float* d_pack_ = nullptr;
   int64_t pack_need_ = 0;

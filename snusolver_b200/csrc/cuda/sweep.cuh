@@ -3,153 +3,276 @@
 // the back solve, SnuMat_factorize.cu:258-345, kernel_sparse.cu:915-944).
 //
 // Per front the work vector W (dim x nrhs) and the pivot part Y (p x nrhs)
-// are updated tile by tile.  One launch per tile step (batched over the
-// fronts of a level): every CTA multiplies the tile's right-hand side by the
-// stored inverse of the diagonal tile and updates its own chunk of rows, so
-// no CTA waits on another.
+// are updated.  Each level of a sweep is two launches:
+//
+// * the pivot block (rows and columns [0, p)): one cooperative launch over
+//   (front, 128-row chunk) tasks.  The chunk holding a tile's rows solves the
+//   tile with the stored inverse of the diagonal tile, writes the result to Y
+//   and raises the tile's flag; the other chunks of the front wait for the
+//   flag (bounded spin), read the tile's solution and update their rows.
+//   The factor columns a chunk needs for a tile are staged into shared
+//   memory with cp.async while it waits.
+// * the off-diagonal part (L21 y for the forward sweep, U12 x_Q for the
+//   backward sweep): a tall-skinny product over (front, 64-row, 256-column)
+//   blocks that adds into W with atomics.
 #pragma once
 #include "kernels.cuh"
 
 namespace snu {
 
-constexpr int SWEEP_ROWS = 256;  // rows updated per CTA
-constexpr int RG = 16;           // right-hand sides per register group
+constexpr int RG = 16;          // right-hand sides per register group
+constexpr int DIAG_ROWS = 128;  // rows of a pivot-block chunk (= threads)
+constexpr long WAVE_SPIN_LIMIT = 1L << 22;
 
-// Dynamic shared memory of the sweep steps: the staged tile inverse.
+// Dynamic shared memory of the pivot-block sweeps: the staged factor
+// columns of a chunk [NB][DIAG_ROWS] and one tile inverse [NB][NB].
 template <typename T>
 constexpr size_t sweep_smem() {
-  return (size_t)NB * (NB + 1) * sizeof(T);
+  return (size_t)(NB * DIAG_ROWS + NB * NB) * sizeof(T);
 }
 
-// Forward step at tile (k0, kb): y = Linv * W[k0:k1]; Y[k0:k1] = y (chunk
-// 0); W[r] -= L[r, k0:k1] y for the CTA's rows r >= k1.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Spins (bounded) until *flag is set; on timeout sets *err and returns false.
+__device__ __forceinline__ bool wait_flag(const int* flag, int* err) {
+  for (long it = 0; it < WAVE_SPIN_LIMIT; it++) {
+    if (*(const volatile int*)flag) {
+      __threadfence();  // order the flag read before the reads of Y
+      return true;
+    }
+    __nanosleep(64);
+  }
+  atomicExch(err, 1);
+  return false;
+}
+
+__device__ __forceinline__ void raise_flag(int* flag) {
+  __threadfence();
+  atomicExch(flag, 1);
+}
+
+// Stages rows [r0, r1) of factor columns [k0, k0 + kb) of front f into
+// Ls[m * DIAG_ROWS + (row - rbase)] (rbase = the chunk's first row; r0 and
+// rbase are multiples of the 16-byte vector).  Rows up to r1 rounded up to
+// the vector stay inside the column (ld is a multiple of 4).
+template <typename T>
+__device__ __forceinline__ void stage_cols(T* Ls, const T* F, const FrontDev& f,
+                                           int rbase, int r0, int r1, int k0,
+                                           int kb) {
+  constexpr int V = 16 / sizeof(T);
+  const int nv = (r1 - r0 + V - 1) / V;
+  if (nv <= 0) return;
+  const T* src = F + f.off + r0 + (int64_t)k0 * f.ld;
+  T* dst = Ls + (r0 - rbase);
+  for (int e = threadIdx.x; e < kb * nv; e += blockDim.x) {
+    const int m = e / nv, v = e - m * nv;
+    cp_async16(dst + m * DIAG_ROWS + v * V, src + (int64_t)m * f.ld + v * V);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_inv(T* Xs, const T* inv) {
+  constexpr int V = 16 / sizeof(T);
+  for (int e = threadIdx.x; e < NB * NB / V; e += blockDim.x)
+    cp_async16(Xs + e * V, inv + e * V);
+}
+
+// out[i][r] = sum_m Xs[i + m NB] in[m][r] for the kb x nr block; written to
+// Yf (ld p) as well.  Called by all threads of the CTA.
 template <typename T, int R>
-__global__ void __launch_bounds__(256)
-    k_fwd_step(const SweepTask* __restrict__ tasks,
+__device__ __forceinline__ void tile_apply(const T* Xs, T (*in)[R],
+                                           T (*out)[R], T* Yf, int ldy, int k0,
+                                           int kb, int r0, int nr) {
+  for (int e = threadIdx.x; e < NB * R; e += blockDim.x) {
+    const int i = e % NB, r = e / NB;
+    T a = (T)0;
+#pragma unroll 16
+    for (int m = 0; m < NB; m++) a += Xs[i + m * NB] * in[m][r];
+    const bool ok = i < kb && r < nr;
+    out[i][r] = ok ? a : (T)0;
+    if (ok) Yf[k0 + i + (int64_t)(r0 + r) * ldy] = a;
+  }
+}
+
+// Forward sweep of the pivot blocks of one level.  Tasks are (front, chunk)
+// with the chunks of a front in ascending order, so every chunk waits only
+// on tasks of lower index; the grid is co-resident (cooperative launch) and
+// every block takes its tasks in ascending order, which rules out a cycle
+// of waits.  Tile s: y_s = Linv_s W[k0:k1]; W[r] -= L[r, k0:k1] y_s, r >= k1.
+template <typename T, int R>
+__global__ void __launch_bounds__(DIAG_ROWS)
+    k_fwd_diag(const SweepTask* __restrict__ tasks, int ntasks,
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
-               const T* __restrict__ INV, int k0, int step, int nrhs,
-               T* __restrict__ W, T* __restrict__ Y) {
-  extern __shared__ unsigned char smem_raw[];
-  T* X = reinterpret_cast<T*>(smem_raw);  // Linv, leading dimension NB + 1
+               const T* __restrict__ INV, const int64_t* __restrict__ flag_off,
+               int nrhs, T* __restrict__ W, T* __restrict__ Y, int* flags,
+               int* err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Ls = reinterpret_cast<T*>(smem_raw);
+  T* Xs = Ls + NB * DIAG_ROWS;
   __shared__ T ws[NB][R];
   __shared__ T ys[NB][R];
-  const SweepTask t = tasks[blockIdx.x];
-  const FrontDev f = fr[t.front];
-  const int kb = min(NB, f.p - k0), k1 = k0 + kb, dim = f.p + f.q;
-  const T* linv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
-  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x)
-    X[(e % NB) + (e / NB) * (NB + 1)] = linv[e];
-  T* Wf = W + f.w_off * nrhs;
-  T* Yf = Y + f.y_off * nrhs;
+  __shared__ int bad;
   const int tid = threadIdx.x;
-  const int row = k1 + t.chunk * SWEEP_ROWS + tid;
-  const T* lrow = F + f.off + row + (int64_t)k0 * f.ld;
-  for (int r0 = 0; r0 < nrhs; r0 += R) {
-    const int nr = min(R, nrhs - r0);
-    for (int e = tid; e < NB * R; e += blockDim.x) {
-      int i = e % NB, r = e / NB;
-      ws[i][r] = (i < kb && r < nr) ? Wf[k0 + i + (int64_t)(r0 + r) * dim] : (T)0;
-    }
-    __syncthreads();
-    for (int e = tid; e < NB * R; e += blockDim.x) {
-      int i = e % NB, r = e / NB;
-      T s = (T)0;
-#pragma unroll 16
-      for (int m = 0; m < NB; m++) s += X[i + m * (NB + 1)] * ws[m][r];
-      ys[i][r] = (i < kb && r < nr) ? s : (T)0;
-    }
-    __syncthreads();
-    if (t.chunk == 0)
-      for (int e = tid; e < NB * R; e += blockDim.x) {
-        int i = e % NB, r = e / NB;
-        if (i < kb && r < nr) Yf[k0 + i + (int64_t)(r0 + r) * f.p] = ys[i][r];
+  if (tid == 0) bad = 0;
+  __syncthreads();
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    const SweepTask t = tasks[task];
+    const FrontDev f = fr[t.front];
+    const int dim = f.p + f.q;
+    const int c0 = t.chunk * DIAG_ROWS, c1 = min(f.p, c0 + DIAG_ROWS);
+    const int ntiles = (f.p + NB - 1) / NB;
+    int* fl = flags + flag_off[t.front];
+    T* Wf = W + f.w_off * nrhs;
+    T* Yf = Y + f.y_off * nrhs;
+    const int row = c0 + tid;
+    for (int s = 0; s < ntiles; s++) {
+      const int k0 = s * NB, kb = min(NB, f.p - k0), k1 = k0 + kb;
+      if (k0 >= c1) break;  // owned by a later chunk; updates no row of ours
+      const bool owner = k0 >= c0;
+      const int u0 = max(c0, k1);  // rows [u0, c1) take this tile's update
+      stage_cols(Ls, F, f, c0, u0 & ~(16 / (int)sizeof(T) - 1), c1, k0, kb);
+      if (owner) stage_inv(Xs, INV + f.inv_off + (int64_t)s * 2 * NB * NB);
+      cp_async_commit();
+      if (!owner && tid == 0 && !wait_flag(fl + s, err)) bad = 1;
+      cp_async_wait_all();
+      __syncthreads();
+      if (bad) return;
+      for (int r0 = 0; r0 < nrhs; r0 += R) {
+        const int nr = min(R, nrhs - r0);
+        if (owner) {
+          for (int e = tid; e < NB * R; e += blockDim.x) {
+            const int i = e % NB, r = e / NB;
+            ws[i][r] = (i < kb && r < nr) ? Wf[k0 + i + (int64_t)(r0 + r) * dim]
+                                          : (T)0;
+          }
+          __syncthreads();
+          tile_apply<T, R>(Xs, ws, ys, Yf, f.p, k0, kb, r0, nr);
+          __threadfence();  // publish this thread's Y stores device-wide
+          __syncthreads();
+          if (tid == 0 && r0 + R >= nrhs) raise_flag(fl + s);
+        } else {
+          for (int e = tid; e < NB * R; e += blockDim.x) {
+            const int i = e % NB, r = e / NB;
+            ys[i][r] = (i < kb && r < nr)
+                           ? __ldcg(Yf + k0 + i + (int64_t)(r0 + r) * f.p)
+                           : (T)0;
+          }
+          __syncthreads();
+        }
+        if (row >= u0 && row < c1) {
+          T acc[R];
+#pragma unroll
+          for (int r = 0; r < R; r++) acc[r] = (T)0;
+#pragma unroll 8
+          for (int m = 0; m < kb; m++) {
+            const T l = Ls[m * DIAG_ROWS + tid];
+#pragma unroll
+            for (int r = 0; r < R; r++) acc[r] += l * ys[m][r];
+          }
+#pragma unroll
+          for (int r = 0; r < R; r++)
+            if (r < nr) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
+        }
+        __syncthreads();
       }
-    if (row < dim) {
-      T acc[R];
-#pragma unroll
-      for (int r = 0; r < R; r++) acc[r] = (T)0;
-      for (int m0 = 0; m0 < kb; m0 += 16) {
-        T lv[16];
-#pragma unroll
-        for (int u = 0; u < 16; u++)
-          lv[u] = m0 + u < kb ? lrow[(int64_t)(m0 + u) * f.ld] : (T)0;
-#pragma unroll
-        for (int u = 0; u < 16; u++)
-#pragma unroll
-          for (int r = 0; r < R; r++) acc[r] += lv[u] * ys[m0 + u][r];
-      }
-#pragma unroll
-      for (int r = 0; r < R; r++)
-        if (r < nr) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
     }
-    __syncthreads();
   }
 }
 
-// Backward step at tile (k0, kb): x = Uinv * W[k0:k1]; Y[k0:k1] = x (chunk
-// 0); W[r] -= U[r, k0:k1] x for the CTA's rows r < k0.
+// Backward sweep of the pivot blocks of one level (after W[0:p] -= U12 x_Q).
+// Tasks list the chunks of a front from the last to the first, so again
+// every wait is on a task of lower index.  Tile s (from the last):
+// x_s = Uinv_s W[k0:k1]; W[r] -= U[r, k0:k1] x_s for r < k0.
 template <typename T, int R>
-__global__ void __launch_bounds__(256)
-    k_bwd_step(const SweepTask* __restrict__ tasks,
+__global__ void __launch_bounds__(DIAG_ROWS)
+    k_bwd_diag(const SweepTask* __restrict__ tasks, int ntasks,
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
-               const T* __restrict__ INV, int k0, int step, int nrhs,
-               T* __restrict__ W, T* __restrict__ Y) {
-  extern __shared__ unsigned char smem_raw[];
-  T* X = reinterpret_cast<T*>(smem_raw);  // Uinv, leading dimension NB + 1
+               const T* __restrict__ INV, const int64_t* __restrict__ flag_off,
+               int nrhs, T* __restrict__ W, T* __restrict__ Y, int* flags,
+               int* err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Ls = reinterpret_cast<T*>(smem_raw);
+  T* Xs = Ls + NB * DIAG_ROWS;
   __shared__ T ws[NB][R];
   __shared__ T xs[NB][R];
-  const SweepTask t = tasks[blockIdx.x];
-  const FrontDev f = fr[t.front];
-  const int kb = min(NB, f.p - k0), dim = f.p + f.q;
-  const T* uinv = INV + f.inv_off + (int64_t)step * 2 * NB * NB + NB * NB;
-  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x)
-    X[(e % NB) + (e / NB) * (NB + 1)] = uinv[e];
-  T* Wf = W + f.w_off * nrhs;
-  T* Yf = Y + f.y_off * nrhs;
+  __shared__ int bad;
   const int tid = threadIdx.x;
-  const int row = t.chunk * SWEEP_ROWS + tid;
-  const T* urow = F + f.off + row + (int64_t)k0 * f.ld;
-  for (int r0 = 0; r0 < nrhs; r0 += R) {
-    const int nr = min(R, nrhs - r0);
-    for (int e = tid; e < NB * R; e += blockDim.x) {
-      int i = e % NB, r = e / NB;
-      ws[i][r] = (i < kb && r < nr) ? Wf[k0 + i + (int64_t)(r0 + r) * dim] : (T)0;
-    }
-    __syncthreads();
-    for (int e = tid; e < NB * R; e += blockDim.x) {
-      int i = e % NB, r = e / NB;
-      T s = (T)0;
-#pragma unroll 16
-      for (int m = 0; m < NB; m++) s += X[i + m * (NB + 1)] * ws[m][r];
-      xs[i][r] = (i < kb && r < nr) ? s : (T)0;
-    }
-    __syncthreads();
-    if (t.chunk == 0)
-      for (int e = tid; e < NB * R; e += blockDim.x) {
-        int i = e % NB, r = e / NB;
-        if (i < kb && r < nr) Yf[k0 + i + (int64_t)(r0 + r) * f.p] = xs[i][r];
+  if (tid == 0) bad = 0;
+  __syncthreads();
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    const SweepTask t = tasks[task];
+    const FrontDev f = fr[t.front];
+    const int dim = f.p + f.q;
+    const int c0 = t.chunk * DIAG_ROWS, c1 = min(f.p, c0 + DIAG_ROWS);
+    const int ntiles = (f.p + NB - 1) / NB;
+    int* fl = flags + flag_off[t.front];
+    T* Wf = W + f.w_off * nrhs;
+    T* Yf = Y + f.y_off * nrhs;
+    const int row = c0 + tid;
+    for (int s = ntiles - 1; s >= 0; s--) {
+      const int k0 = s * NB, kb = min(NB, f.p - k0);
+      if (k0 < c0) break;  // tile lies above our rows: nothing left
+      const bool owner = k0 < c1;
+      const int u1 = min(c1, k0);  // rows [c0, u1) take this tile's update
+      stage_cols(Ls, F, f, c0, c0, u1, k0, kb);
+      if (owner)
+        stage_inv(Xs, INV + f.inv_off + (int64_t)s * 2 * NB * NB + NB * NB);
+      cp_async_commit();
+      if (!owner && tid == 0 && !wait_flag(fl + s, err)) bad = 1;
+      cp_async_wait_all();
+      __syncthreads();
+      if (bad) return;
+      for (int r0 = 0; r0 < nrhs; r0 += R) {
+        const int nr = min(R, nrhs - r0);
+        if (owner) {
+          for (int e = tid; e < NB * R; e += blockDim.x) {
+            const int i = e % NB, r = e / NB;
+            ws[i][r] = (i < kb && r < nr) ? Wf[k0 + i + (int64_t)(r0 + r) * dim]
+                                          : (T)0;
+          }
+          __syncthreads();
+          tile_apply<T, R>(Xs, ws, xs, Yf, f.p, k0, kb, r0, nr);
+          __threadfence();
+          __syncthreads();
+          if (tid == 0 && r0 + R >= nrhs) raise_flag(fl + s);
+        } else {
+          for (int e = tid; e < NB * R; e += blockDim.x) {
+            const int i = e % NB, r = e / NB;
+            xs[i][r] = (i < kb && r < nr)
+                           ? __ldcg(Yf + k0 + i + (int64_t)(r0 + r) * f.p)
+                           : (T)0;
+          }
+          __syncthreads();
+        }
+        if (row < u1) {
+          T acc[R];
+#pragma unroll
+          for (int r = 0; r < R; r++) acc[r] = (T)0;
+#pragma unroll 8
+          for (int m = 0; m < kb; m++) {
+            const T u = Ls[m * DIAG_ROWS + tid];
+#pragma unroll
+            for (int r = 0; r < R; r++) acc[r] += u * xs[m][r];
+          }
+#pragma unroll
+          for (int r = 0; r < R; r++)
+            if (r < nr) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
+        }
+        __syncthreads();
       }
-    if (row < k0) {
-      T acc[R];
-#pragma unroll
-      for (int r = 0; r < R; r++) acc[r] = (T)0;
-      for (int m0 = 0; m0 < kb; m0 += 16) {
-        T uv[16];
-#pragma unroll
-        for (int u = 0; u < 16; u++)
-          uv[u] = m0 + u < kb ? urow[(int64_t)(m0 + u) * f.ld] : (T)0;
-#pragma unroll
-        for (int u = 0; u < 16; u++)
-#pragma unroll
-          for (int r = 0; r < R; r++) acc[r] += uv[u] * xs[m0 + u][r];
-      }
-#pragma unroll
-      for (int r = 0; r < R; r++)
-        if (r < nr) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
     }
-    __syncthreads();
   }
-  (void)dim;
 }
 
 // Backward start of a front: W[0:p] = Y (the forward result) and
@@ -175,27 +298,35 @@ __global__ void k_bwd_init(const int* __restrict__ list,
 
 constexpr int GEMV_ROWS = 64, GEMV_K = 256;
 
-// W[0:p] -= F12 W[p:dim] for a (64-row, 256-column) block of F12 per CTA;
-// column blocks of one front add into W with atomics.
-template <typename T, int R>
-__global__ void __launch_bounds__(256)
-    k_gemv_q(const SweepTask* __restrict__ tasks,
-             const FrontDev* __restrict__ fr, const T* __restrict__ F,
-             int nrhs, T* __restrict__ W) {
+// Off-diagonal products of the sweeps, one (64-row, 256-column) block per
+// CTA; the column blocks of a front add into W with atomics.
+//   FWD:  W[p + i] -= L21[i, :] Y        (i < q, over the p pivot columns)
+//   !FWD: W[i]     -= U12[i, :] W[p:dim] (i < p, over the q update columns)
+template <typename T, int R, bool FWD>
+__device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
+                                         const FrontDev* __restrict__ fr,
+                                         const T* __restrict__ F, int nrhs,
+                                         T* __restrict__ W,
+                                         const T* __restrict__ Y) {
   __shared__ T red[4][GEMV_ROWS][R + 1];
   const SweepTask t = tasks[blockIdx.x];
   const FrontDev f = fr[t.front];
   const int dim = f.p + f.q;
+  const int nrows = FWD ? f.q : f.p, nk = FWD ? f.p : f.q;
   const int i = t.chunk * GEMV_ROWS + (threadIdx.x & 63), g = threadIdx.x >> 6;
-  const int kc0 = t.kchunk * GEMV_K, kc1 = min(f.q, kc0 + GEMV_K);
+  const int kc0 = t.kchunk * GEMV_K, kc1 = min(nk, kc0 + GEMV_K);
   T* Wf = W + f.w_off * nrhs;
-  const T* a = F + f.off + i + (int64_t)f.p * f.ld;
+  // source vector (ld lds) and the operand block's first element
+  const T* src = FWD ? Y + f.y_off * nrhs : Wf + f.p;
+  const int lds = FWD ? f.p : dim;
+  const T* a = FWD ? F + f.off + f.p + i : F + f.off + i + (int64_t)f.p * f.ld;
+  T* dst = FWD ? Wf + f.p : Wf;
   for (int r0 = 0; r0 < nrhs; r0 += R) {
     const int nr = min(R, nrhs - r0);
     T acc[R];
 #pragma unroll
     for (int r = 0; r < R; r++) acc[r] = (T)0;
-    if (i < f.p) {
+    if (i < nrows) {
       constexpr int UB = R <= 4 ? 8 : (R <= 8 ? 4 : 2);  // loads in flight
       for (int k0 = kc0 + g; k0 < kc1; k0 += 4 * UB) {
         T av[UB], wv[UB][R];
@@ -205,7 +336,7 @@ __global__ void __launch_bounds__(256)
           av[u] = k < kc1 ? a[(int64_t)k * f.ld] : (T)0;
 #pragma unroll
           for (int r = 0; r < R; r++)
-            wv[u][r] = (k < kc1 && r < nr) ? Wf[f.p + k + (int64_t)(r0 + r) * dim]
+            wv[u][r] = (k < kc1 && r < nr) ? src[k + (int64_t)(r0 + r) * lds]
                                            : (T)0;
         }
 #pragma unroll
@@ -217,15 +348,31 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int r = 0; r < R; r++) red[g][threadIdx.x & 63][r] = acc[r];
     __syncthreads();
-    if (g == 0 && i < f.p) {
+    if (g == 0 && i < nrows) {
       for (int r = 0; r < nr; r++) {
         T s = red[0][threadIdx.x][r] + red[1][threadIdx.x][r] +
               red[2][threadIdx.x][r] + red[3][threadIdx.x][r];
-        atomicAdd(Wf + i + (int64_t)(r0 + r) * dim, -s);
+        atomicAdd(dst + i + (int64_t)(r0 + r) * dim, -s);
       }
     }
     __syncthreads();
   }
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(256)
+    k_gemv_l21(const SweepTask* __restrict__ tasks,
+               const FrontDev* __restrict__ fr, const T* __restrict__ F,
+               int nrhs, T* __restrict__ W, const T* __restrict__ Y) {
+  gemv_off<T, R, true>(tasks, fr, F, nrhs, W, Y);
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(256)
+    k_gemv_u12(const SweepTask* __restrict__ tasks,
+               const FrontDev* __restrict__ fr, const T* __restrict__ F,
+               int nrhs, T* __restrict__ W, const T* __restrict__ Y) {
+  gemv_off<T, R, false>(tasks, fr, F, nrhs, W, Y);
 }
 
 // X[gidx[t]] = Y[t] for the pivot rows of every front of a level.

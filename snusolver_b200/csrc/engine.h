@@ -57,6 +57,11 @@ struct KernelStat {
   double seconds = 0, flops = 0, bytes = 0;
 };
 
+struct LaunchRec {
+  int family, level;
+  double seconds, flops, bytes;
+};
+
 class Engine {
  public:
   virtual ~Engine() {}
@@ -65,6 +70,8 @@ class Engine {
   virtual void set_profiling(unsigned mask) = 0;
   virtual void profile(KernelStat* out) const = 0;  // KF_COUNT entries
   virtual void reset_profile() = 0;
+  // Per-launch records kept while the trace bit (1u << 31) is set.
+  virtual const std::vector<LaunchRec>& trace() const = 0;
   // Stream for all work of the handle (nullptr: the engine's own stream).
   virtual int set_stream(void* stream) = 0;
   // Uploads the plan and the CSR pattern (kept for the FP64 residual).
