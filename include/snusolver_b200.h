@@ -199,6 +199,88 @@ SNU_API snu_status snu_get_leaf_factor(snu_handle* h, int rank,
 SNU_API snu_status snu_get_dense_block(snu_handle* h, int i, int j,
                                        double* out);
 
+/* ---- request server (continuous batching; no reference counterpart) ----
+   A server runs factor, refactor-same-pattern and solve requests on one GPU
+   as they arrive.  Up to `slots` requests run at once, each on its own CUDA
+   stream, so their device work overlaps; a request is admitted when a slot
+   is free and, for a factor request, when its device memory fits in what
+   the budget leaves beside the resident factors (otherwise it waits for a
+   release, or fails with SNU_ENOMEM when nothing running could free
+   memory).  Requests on one matrix run in submission order; requests on
+   different matrices in any order.  Factors stay resident until released.
+   Factor requests whose sparsity pattern the server has seen before reuse
+   the cached host plan (ordering, structure, fronts) and skip the analysis.
+   Submit calls copy their input arrays; the X of a solve request must stay
+   valid until the request completes.  All calls are thread-safe. */
+typedef struct snu_server snu_server;
+
+typedef struct snu_server_opts {
+  int device;           /* CUDA device; default 0 */
+  int slots;            /* requests on the GPU at once; default 4 */
+  int64_t mem_budget;   /* device bytes for resident factors and work;
+                           default 120 GB, capped at 90% of the free memory */
+  int nleaves;          /* as snu_opts; default 8 */
+  int precision;        /* as snu_opts; default SNU_FP32_IR */
+  double ir_tol;        /* as snu_opts; default 1e-10 */
+  int ir_max_iter;      /* as snu_opts; default 10 */
+  int plan_cache;       /* host plans kept by pattern; default 64 */
+  int reserved[8];
+} snu_server_opts;
+
+typedef enum snu_request_type {
+  SNU_REQ_FACTOR = 0,    /* construct + factorize a new matrix */
+  SNU_REQ_REFACTOR = 1,  /* new values, same pattern, factorize */
+  SNU_REQ_SOLVE = 2,     /* X = A^-1 B against the resident factors */
+  SNU_REQ_RELEASE = 3    /* free the matrix's plan and factors */
+} snu_request_type;
+
+typedef struct snu_completion {
+  int64_t request;        /* id given by the submit call */
+  int64_t matrix;         /* matrix id */
+  int type;               /* snu_request_type */
+  int status;             /* snu_status of the request */
+  double queue_s;         /* submit -> start of service */
+  double service_s;       /* start of service -> completion */
+  double latency_s;       /* submit -> completion */
+  double backward_error;  /* solve requests */
+  int ir_iters;           /* solve requests */
+  int plan_reused;        /* factor requests: cached plan used */
+  int reserved[6];
+} snu_completion;
+
+typedef struct snu_server_stats {
+  int64_t resident_bytes;  /* device bytes held by resident matrices */
+  int64_t peak_bytes;      /* high-water mark of resident + admitted */
+  int64_t budget_bytes;
+  int64_t submitted, completed, failed;
+  int queued, running, matrices, cached_plans;
+  int reserved[8];
+} snu_server_stats;
+
+SNU_API void snu_server_default_opts(snu_server_opts* o);
+SNU_API snu_status snu_server_create(snu_server** s, const snu_server_opts* o);
+/* Waits for every submitted request, then frees everything. */
+SNU_API snu_status snu_server_destroy(snu_server* s);
+SNU_API const char* snu_server_last_error(const snu_server* s);
+/* New matrix (CSR host arrays, copied): *matrix receives its id. */
+SNU_API snu_status snu_server_factor(snu_server* s, int n, int nnz,
+                                     const int* rowptr, const int* colidx,
+                                     const double* vals, int64_t* matrix,
+                                     int64_t* request);
+SNU_API snu_status snu_server_refactor(snu_server* s, int64_t matrix,
+                                       const double* vals, int64_t* request);
+/* B (n x nrhs, leading dimension ldb) is copied; X is written on completion. */
+SNU_API snu_status snu_server_solve(snu_server* s, int64_t matrix,
+                                    const double* B, double* X, int nrhs,
+                                    int ldb, int64_t* request);
+SNU_API snu_status snu_server_release(snu_server* s, int64_t matrix,
+                                      int64_t* request);
+/* Completed requests, oldest first: waits up to wait_ms (0: no wait, -1:
+   until at least one completes or nothing is outstanding). */
+SNU_API snu_status snu_server_poll(snu_server* s, snu_completion* out, int max,
+                                   int* count, int wait_ms);
+SNU_API snu_status snu_server_get_stats(snu_server* s, snu_server_stats* st);
+
 /* ---- MatrixMarket input (read_matrix.cpp semantics) ---- */
 /* Reads a coordinate file into CSR arrays allocated with malloc (free with
    snu_free).  expand_symmetric mirrors symmetric files (reference: off). */

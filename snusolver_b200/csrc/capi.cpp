@@ -9,27 +9,10 @@
 #include <string>
 #include <vector>
 
-#include "engine.h"
-#include "host/fronts.h"
-#include "host/structure.h"
+#include "handle.h"
 
 // CUDA runtime calls used directly here (host staging for snu_solve).
 #include <cuda_runtime_api.h>
-
-struct snu_handle {
-  snu_opts opts;
-  std::string err;
-  snu::Structure S;
-  snu::FrontPlan FP;
-  std::vector<int> rowptr, colidx;
-  std::unique_ptr<snu::Engine> eng;
-  int state = 0;  // 0 empty, 1 analyzed, 2 constructed, 3 factorized
-  snu_stats stats;
-  double* dB = nullptr;  // staging for host solves
-  size_t dcap = 0;
-  void* stream = nullptr;    // user stream (applied at construct)
-  unsigned prof_mask = 0;    // profiling families (applied at construct)
-};
 
 namespace {
 
@@ -172,36 +155,7 @@ SNU_API snu_status snu_construct(snu_handle* h, int n, int nnz,
   if (nnz > 0 && !vals) return fail(h, SNU_EINVAL, "null values");
   snu_status s = snu_analyze(h, n, nnz, rowptr, colidx);
   if (s != SNU_OK) return s;
-  double t0 = now_s();
-  std::string err;
-  snu::FrontOptions fo;
-  if (snu::build_front_plan(h->S, fo, h->FP, err)) {
-    h->state = 1;
-    return fail(h, SNU_EINVAL, err);
-  }
-  snu::EngineOptions eo;
-  eo.device = h->opts.device;
-  eo.pivot_eps = h->opts.pivot_eps;
-  eo.ir_tol = h->opts.ir_tol;
-  eo.ir_max_iter = h->opts.ir_max_iter;
-  eo.mem_budget = h->opts.mem_budget;
-  h->eng = snu::make_engine(eo, err);
-  if (!h->eng) return fail(h, SNU_ECUDA, "CUDA engine unavailable: " + err);
-  int rc = h->eng->set_stream(h->stream);
-  if (rc) return from_engine(h, rc);
-  h->eng->set_profiling(h->prof_mask);
-  rc = h->eng->setup(h->S, h->FP, rowptr, colidx);
-  if (rc) return from_engine(h, rc);
-  rc = h->eng->set_values(vals);
-  if (rc) return from_engine(h, rc);
-  h->stats.analyze_s += now_s() - t0;
-  h->stats.nfronts = h->FP.nfronts;
-  h->stats.nlevels = h->FP.nlevels;
-  h->stats.factor_entries = h->FP.factor_entries;
-  h->stats.factor_flops = h->FP.flops;
-  h->stats.device_bytes = h->eng->device_bytes();
-  h->state = 2;
-  return SNU_OK;
+  return snu::finish_construct(h, vals, false);
 }
 
 SNU_API snu_status snu_factorize(snu_handle* h) {
@@ -293,16 +247,22 @@ SNU_API snu_status snu_solve(snu_handle* h, const double* B, double* X,
   }
   double* dB = h->dB;
   double* dX = h->dB + (size_t)n * nrhs;
+  // copies on the engine's stream, so they are ordered with its kernels
+  cudaStream_t st = (cudaStream_t)h->eng->stream();
   for (int r = 0; r < nrhs; r++)
-    if (cudaMemcpy(dB + (size_t)r * n, B + (size_t)r * ldb, sizeof(double) * n,
-                   cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(dB + (size_t)r * n, B + (size_t)r * ldb,
+                        sizeof(double) * n, cudaMemcpyHostToDevice,
+                        st) != cudaSuccess)
       return fail(h, SNU_ECUDA, "host to device copy failed");
-  snu_status s = snu_solve_device(h, dB, dX, nrhs, n, nullptr);
+  snu_status s = snu_solve_device(h, dB, dX, nrhs, n, st);
   if (s != SNU_OK && s != SNU_ENOTCONV) return s;
   for (int r = 0; r < nrhs; r++)
-    if (cudaMemcpy(X + (size_t)r * ldb, dX + (size_t)r * n, sizeof(double) * n,
-                   cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cudaMemcpyAsync(X + (size_t)r * ldb, dX + (size_t)r * n,
+                        sizeof(double) * n, cudaMemcpyDeviceToHost,
+                        st) != cudaSuccess)
       return fail(h, SNU_ECUDA, "device to host copy failed");
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return fail(h, SNU_ECUDA, "stream synchronize failed");
   return s;
 }
 
@@ -478,3 +438,45 @@ SNU_API snu_status snu_read_mtx(const char* path, int expand_symmetric,
 SNU_API void snu_free(void* p) { std::free(p); }
 
 }  // extern "C"
+
+namespace snu {
+
+snu_status finish_construct(snu_handle* h, const double* vals, bool have_plan) {
+  double t0 = now_s();
+  std::string err;
+  if (!have_plan) {
+    snu::FrontOptions fo;
+    if (snu::build_front_plan(h->S, fo, h->FP, err)) {
+      h->state = 1;
+      return fail(h, SNU_EINVAL, err);
+    }
+  }
+  snu::EngineOptions eo;
+  eo.device = h->opts.device;
+  eo.pivot_eps = h->opts.pivot_eps;
+  eo.ir_tol = h->opts.ir_tol;
+  eo.ir_max_iter = h->opts.ir_max_iter;
+  eo.mem_budget = h->opts.mem_budget;
+  h->eng = snu::make_engine(eo, err);
+  if (!h->eng) return fail(h, SNU_ECUDA, "CUDA engine unavailable: " + err);
+  int rc = h->eng->set_stream(h->stream);
+  if (rc) return from_engine(h, rc);
+  h->eng->set_profiling(h->prof_mask);
+  rc = h->eng->setup(h->S, h->FP, h->rowptr.data(), h->colidx.data());
+  if (rc) return from_engine(h, rc);
+  rc = h->eng->set_values(vals);
+  if (rc) return from_engine(h, rc);
+  h->stats.n = h->S.n;
+  h->stats.nnz = h->S.nnz;
+  h->stats.nleaves = h->opts.nleaves;
+  h->stats.analyze_s += now_s() - t0;
+  h->stats.nfronts = h->FP.nfronts;
+  h->stats.nlevels = h->FP.nlevels;
+  h->stats.factor_entries = h->FP.factor_entries;
+  h->stats.factor_flops = h->FP.flops;
+  h->stats.device_bytes = h->eng->device_bytes();
+  h->state = 2;
+  return SNU_OK;
+}
+
+}  // namespace snu

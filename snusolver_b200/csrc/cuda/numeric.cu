@@ -201,6 +201,7 @@ class CudaEngine : public Engine {
 
   const std::string& error() const override { return err_; }
 
+  void* stream() const override { return (void*)stream_; }
   int set_stream(void* st) override {
     CK(cudaSetDevice(opt_.device));
     CK(cudaStreamSynchronize(stream_));

@@ -74,6 +74,7 @@ class Engine {
   virtual const std::vector<LaunchRec>& trace() const = 0;
   // Stream for all work of the handle (nullptr: the engine's own stream).
   virtual int set_stream(void* stream) = 0;
+  virtual void* stream() const = 0;  // the stream work goes to
   // Uploads the plan and the CSR pattern (kept for the FP64 residual).
   virtual int setup(const Structure& s, const FrontPlan& fp, const int* rowptr,
                     const int* colidx) = 0;

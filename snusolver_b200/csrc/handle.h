@@ -1,0 +1,34 @@
+// Internal: the state behind an snu_handle, shared by the C-ABI (capi.cpp)
+// and the request server (server.cpp).
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/snusolver_b200.h"
+#include "engine.h"
+#include "host/fronts.h"
+#include "host/structure.h"
+
+struct snu_handle {
+  snu_opts opts;
+  std::string err;
+  snu::Structure S;
+  snu::FrontPlan FP;
+  std::vector<int> rowptr, colidx;
+  std::unique_ptr<snu::Engine> eng;
+  int state = 0;  // 0 empty, 1 analyzed, 2 constructed, 3 factorized
+  snu_stats stats;
+  double* dB = nullptr;  // staging for host solves
+  size_t dcap = 0;
+  void* stream = nullptr;    // user stream (applied at construct)
+  unsigned prof_mask = 0;    // profiling families (applied at construct)
+};
+
+namespace snu {
+// Builds the device plan and uploads values for a handle whose host
+// structure (S, rowptr, colidx; state 1) is in place: front plan (unless
+// have_plan), engine, setup, values.  Used by snu_construct and by the
+// server when it reuses a cached plan.
+snu_status finish_construct(snu_handle* h, const double* vals, bool have_plan);
+}  // namespace snu
