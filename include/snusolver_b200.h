@@ -61,7 +61,7 @@ typedef enum snu_precision {
 
 typedef struct snu_opts {
   int nleaves;          /* leaves of the separator tree (the reference's MPI
-                           rank count np); power of two, 1..512; default 8 */
+                           rank count np); power of two, 2..512; default 8 */
   int precision;        /* snu_precision; default SNU_FP64 */
   double pivot_eps;     /* static pivot of leaf pivots: |p| < eps -> +-eps
                            (src/param.h:3, kernel_sparse.cu:742-749); 1e-15 */

@@ -190,3 +190,17 @@ def config(name):
         rp, ci, v = convdiff3d(m)
         return rp, ci, v, rhs(len(rp) - 1, 4, seed=2)
     raise KeyError(name)
+
+
+if __name__ == "__main__":
+    # python -m snusolver_b200.generators NAME OUT.mtx [RHS.bin]
+    # writes a named workload as MatrixMarket (and its right-hand sides as
+    # raw column-major float64) for the driver or the reference's driver
+    import sys
+    if len(sys.argv) < 3:
+        sys.exit("usage: python -m snusolver_b200.generators "
+                 "{c1_2d128|c2_convdiff64|c4_27pt96|convdiffN} OUT.mtx [RHS.bin]")
+    rp, ci, v, B = config(sys.argv[1])
+    write_mtx(sys.argv[2], rp, ci, v, comment=f"snusolver_b200 {sys.argv[1]}")
+    if len(sys.argv) > 3:
+        np.asfortranarray(B).T.astype(np.float64).tofile(sys.argv[3])
