@@ -104,6 +104,21 @@ SNU_API snu_status snu_analyze(snu_handle* h, int n, int nnz,
 SNU_API snu_status snu_construct(snu_handle* h, int n, int nnz,
                                  const int* rowptr, const int* colidx,
                                  const double* vals);
+/* No reference counterpart: a batch of independent matrices given as one
+   block-diagonal CSR (matrix b owns rows and columns [row_start[b],
+   row_start[b+1]); an entry outside its block is refused).  Every matrix
+   gets its own ordering and front tree (as snu_construct would build it);
+   the trees are merged level by level so that one launch per kernel and
+   level covers the whole batch.  snu_factorize / snu_refactor / snu_solve
+   then act on all matrices at once (the solve's B and X have
+   row_start[nmat] rows); the refinement tolerance applies to the
+   block-diagonal system as a whole.  The single-matrix read-backs
+   (ordering, blocks, COO, leaf and dense factors) are not available on a
+   batch handle. */
+SNU_API snu_status snu_construct_batch(snu_handle* h, int nmat,
+                                       const int* row_start, int n, int nnz,
+                                       const int* rowptr, const int* colidx,
+                                       const double* vals);
 SNU_API snu_status snu_factorize(snu_handle* h);
 /* New values for the same pattern (host array, CSR order), then factorize. */
 SNU_API snu_status snu_refactor(snu_handle* h, const double* vals);

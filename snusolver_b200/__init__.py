@@ -90,6 +90,8 @@ _EXPORTS = {
     "snu_status_string": (C.c_char_p, [C.c_int]),
     "snu_analyze": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _I, _I]),
     "snu_construct": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _I, _I, _D]),
+    "snu_construct_batch": (C.c_int, [C.c_void_p, C.c_int, _I, C.c_int,
+                                      C.c_int, _I, _I, _D]),
     "snu_factorize": (C.c_int, [C.c_void_p]),
     "snu_refactor": (C.c_int, [C.c_void_p, _D]),
     "snu_solve": (C.c_int, [C.c_void_p, _D, _D, C.c_int, C.c_int]),
@@ -201,6 +203,32 @@ class Solver:
         self._check(self._lib.snu_construct(self._h, len(rp) - 1, len(ci),
                                             _iptr(rp), _iptr(ci), _dptr(v)))
         self.n, self.nnz = len(rp) - 1, len(ci)
+        return self
+
+    def construct_batch(self, mats):
+        """A batch of independent matrices [(rowptr, colidx, vals), ...] as
+        one block-diagonal system (see ``snu_construct_batch``).  Solves take
+        the right-hand sides of all matrices stacked in matrix order;
+        ``self.row_start`` gives each matrix's rows."""
+        rps, cis, vs, starts = [], [], [], [0]
+        nz = 0
+        for rp, ci, v in mats:
+            rp = np.asarray(rp, dtype=np.int64)
+            rps.append(rp[:-1] + nz)
+            cis.append(np.asarray(ci, dtype=np.int64) + starts[-1])
+            vs.append(np.asarray(v, dtype=np.float64))
+            nz += int(rp[-1])
+            starts.append(starts[-1] + len(rp) - 1)
+        rp = np.ascontiguousarray(np.concatenate(rps + [np.array([nz])]),
+                                  dtype=np.int32)
+        ci = np.ascontiguousarray(np.concatenate(cis), dtype=np.int32)
+        v = np.ascontiguousarray(np.concatenate(vs))
+        st = np.ascontiguousarray(starts, dtype=np.int32)
+        self._check(self._lib.snu_construct_batch(
+            self._h, len(mats), _iptr(st), len(rp) - 1, len(ci), _iptr(rp),
+            _iptr(ci), _dptr(v)))
+        self.n, self.nnz = len(rp) - 1, len(ci)
+        self.row_start = st
         return self
 
     def factorize(self):

@@ -2,6 +2,8 @@
 #include "../../include/snusolver_b200.h"
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -139,6 +141,8 @@ SNU_API snu_status snu_analyze(snu_handle* h, int n, int nnz,
     return fail(h, SNU_EINVAL, err);
   h->rowptr.assign(rowptr, rowptr + n + 1);
   h->colidx.assign(colidx, colidx + nnz);
+  h->batch = 0;
+  h->batch_rows.clear();
   h->state = 1;
   h->eng.reset();
   h->stats.n = n;
@@ -156,6 +160,82 @@ SNU_API snu_status snu_construct(snu_handle* h, int n, int nnz,
   snu_status s = snu_analyze(h, n, nnz, rowptr, colidx);
   if (s != SNU_OK) return s;
   return snu::finish_construct(h, vals, false);
+}
+
+SNU_API snu_status snu_construct_batch(snu_handle* h, int nmat,
+                                       const int* row_start, int n, int nnz,
+                                       const int* rowptr, const int* colidx,
+                                       const double* vals) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  std::string why;
+  if (nmat < 1 || !row_start || row_start[0] != 0 || row_start[nmat] != n)
+    return fail(h, SNU_EINVAL, "row_start must run from 0 to n");
+  if (!valid_csr(n, nnz, rowptr, colidx, why)) return fail(h, SNU_EINVAL, why);
+  if (nnz > 0 && !vals) return fail(h, SNU_EINVAL, "null values");
+  for (int b = 0; b < nmat; b++) {
+    if (row_start[b + 1] <= row_start[b])
+      return fail(h, SNU_EINVAL, "empty matrix in the batch");
+    for (int i = row_start[b]; i < row_start[b + 1]; i++)
+      for (int k = rowptr[i]; k < rowptr[i + 1]; k++)
+        if (colidx[k] < row_start[b] || colidx[k] >= row_start[b + 1])
+          return fail(h, SNU_EINVAL, "entry outside its diagonal block");
+  }
+  double t0 = now_s();
+  // every matrix: its own ordering, structure and front plan, in parallel
+  std::vector<snu::FrontPlan> plans(nmat);
+  std::vector<std::string> errs(nmat);
+  std::vector<int> rcs(nmat, 0);
+  std::atomic<int> next(0);
+  auto work = [&]() {
+    for (int b; (b = next.fetch_add(1)) < nmat;) {
+      const int r0 = row_start[b], nb = row_start[b + 1] - r0;
+      const int k0 = rowptr[r0], nzb = rowptr[r0 + nb] - k0;
+      std::vector<int> rp(nb + 1), ci(nzb);
+      for (int i = 0; i <= nb; i++) rp[i] = rowptr[r0 + i] - k0;
+      for (int k = 0; k < nzb; k++) ci[k] = colidx[k0 + k] - r0;
+      std::vector<int> order, sizes;
+      snu::Structure S;
+      snu::FrontOptions fo;
+      rcs[b] = snu::compute_ordering(nb, nzb, rp.data(), ci.data(),
+                                     h->opts.nleaves, order, sizes, errs[b]);
+      if (!rcs[b])
+        rcs[b] = snu::build_structure(nb, nzb, rp.data(), ci.data(),
+                                      h->opts.nleaves, order, sizes, S, errs[b]);
+      if (!rcs[b]) rcs[b] = snu::build_front_plan(S, fo, plans[b], errs[b]);
+    }
+  };
+  int nth = (int)std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()),
+                                    (unsigned)nmat);
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nth; t++) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  for (int b = 0; b < nmat; b++)
+    if (rcs[b])
+      return fail(h, SNU_EINVAL, "matrix " + std::to_string(b) + ": " + errs[b]);
+  std::vector<const snu::FrontPlan*> pp(nmat);
+  std::vector<int> roff(nmat);
+  std::vector<int64_t> zoff(nmat);
+  for (int b = 0; b < nmat; b++) {
+    pp[b] = &plans[b];
+    roff[b] = row_start[b];
+    zoff[b] = rowptr[row_start[b]];
+  }
+  std::string err;
+  h->eng.reset();
+  h->S = snu::Structure();
+  h->S.n = n;
+  h->S.nnz = nnz;
+  if (snu::merge_front_plans(pp, roff, zoff, h->FP, err))
+    return fail(h, SNU_EINVAL, err);
+  h->rowptr.assign(rowptr, rowptr + n + 1);
+  h->colidx.assign(colidx, colidx + nnz);
+  h->batch = nmat;
+  h->batch_rows.assign(row_start, row_start + nmat + 1);
+  h->state = 1;
+  h->stats = snu_stats();
+  h->stats.analyze_s = now_s() - t0;
+  return snu::finish_construct(h, vals, true);
 }
 
 SNU_API snu_status snu_factorize(snu_handle* h) {
@@ -325,6 +405,9 @@ SNU_API snu_status snu_reset_profile(snu_handle* h) {
 
 SNU_API snu_status snu_get_ordering(const snu_handle* h, int* order,
                                     int* sizes) {
+  if (h && h->batch)
+    return fail(const_cast<snu_handle*>(h), SNU_EINVAL,
+                "not available on a batch handle");
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
   if (h->state < 1) return fail(const_cast<snu_handle*>(h), SNU_ESTATE, "not analyzed");
   if (order) std::memcpy(order, h->S.order.data(), sizeof(int) * h->S.n);
@@ -335,6 +418,9 @@ SNU_API snu_status snu_get_ordering(const snu_handle* h, int* order,
 
 SNU_API snu_status snu_get_blocks(const snu_handle* h, int* block_start,
                                   int* block_size) {
+  if (h && h->batch)
+    return fail(const_cast<snu_handle*>(h), SNU_EINVAL,
+                "not available on a batch handle");
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
   if (h->state < 1) return fail(const_cast<snu_handle*>(h), SNU_ESTATE, "not analyzed");
   size_t m = h->S.block_start.size();
@@ -345,6 +431,9 @@ SNU_API snu_status snu_get_blocks(const snu_handle* h, int* block_start,
 
 SNU_API snu_status snu_get_coo(const snu_handle* h, int* perm_map, int* coo_r,
                                int* coo_c) {
+  if (h && h->batch)
+    return fail(const_cast<snu_handle*>(h), SNU_EINVAL,
+                "not available on a batch handle");
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
   if (h->state < 1) return fail(const_cast<snu_handle*>(h), SNU_ESTATE, "not analyzed");
   size_t m = h->S.perm_map.size();
@@ -464,6 +553,10 @@ snu_status finish_construct(snu_handle* h, const double* vals, bool have_plan) {
   h->eng->set_profiling(h->prof_mask);
   rc = h->eng->setup(h->S, h->FP, h->rowptr.data(), h->colidx.data());
   if (rc) return from_engine(h, rc);
+  if (h->batch) {
+    rc = h->eng->set_segments(h->batch_rows);
+    if (rc) return from_engine(h, rc);
+  }
   rc = h->eng->set_values(vals);
   if (rc) return from_engine(h, rc);
   h->stats.n = h->S.n;

@@ -145,18 +145,23 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 // ------------------------------------------------------------------ solves
 
 // Work vectors: front f holds dim x nrhs values at W + w_off * nrhs.
+// Gather / scatter kernels of the sweeps: SOLVE_SPLIT CTAs per front of
+// the level list, front = blockIdx.x / SOLVE_SPLIT (a 1-D grid, so a level
+// may hold any number of fronts).
+constexpr int SOLVE_SPLIT = 8;
+
 template <typename T>
 __global__ void k_solve_init(const int* __restrict__ list,
                              const FrontDev* __restrict__ fr,
                              const int* __restrict__ gidx,
                              const double* __restrict__ B, int ldb, int nrhs,
                              T* __restrict__ W) {
-  const FrontDev f = fr[list[blockIdx.y]];
+  const FrontDev f = fr[list[blockIdx.x / SOLVE_SPLIT]];
   const int dim = f.p + f.q;
   T* w = W + f.w_off * nrhs;
   const int* g = gidx + f.idx_off;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < dim * nrhs;
-       e += gridDim.x * blockDim.x) {
+  for (int e = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x;
+       e < dim * nrhs; e += SOLVE_SPLIT * blockDim.x) {
     int t = e % dim, r = e / dim;
     w[t + (int64_t)r * dim] = t < f.p ? (T)B[g[t] + (int64_t)r * ldb] : (T)0;
   }
@@ -214,6 +219,33 @@ __global__ void k_colmax(int n, int nrhs, const double* __restrict__ M, int ld,
     for (int o = 16; o > 0; o >>= 1)
       m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) atomicMax(out + r, __double_as_longlong(m));
+  }
+}
+
+// Per-segment column maxima: out[seg[i] * nrhs + r] = max |M[i, r]| over the
+// rows i of each segment (the matrices of a batch).  A warp whose rows all
+// lie in one segment reduces before its single atomic.
+__global__ void k_colmax_seg(int n, int nrhs, const double* __restrict__ M,
+                             int ld, const int* __restrict__ seg,
+                             unsigned long long* out) {
+  const unsigned full = 0xffffffffu;
+  for (int base = blockIdx.x * blockDim.x; base < n;
+       base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int sg = i < n ? seg[i] : -1;
+    const int s0 = __shfl_sync(full, sg, 0);
+    const bool same = __all_sync(full, sg == s0 || sg < 0);
+    for (int r = 0; r < nrhs; r++) {
+      double m = i < n ? fabs(M[i + (int64_t)r * ld]) : 0.0;
+      if (same) {
+        for (int o = 16; o > 0; o >>= 1)
+          m = fmax(m, __shfl_xor_sync(full, m, o));
+        if ((threadIdx.x & 31) == 0 && s0 >= 0)
+          atomicMax(out + (int64_t)s0 * nrhs + r, __double_as_longlong(m));
+      } else if (sg >= 0) {
+        atomicMax(out + (int64_t)sg * nrhs + r, __double_as_longlong(m));
+      }
+    }
   }
 }
 

@@ -287,16 +287,45 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
+  int set_segments(const std::vector<int>& row_start) override {
+    CK(cudaSetDevice(opt_.device));
+    const int ns = (int)row_start.size() - 1;
+    if (ns < 1 || row_start[0] != 0 || row_start[ns] != n_) {
+      err_ = "bad segment boundaries";
+      return ENG_EINVAL;
+    }
+    seg_start_ = row_start;
+    nseg_ = ns;
+    if (ns > 1) {
+      std::vector<int> seg(n_);
+      for (int b = 0; b < ns; b++)
+        for (int i = row_start[b]; i < row_start[b + 1]; i++) seg[i] = b;
+      int rc;
+      if ((rc = upload(d_seg_, seg))) return rc;
+      if ((rc = alloc(d_segnorms_, (size_t)ns * 64))) return rc;
+    }
+    anorm_seg_.assign(ns, 0.0);
+    return ENG_OK;
+  }
+
   int set_values(const double* vals) override {
     CK(cudaSetDevice(opt_.device));
     CK(cudaMemcpyAsync(d_vals_, vals, sizeof(double) * nnz_,
                        cudaMemcpyHostToDevice, stream_));
-    // ||A||_inf for the backward error
+    // ||A||_inf for the backward error (per matrix of a batch)
     anorm_ = 0;
-    for (int i = 0; i < n_; i++) {
-      double s = 0;
-      for (int k = rowptr_h_[i]; k < rowptr_h_[i + 1]; k++) s += std::fabs(vals[k]);
-      anorm_ = std::max(anorm_, s);
+    if ((int)anorm_seg_.size() != nseg_) anorm_seg_.assign(nseg_, 0.0);
+    for (int b = 0; b < nseg_; b++) {
+      const int i0 = nseg_ > 1 ? seg_start_[b] : 0;
+      const int i1 = nseg_ > 1 ? seg_start_[b + 1] : n_;
+      double a = 0;
+      for (int i = i0; i < i1; i++) {
+        double s = 0;
+        for (int k = rowptr_h_[i]; k < rowptr_h_[i + 1]; k++) s += std::fabs(vals[k]);
+        a = std::max(a, s);
+      }
+      anorm_seg_[b] = a;
+      anorm_ = std::max(anorm_, a);
     }
     have64_ = have32_ = false;
     CK(cudaStreamSynchronize(stream_));
@@ -643,7 +672,8 @@ class CudaEngine : public Engine {
     std::vector<GemmProb> rest;
     int64_t apos = 0;
     for (const GemmProb& g : probs) {
-      if (!tc_eligible(g)) {
+      // (the pack grids index problems in gridDim.y / z: at most 65535)
+      if (!tc_eligible(g) || gb.tc_host.size() >= 65535) {
         rest.push_back(g);
         continue;
       }
@@ -981,7 +1011,7 @@ class CudaEngine : public Engine {
       int nf = L.f1 - L.f0;
       if (!nf) continue;
       pi = prof_begin(KF_SOLVE_MISC, st);
-      k_solve_init<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_, B,
+      k_solve_init<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_, B,
                                                    ldb, nrhs, W);
       CKL();
       if (L.nea_kids) {
@@ -1012,7 +1042,7 @@ class CudaEngine : public Engine {
       int nf = L.f1 - L.f0;
       if (!nf) continue;
       pi = prof_begin(KF_SOLVE_MISC, st);
-      k_bwd_init<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_, X,
+      k_bwd_init<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_, X,
                                                  ldx, nrhs, Y, W);
       CKL();
       prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
@@ -1032,7 +1062,7 @@ class CudaEngine : public Engine {
                  L.diag_elems * es);
       }
       pi = prof_begin(KF_SOLVE_MISC, st);
-      k_scatter_y<T><<<dim3(8, nf), 256, 0, st>>>(L.list, d_fr_, d_gidx_, Y,
+      k_scatter_y<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_, Y,
                                                   nrhs, X, ldx);
       CKL();
       prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
@@ -1041,20 +1071,43 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
-  // Per-column max norms of up to 64 columns of M into host out[].
+  // Max norms of up to 64 columns of M into host out[], per matrix of a
+  // batch (out[b * nc + r]; one matrix: out[r]).
   int colmax(const double* M, int ld, int nrhs, cudaStream_t st,
              std::vector<double>& out) {
-    int nc = std::min(nrhs, 64);
-    CK(cudaMemsetAsync(d_norms_, 0, sizeof(unsigned long long) * 64, st));
-    k_colmax<<<148, 256, 0, st>>>(n_, nc, M, ld, d_norms_);
+    const int nc = std::min(nrhs, 64);
+    const size_t cnt = (size_t)nseg_ * nc;
+    unsigned long long* d = nseg_ > 1 ? d_segnorms_ : d_norms_;
+    CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * cnt, st));
+    if (nseg_ > 1)
+      k_colmax_seg<<<4 * 148, 256, 0, st>>>(n_, nc, M, ld, d_seg_, d);
+    else
+      k_colmax<<<148, 256, 0, st>>>(n_, nc, M, ld, d);
     CKL();
-    std::vector<unsigned long long> h(64);
-    CK(cudaMemcpyAsync(h.data(), d_norms_, sizeof(unsigned long long) * 64,
+    std::vector<unsigned long long> h(cnt);
+    CK(cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long) * cnt,
                        cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    out.assign(nc, 0.0);
-    for (int r = 0; r < nc; r++) memcpy(&out[r], &h[r], 8);
+    out.assign(cnt, 0.0);
+    for (size_t k = 0; k < cnt; k++) memcpy(&out[k], &h[k], 8);
     return ENG_OK;
+  }
+
+  // max over matrices and columns of ||r|| / (||A|| ||x|| + ||b||)
+  double backward_error(const std::vector<double>& rn,
+                        const std::vector<double>& xn,
+                        const std::vector<double>& bn) const {
+    const int nc = nseg_ > 0 ? (int)(rn.size() / nseg_) : 0;
+    double worst = 0;
+    for (int b = 0; b < nseg_; b++)
+      for (int r = 0; r < nc; r++) {
+        const size_t k = (size_t)b * nc + r;
+        const double den = anorm_seg_[b] * xn[k] + bn[k];
+        double be = den > 0 ? rn[k] / den : rn[k];
+        if (!(be == be)) be = INFINITY;
+        worst = std::max(worst, be);
+      }
+    return worst;
   }
 
   // Backward error max_r ||B - A X||inf / (||A||inf ||X||inf + ||B||inf)
@@ -1075,14 +1128,7 @@ class CudaEngine : public Engine {
     std::vector<double> rn, xn;
     if ((rc = colmax(d_R_, n_, nrhs, st, rn))) return rc;
     if ((rc = colmax(X, ldx, nrhs, st, xn))) return rc;
-    double worst = 0;
-    for (size_t r = 0; r < rn.size(); r++) {
-      double den = anorm_ * xn[r] + bnorm_[r];
-      double be = den > 0 ? rn[r] / den : rn[r];
-      if (!(be == be)) be = INFINITY;
-      worst = std::max(worst, be);
-    }
-    *out = worst;
+    *out = backward_error(rn, xn, bnorm_);
     return ENG_OK;
   }
 
@@ -1137,14 +1183,7 @@ class CudaEngine : public Engine {
       CKL();
       if ((q = colmax(R, n_, nrhs, st, rn))) return q;
       if ((q = colmax(X, ldb, nrhs, st, xn))) return q;
-      double worst = 0;
-      for (size_t c = 0; c < rn.size(); c++) {
-        double den = anorm_ * xn[c] + bn[c];
-        double be = den > 0 ? rn[c] / den : rn[c];
-        if (!(be == be)) be = INFINITY;
-        worst = std::max(worst, be);
-      }
-      r.backward_error = worst;
+      r.backward_error = backward_error(rn, xn, bn);
       return ENG_OK;
     };
     CK(cudaMemsetAsync(d_flags_ + 4, 0, sizeof(int), st));
@@ -1298,6 +1337,12 @@ class CudaEngine : public Engine {
   bool have64_ = false, have32_ = false;
   int tiny_ = 0;
   double anorm_ = 0;
+  // matrices of a batch (segments of rows) and their ||A||inf
+  int nseg_ = 1;
+  std::vector<int> seg_start_;
+  std::vector<double> anorm_seg_{0.0};
+  int* d_seg_ = nullptr;
+  unsigned long long* d_segnorms_ = nullptr;
   std::vector<double> bnorm_;
   std::vector<int> rowptr_h_;
   std::vector<LevelSched> lv_;

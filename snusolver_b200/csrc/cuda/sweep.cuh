@@ -283,13 +283,13 @@ __global__ void k_bwd_init(const int* __restrict__ list,
                            const int* __restrict__ gidx,
                            const double* __restrict__ X, int ldx, int nrhs,
                            const T* __restrict__ Y, T* __restrict__ W) {
-  const FrontDev f = fr[list[blockIdx.y]];
+  const FrontDev f = fr[list[blockIdx.x / SOLVE_SPLIT]];
   const int dim = f.p + f.q;
   T* w = W + f.w_off * nrhs;
   const T* y = Y + f.y_off * nrhs;
   const int* g = gidx + f.idx_off;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < dim * nrhs;
-       e += gridDim.x * blockDim.x) {
+  for (int e = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x;
+       e < dim * nrhs; e += SOLVE_SPLIT * blockDim.x) {
     int t = e % dim, r = e / dim;
     w[t + (int64_t)r * dim] = t < f.p ? y[t + (int64_t)r * f.p]
                                       : (T)X[g[t] + (int64_t)r * ldx];
@@ -382,11 +382,11 @@ __global__ void k_scatter_y(const int* __restrict__ list,
                             const int* __restrict__ gidx,
                             const T* __restrict__ Y, int nrhs,
                             double* __restrict__ X, int ldx) {
-  const FrontDev f = fr[list[blockIdx.y]];
+  const FrontDev f = fr[list[blockIdx.x / SOLVE_SPLIT]];
   const T* y = Y + f.y_off * nrhs;
   const int* g = gidx + f.idx_off;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < f.p * nrhs;
-       e += gridDim.x * blockDim.x) {
+  for (int e = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x;
+       e < f.p * nrhs; e += SOLVE_SPLIT * blockDim.x) {
     int t = e % f.p, r = e / f.p;
     X[g[t] + (int64_t)r * ldx] = (double)y[t + (int64_t)r * f.p];
   }

@@ -79,6 +79,10 @@ class Engine {
   virtual int setup(const Structure& s, const FrontPlan& fp, const int* rowptr,
                     const int* colidx) = 0;
   // Copies new values (host, original CSR order) to the device.
+  // Matrices of a batch: row ranges [row_start[b], row_start[b+1]); the
+  // backward error is then taken per matrix (max over matrices).  Call
+  // after setup, before set_values.
+  virtual int set_segments(const std::vector<int>& row_start) = 0;
   virtual int set_values(const double* vals) = 0;
   // Numeric factorization in FP64 (precision 0) or FP32 (precision 1).
   virtual int factorize(int precision, double* seconds) = 0;

@@ -7,6 +7,7 @@
 
 #include "../../include/snusolver_b200.h"
 #include "engine.h"
+#include "host/batch.h"
 #include "host/fronts.h"
 #include "host/structure.h"
 
@@ -23,6 +24,8 @@ struct snu_handle {
   size_t dcap = 0;
   void* stream = nullptr;    // user stream (applied at construct)
   unsigned prof_mask = 0;    // profiling families (applied at construct)
+  int batch = 0;             // matrices of a batch handle (0: one matrix)
+  std::vector<int> batch_rows;  // row_start of every matrix (batch + 1)
 };
 
 namespace snu {

@@ -152,6 +152,18 @@ def stencil27_lognormal(n=96, seed=4, sigma=2.0):
     return rowptr, colidx, vals, rng
 
 
+def batch_config(name="c3_batch256", count=256, seed=3, lo=32, hi=256):
+    """The batched workload: `count` independent SPD 2D 5-point matrices,
+    grid sides drawn uniformly from lo..hi per axis (seed 3), edge weights
+    lognormal(0, 1).  Returns a list of (rowptr, colidx, vals)."""
+    if name != "c3_batch256":
+        raise KeyError(name)
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(lo, hi + 1, size=(count, 2))
+    return [laplace2d_lognormal(int(nx), int(ny), seed=seed * 1000 + k)
+            for k, (nx, ny) in enumerate(sides)]
+
+
 def rhs(n, nrhs, seed, lo=-1.0, hi=1.0):
     """Column-major (n, nrhs) right-hand sides U[lo, hi]."""
     rng = np.random.default_rng(seed)
