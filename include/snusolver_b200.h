@@ -225,8 +225,10 @@ SNU_API snu_status snu_get_dense_block(snu_handle* h, int i, int j,
    different matrices in any order.  Factors stay resident until released.
    Factor requests whose sparsity pattern the server has seen before reuse
    the cached host plan (ordering, structure, fronts) and skip the analysis.
-   Submit calls copy their input arrays; the X of a solve request must stay
-   valid until the request completes.  All calls are thread-safe. */
+   Factor and refactor calls copy their arrays; a solve request reads B and
+   writes X when it runs, so both must stay valid (and B unchanged) until
+   the request completes -- submitting is then O(1) however large B is.
+   All calls are thread-safe. */
 typedef struct snu_server snu_server;
 
 typedef struct snu_server_opts {
@@ -284,7 +286,8 @@ SNU_API snu_status snu_server_factor(snu_server* s, int n, int nnz,
                                      int64_t* request);
 SNU_API snu_status snu_server_refactor(snu_server* s, int64_t matrix,
                                        const double* vals, int64_t* request);
-/* B (n x nrhs, leading dimension ldb) is copied; X is written on completion. */
+/* B and X: n x nrhs, leading dimension ldb; kept by the caller until the
+   request completes. */
 SNU_API snu_status snu_server_solve(snu_server* s, int64_t matrix,
                                     const double* B, double* X, int nrhs,
                                     int ldb, int64_t* request);

@@ -314,7 +314,9 @@ SNU_API snu_status snu_solve(snu_handle* h, const double* B, double* X,
   if (!B || !X || nrhs <= 0 || ldb < h->S.n)
     return fail(h, SNU_EINVAL, "bad right-hand side arguments");
   const int n = h->S.n;
-  size_t need = (size_t)n * nrhs * 2;
+  // staged in chunks of up to 16 columns, so device staging stays bounded
+  const int chunk = std::min(nrhs, 16);
+  size_t need = (size_t)n * chunk * 2;
   if (need > h->dcap) {
     if (h->dB) cudaFree(h->dB);
     h->dB = nullptr;
@@ -325,25 +327,40 @@ SNU_API snu_status snu_solve(snu_handle* h, const double* B, double* X,
     }
     h->dcap = need;
   }
-  double* dB = h->dB;
-  double* dX = h->dB + (size_t)n * nrhs;
   // copies on the engine's stream, so they are ordered with its kernels
   cudaStream_t st = (cudaStream_t)h->eng->stream();
-  for (int r = 0; r < nrhs; r++)
-    if (cudaMemcpyAsync(dB + (size_t)r * n, B + (size_t)r * ldb,
-                        sizeof(double) * n, cudaMemcpyHostToDevice,
-                        st) != cudaSuccess)
-      return fail(h, SNU_ECUDA, "host to device copy failed");
-  snu_status s = snu_solve_device(h, dB, dX, nrhs, n, st);
-  if (s != SNU_OK && s != SNU_ENOTCONV) return s;
-  for (int r = 0; r < nrhs; r++)
-    if (cudaMemcpyAsync(X + (size_t)r * ldb, dX + (size_t)r * n,
-                        sizeof(double) * n, cudaMemcpyDeviceToHost,
-                        st) != cudaSuccess)
-      return fail(h, SNU_ECUDA, "device to host copy failed");
-  if (cudaStreamSynchronize(st) != cudaSuccess)
-    return fail(h, SNU_ECUDA, "stream synchronize failed");
-  return s;
+  double be = 0, secs = 0;
+  int iters = 0, fb = 0;
+  snu_status result = SNU_OK;
+  for (int c0 = 0; c0 < nrhs; c0 += chunk) {
+    const int nc = std::min(chunk, nrhs - c0);
+    double* dB = h->dB;
+    double* dX = h->dB + (size_t)n * nc;
+    for (int r = 0; r < nc; r++)
+      if (cudaMemcpyAsync(dB + (size_t)r * n, B + (size_t)(c0 + r) * ldb,
+                          sizeof(double) * n, cudaMemcpyHostToDevice,
+                          st) != cudaSuccess)
+        return fail(h, SNU_ECUDA, "host to device copy failed");
+    snu_status s = snu_solve_device(h, dB, dX, nc, n, st);
+    if (s != SNU_OK && s != SNU_ENOTCONV) return s;
+    if (s != SNU_OK) result = s;
+    be = std::max(be, h->stats.backward_error);
+    iters = std::max(iters, h->stats.ir_iters);
+    fb |= h->stats.fp64_fallback;
+    secs += h->stats.solve_s;
+    for (int r = 0; r < nc; r++)
+      if (cudaMemcpyAsync(X + (size_t)(c0 + r) * ldb, dX + (size_t)r * n,
+                          sizeof(double) * n, cudaMemcpyDeviceToHost,
+                          st) != cudaSuccess)
+        return fail(h, SNU_ECUDA, "device to host copy failed");
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return fail(h, SNU_ECUDA, "stream synchronize failed");
+  }
+  h->stats.backward_error = be;
+  h->stats.ir_iters = iters;
+  h->stats.fp64_fallback = fb;
+  h->stats.solve_s = secs;
+  return result;
 }
 
 SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st) {

@@ -229,6 +229,9 @@ class CudaEngine : public Engine {
     nfronts_ = fp.nfronts;
     nlevels_ = fp.nlevels;
     arena_ = fp.arena;
+    deferring_ = true;
+    fix_.clear();
+    blob_.clear();
     // fronts
     frh_.resize(nfronts_);
     int64_t woff = 0, yoff = 0, ioff = 0;
@@ -283,6 +286,7 @@ class CudaEngine : public Engine {
     if ((rc = alloc(d_norms_, 3 * 64))) return rc;
     if ((rc = build_schedule())) return rc;
     if ((rc = finalize_tc())) return rc;
+    if ((rc = flush_uploads())) return rc;
     have64_ = have32_ = false;
     return ENG_OK;
   }
@@ -383,9 +387,26 @@ class CudaEngine : public Engine {
       err_ = "solve before factorize";
       return ENG_ESTATE;
     }
+    if (nrhs > SOLVE_CHUNK) {
+      // columns in chunks: work vectors stay bounded by SOLVE_CHUNK columns
+      SolveReport agg;
+      for (int c0 = 0; c0 < nrhs; c0 += SOLVE_CHUNK) {
+        SolveReport r;
+        int rc = solve(dB + (size_t)c0 * ldb, dX + (size_t)c0 * ldb,
+                       std::min(SOLVE_CHUNK, nrhs - c0), ldb, stream,
+                       precision, &r);
+        if (rc) return rc;
+        agg.backward_error = std::max(agg.backward_error, r.backward_error);
+        agg.ir_iters = std::max(agg.ir_iters, r.ir_iters);
+        agg.fp64_fallback |= r.fp64_fallback;
+        agg.seconds += r.seconds;
+      }
+      if (rep) *rep = agg;
+      return ENG_OK;
+    }
     cudaStream_t st = stream ? (cudaStream_t)stream : stream_;
     int rc;
-    if ((rc = ensure_solve(nrhs))) return rc;
+    if ((rc = ensure_solve(nrhs, precision == 0))) return rc;
     bnorm_.clear();
     CK(cudaMemsetAsync(d_flags_ + 4, 0, sizeof(int), st));
     CK(cudaEventRecord(sev0_, st));
@@ -607,12 +628,38 @@ class CudaEngine : public Engine {
     sizes_.push_back((int64_t)b);
     return ENG_OK;
   }
+  // Uploads a host array.  While the plan is being set up the arrays are
+  // packed into one host blob instead (256-byte aligned pieces) and go to
+  // the device in one allocation and one copy (flush_uploads), which keeps
+  // set-up from issuing hundreds of small synchronous copies.
   template <typename T>
   int upload(T*& p, const std::vector<T>& v) {
+    if (deferring_) {
+      size_t off = (blob_.size() + 255) / 256 * 256;
+      size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(T);
+      blob_.resize(off + bytes, 0);
+      if (!v.empty()) memcpy(blob_.data() + off, v.data(), v.size() * sizeof(T));
+      fix_.push_back({(void**)&p, off});
+      p = nullptr;
+      return ENG_OK;
+    }
     int rc = alloc(p, v.size());
     if (rc) return rc;
     if (!v.empty())
       CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return ENG_OK;
+  }
+  int flush_uploads() {
+    deferring_ = false;
+    if (fix_.empty()) return ENG_OK;
+    unsigned char* d = nullptr;
+    int rc = alloc(d, blob_.size());
+    if (rc) return rc;
+    CK(cudaMemcpy(d, blob_.data(), blob_.size(), cudaMemcpyHostToDevice));
+    for (const auto& f : fix_) *f.first = d + f.second;
+    fix_.clear();
+    blob_.clear();
+    blob_.shrink_to_fit();
     return ENG_OK;
   }
   void release() {
@@ -889,24 +936,44 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
-  int ensure_solve(int nrhs) {
-    int rc;
-    if ((size_t)(wtot_ * nrhs) > wcap_) {
-      wcap_ = (size_t)(wtot_ * nrhs);
-      if ((rc = alloc(d_W64_, wcap_))) return rc;
-      if ((rc = alloc(d_W32_, wcap_))) return rc;
+  // Work vectors for nrhs (<= SOLVE_CHUNK) columns: FP64 (fp64) or FP32
+  // sweeps, FP64 residual and correction.  Buffers only grow; a grown
+  // buffer replaces (and frees) the smaller one.
+  template <typename T>
+  int grow(T*& p, size_t& cap, size_t need) {
+    if (need <= cap && p) return ENG_OK;
+    if (p) {
+      release_ptr(p);
+      p = nullptr;
     }
-    if ((size_t)(ytot_ * nrhs) > ycap_) {
-      ycap_ = (size_t)(ytot_ * nrhs);
-      if ((rc = alloc(d_Y64_, ycap_))) return rc;
-      if ((rc = alloc(d_Y32_, ycap_))) return rc;
-    }
-    if ((size_t)n_ * nrhs > rcap_) {
-      rcap_ = (size_t)n_ * nrhs;
-      if ((rc = alloc(d_R_, rcap_))) return rc;
-      if ((rc = alloc(d_D_, rcap_))) return rc;
-    }
+    int rc = alloc(p, need);
+    if (rc) return rc;
+    cap = need;
     return ENG_OK;
+  }
+  int ensure_solve(int nrhs, bool fp64) {
+    int rc;
+    const size_t w = (size_t)wtot_ * nrhs, y = (size_t)ytot_ * nrhs;
+    const size_t r = (size_t)n_ * nrhs;
+    if (fp64) {
+      if ((rc = grow(d_W64_, wcap64_, w)) || (rc = grow(d_Y64_, ycap64_, y)))
+        return rc;
+    } else {
+      if ((rc = grow(d_W32_, wcap32_, w)) || (rc = grow(d_Y32_, ycap32_, y)))
+        return rc;
+    }
+    if ((rc = grow(d_R_, rcapR_, r)) || (rc = grow(d_D_, rcapD_, r))) return rc;
+    return ENG_OK;
+  }
+  void release_ptr(void* p) {
+    for (size_t k = 0; k < ptrs_.size(); k++)
+      if (ptrs_[k] == p) {
+        cudaFree(p);
+        bytes_ -= sizes_[k];
+        ptrs_.erase(ptrs_.begin() + k);
+        sizes_.erase(sizes_.begin() + k);
+        return;
+      }
   }
 
   // --------------------------------------------------------- launches
@@ -1255,6 +1322,7 @@ class CudaEngine : public Engine {
           int frc = factorize(0, &sec);
           if (frc) return frc;
         }
+        if ((rc = ensure_solve(nrhs, true))) return rc;
         if ((rc = tree_solve<double>(d_F64_, d_I64_, d_W64_, d_Y64_, d_R_, n_, d_D_, n_,
                                      nrhs, st)))
           return rc;
@@ -1305,7 +1373,8 @@ class CudaEngine : public Engine {
   const FrontPlan* fp_ = nullptr;
   int n_ = 0, nnz_ = 0, nfronts_ = 0, nlevels_ = 0;
   int64_t arena_ = 0, wtot_ = 0;
-  size_t wcap_ = 0, rcap_ = 0, ycap_ = 0;
+  size_t wcap64_ = 0, wcap32_ = 0, ycap64_ = 0, ycap32_ = 0, rcapR_ = 0,
+         rcapD_ = 0;
   int64_t ytot_ = 0, invtot_ = 0;
   // pivot-block sweep flags (forward, then backward) and per-front offsets
   int64_t* d_flag_off_ = nullptr;
@@ -1337,6 +1406,10 @@ class CudaEngine : public Engine {
   bool have64_ = false, have32_ = false;
   int tiny_ = 0;
   double anorm_ = 0;
+  // deferred uploads of the set-up (see upload / flush_uploads)
+  bool deferring_ = false;
+  std::vector<unsigned char> blob_;
+  std::vector<std::pair<void**, size_t>> fix_;
   // matrices of a batch (segments of rows) and their ||A||inf
   int nseg_ = 1;
   std::vector<int> seg_start_;

@@ -97,9 +97,10 @@ struct Request {
   int64_t id = 0, matrix = 0;
   int type = 0;
   double t_submit = 0;
-  // factor: pattern + values; refactor: values; solve: B (copied), X
+  // factor: pattern + values; refactor: values; solve: B and X (caller's)
   std::vector<int> rowptr, colidx;
-  std::vector<double> vals, B;
+  std::vector<double> vals;
+  const double* B = nullptr;
   double* X = nullptr;
   int n = 0, nnz = 0, nrhs = 0, ldb = 0;
 };
@@ -395,7 +396,7 @@ int snu_server::run_other(Request& r, Matrix& m, cudaStream_t st, double* be,
   if (r.type == SNU_REQ_REFACTOR) {
     s = snu_refactor(m.h, r.vals.data());
   } else {
-    s = snu_solve(m.h, r.B.data(), r.X, r.nrhs, r.ldb);
+    s = snu_solve(m.h, r.B, r.X, r.nrhs, r.ldb);
     *be = m.h->stats.backward_error;
     *iters = m.h->stats.ir_iters;
   }
@@ -573,8 +574,7 @@ SNU_API snu_status snu_server_solve(snu_server* s, int64_t matrix,
   r->nrhs = nrhs;
   r->ldb = ldb;
   r->X = X;
-  r->B.assign(B, B + (size_t)ldb * (nrhs - 1) + n);
-  r->B.resize((size_t)ldb * nrhs);
+  r->B = B;
   enqueue(s, std::move(r), request);
   return SNU_OK;
 }

@@ -131,6 +131,40 @@ def laplace2d_lognormal(nx, ny, seed, sigma=1.0):
     return rowptr, colidx, vals
 
 
+def laplace3d_lognormal(nx, ny, nz, seed, sigma=1.0):
+    """SPD 3D 7-point: symmetric edge weights lognormal(0, sigma) (one per
+    grid edge, boundary edges to the Dirichlet boundary included in the
+    diagonal), off-diagonal -w, diagonal = sum of incident weights."""
+    rng = np.random.default_rng(seed)
+    shape = (nx, ny, nz)
+    offs = _neighbours(3, False)  # (-1,0,0),(1,0,0),(0,-1,0),(0,1,0),...
+    rowptr, colidx, rows, oid = _grid_csr(shape, offs)
+    # weights of the edges between x and x+1 along each axis (boundary
+    # edges at both ends included): shape + 1 along that axis
+    w = [rng.lognormal(0.0, sigma, size=tuple(s + (a == k) for k, s in
+                                             enumerate(shape)))
+         for a in range(3)]
+    co = np.unravel_index(rows, shape)
+    vals = np.zeros(len(colidx))
+    for k, off in enumerate(offs):
+        a = int(np.nonzero(off)[0][0])
+        m = oid == k
+        idx = [c[m] for c in co]
+        if off[a] > 0:
+            idx[a] = idx[a] + 1
+        vals[m] = -w[a][tuple(idx)]
+    dm = oid < 0
+    d = np.zeros(int(dm.sum()))
+    idx = [c[dm] for c in co]
+    for a in range(3):
+        lo = list(idx)
+        hi = list(idx)
+        hi[a] = hi[a] + 1
+        d += w[a][tuple(lo)] + w[a][tuple(hi)]
+    vals[dm] = d
+    return rowptr, colidx, vals
+
+
 def stencil27_lognormal(n=96, seed=4, sigma=2.0):
     """3D 27-point, symmetric edge weights lognormal(0, sigma) (off-diagonal
     -w), diagonal 1.05 x the row's absolute off-diagonal sum."""

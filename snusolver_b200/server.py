@@ -154,7 +154,7 @@ class Server:
         self._check(self._lib.snu_server_solve(
             self._s, matrix, Bf.ctypes.data_as(_D), X.ctypes.data_as(_D),
             nrhs, n, C.byref(r)))
-        self._keep[r.value] = X
+        self._keep[r.value] = (Bf, X)  # both live until completion
         return r.value, (X[:, 0] if one else X)
 
     def release(self, matrix):
@@ -197,3 +197,164 @@ class Server:
         self._check(self._lib.snu_server_get_stats(self._s, C.byref(s)))
         return {k: getattr(s, k) for k, _ in _ServerStats._fields_
                 if k != "reserved"}
+
+
+# ---------------------------------------------------------------- workload
+SERVE_SHAPES = ((100, 100), (224, 224), (400, 400), (707, 707),
+                (22, 22, 22), (37, 37, 37), (54, 54, 54), (79, 79, 79))
+
+
+def _laplacian(shape, seed):
+    from . import generators
+    if len(shape) == 2:
+        return generators.laplace2d_lognormal(shape[0], shape[1], seed=seed)
+    return generators.laplace3d_lognormal(*shape, seed=seed)
+
+
+def rescale_values(rowptr, colidx, vals, rng, lo=0.5, hi=2.0):
+    """Refactor values: every off-diagonal entry times U[lo, hi]; each
+    diagonal entry scaled with its row's off-diagonal sum, so the row keeps
+    its diagonal dominance (a no-pivot LU of a Laplacian whose entries are
+    all rescaled independently can break down, in the reference too)."""
+    rowptr = np.asarray(rowptr)
+    n = len(rowptr) - 1
+    rows = np.repeat(np.arange(n), np.diff(rowptr))
+    off = np.asarray(colidx) != rows
+    v = np.array(vals, dtype=np.float64)
+    old = np.zeros(n)
+    np.add.at(old, rows[off], np.abs(v[off]))
+    v[off] *= rng.uniform(lo, hi, int(off.sum()))
+    new = np.zeros(n)
+    np.add.at(new, rows[off], np.abs(v[off]))
+    ratio = np.where(old > 0, new / np.where(old > 0, old, 1.0), 1.0)
+    v[~off] *= ratio[rows[~off]]
+    return v
+
+
+def run_stream(rate=200.0, duration=5.0, seed=5, mix=(0.05, 0.10, 0.85),
+               slots=4, mem_budget=120 << 30, max_resident=4, warm=True,
+               shapes=SERVE_SHAPES, device=0):
+    """The serving workload: Poisson arrivals (mean `rate` per second, seeded)
+    for `duration` seconds, mixing new-factor requests on 2D / 3D lognormal
+    Laplacians (n from 1e4 to 5e5, shapes from `shapes`), refactor requests
+    (off-diagonal values times U[0.5, 2] per entry, see rescale_values)
+    and solve requests (1-64 right-hand
+    sides) against resident matrices, FP32 factors + FP64 refinement to
+    1e-10.  At most `max_resident` matrices are kept; the oldest is released
+    when a factor request would pass that.  With `warm`, one matrix of every
+    shape is factored (and released) first, so host plans are cached.
+    Returns per-type p50 / p99 latency, throughput and failure counts."""
+    import time
+    rng = np.random.default_rng(seed)
+    # the request list, drawn up front
+    t, reqs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        u = rng.uniform()
+        kind = 0 if u < mix[0] else (1 if u < mix[0] + mix[1] else 2)
+        reqs.append((t, kind, int(rng.integers(len(shapes))),
+                     int(rng.integers(1, 65)), int(rng.integers(1 << 30))))
+    mats_cache = {}
+
+    def matrix(k):
+        if k not in mats_cache:
+            mats_cache[k] = _laplacian(shapes[k], seed=1000 + k)
+        return mats_cache[k]
+
+    for k in range(len(shapes)):
+        matrix(k)
+    # right-hand sides and refactor values drawn before the clock starts:
+    # per shape a pool of 64 RHS columns and 4 rescaled value sets
+    prng = np.random.default_rng(seed + 1)
+    rhs_pool = {k: np.asfortranarray(prng.uniform(-1.0, 1.0, size=(
+        len(mats_cache[k][0]) - 1, 64))) for k in range(len(shapes))}
+    val_pool = {k: [rescale_values(*mats_cache[k], prng) for _ in range(4)]
+                for k in range(len(shapes))}
+    out = {"requests": len(reqs), "rate": rate, "duration_s": duration,
+           "slots": slots, "mix": list(mix)}
+    with Server(slots=slots, mem_budget=mem_budget, device=device) as s:
+        if warm:
+            t0 = time.perf_counter()
+            ids = [s.factor(*matrix(k))[0] for k in range(len(shapes))]
+            s.drain()
+            for m in ids:
+                s.release(m)
+            s.drain()
+            out["warm_s"] = time.perf_counter() - t0
+        resident = []   # (matrix id, shape index, values)
+        keep = []
+        lag = []
+        start = time.perf_counter()
+        for (ta, kind, k, nrhs, rs) in reqs:
+            now = time.perf_counter() - start
+            if ta > now:
+                time.sleep(ta - now)
+            lag.append(time.perf_counter() - start - ta)
+            r2 = np.random.default_rng(rs)
+            if kind == 0 or not resident:
+                rp, ci, v = matrix(k)
+                v = v * r2.uniform(0.5, 2.0) if kind == 0 else v
+                m, _ = s.factor(rp, ci, v)
+                resident.append((m, k, v))
+                if len(resident) > max_resident:
+                    old = resident.pop(0)
+                    s.release(old[0])
+            elif kind == 1:
+                j = int(r2.integers(len(resident)))
+                m, k2, v = resident[j]
+                v2 = val_pool[k2][int(r2.integers(4))]
+                s.refactor(m, v2)
+                resident[j] = (m, k2, v2)
+            else:
+                j = int(r2.integers(len(resident)))
+                m, k2, _ = resident[j]
+                c0 = int(r2.integers(0, 65 - nrhs))
+                B = rhs_pool[k2][:, c0:c0 + nrhs]
+                _, X = s.solve(m, B)
+                keep.append(X)
+        comps = s.drain()
+        end = time.perf_counter()
+        st = s.stats()
+    done = comps
+    out["completed"] = len(done)
+    out["wall_s"] = end - start
+    out["throughput_rps"] = len([c for c in done if c["type"] != "release"]) / (end - start)
+    out["peak_device_gb"] = st["peak_bytes"] / 1e9
+    out["submit_lag_p99_ms"] = float(np.percentile(lag, 99) * 1e3) if lag else 0.0
+    for typ in ("factor", "refactor", "solve"):
+        lat = np.array([c["latency_s"] for c in done if c["type"] == typ
+                        and c["status"] == 0])
+        svc = np.array([c["service_s"] for c in done if c["type"] == typ
+                        and c["status"] == 0])
+        bad = [c for c in done if c["type"] == typ and c["status"] != 0]
+        if len(lat):
+            out[typ] = {"n": int(len(lat)),
+                        "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                        "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                        "service_p50_ms": float(np.percentile(svc, 50) * 1e3),
+                        "failed": len(bad)}
+        else:
+            out[typ] = {"n": 0, "failed": len(bad)}
+    be = [c["backward_error"] for c in done if c["type"] == "solve"
+          and c["status"] == 0]
+    out["solve_worst_backward_error"] = float(max(be)) if be else None
+    out["statuses"] = sorted({int(c["status"]) for c in done})
+    return out
+
+
+if __name__ == "__main__":
+    # python -m snusolver_b200.server [--rate R] [--duration S] [--slots K]
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--duration", type=float, default=5.0)
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--seed", type=int, default=5)
+    ap.add_argument("--budget-gb", type=float, default=120.0)
+    a = ap.parse_args()
+    print(json.dumps(run_stream(rate=a.rate, duration=a.duration, seed=a.seed,
+                                slots=a.slots,
+                                mem_budget=int(a.budget_gb * (1 << 30)))))
