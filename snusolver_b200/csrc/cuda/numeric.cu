@@ -143,6 +143,8 @@ struct LevelSched {
 
 
 constexpr int GBM = 64, GBN = 64;
+// outer block of the two-level blocked partial LU (a multiple of NB)
+constexpr int OB = 256;
 
 #define SNU_LAUNCH_(K, T, R, CFG, ARGS) K<T, R><<<SNU_UNPACK CFG>>> ARGS
 #define SNU_UNPACK(...) __VA_ARGS__
@@ -876,15 +878,34 @@ class CudaEngine : public Engine {
           S.diag_elems += 2.0 * kb * kb;
           S.panel_flops += 2.0 * rem * (double)kb * kb;
           S.panel_elems += 4.0 * rem * (double)kb;
+          // Two-level blocking: inside the OB-column block [K0, K1) a step
+          // updates only the block's columns (every row below) and the
+          // block's rows (every column right of the block) -- what the next
+          // steps of the block read; the step that completes the block
+          // applies the block's rank-(K1-K0) update to the rest of the pivot
+          // rows and columns.  F22 takes the rank-p Schur update at the end.
           int64_t o = fi.offset, ld = fi.ld;
-          if (dim - k1 > 0 && fi.p - k1 > 0)
-            gp.push_back({dim - k1, fi.p - k1, kb, fi.ld, fi.ld, fi.ld,
-                          o + k1 + S.k0 * ld, o + S.k0 + k1 * ld,
-                          o + k1 + k1 * ld});
-          if (fi.p - k1 > 0 && fi.q > 0)
-            gp.push_back({fi.p - k1, fi.q, kb, fi.ld, fi.ld, fi.ld,
-                          o + k1 + S.k0 * ld, o + S.k0 + fi.p * ld,
-                          o + k1 + fi.p * ld});
+          const int K0 = S.k0 / OB * OB, K1 = std::min(K0 + OB, fi.p);
+          if (k1 < K1) {
+            if (dim - k1 > 0)  // rows k1..dim, block columns k1..K1
+              gp.push_back({dim - k1, K1 - k1, kb, fi.ld, fi.ld, fi.ld,
+                            o + k1 + S.k0 * ld, o + S.k0 + k1 * ld,
+                            o + k1 + k1 * ld});
+            if (dim - K1 > 0)  // block rows k1..K1, columns K1..dim
+              gp.push_back({K1 - k1, dim - K1, kb, fi.ld, fi.ld, fi.ld,
+                            o + k1 + S.k0 * ld, o + S.k0 + K1 * ld,
+                            o + k1 + K1 * ld});
+          } else {
+            const int kk = K1 - K0;
+            if (dim - K1 > 0 && fi.p - K1 > 0)  // rows K1..dim, cols K1..p
+              gp.push_back({dim - K1, fi.p - K1, kk, fi.ld, fi.ld, fi.ld,
+                            o + K1 + K0 * ld, o + K0 + K1 * ld,
+                            o + K1 + K1 * ld});
+            if (fi.p - K1 > 0 && fi.q > 0)  // rows K1..p, cols p..dim
+              gp.push_back({fi.p - K1, fi.q, kk, fi.ld, fi.ld, fi.ld,
+                            o + K1 + K0 * ld, o + K0 + fi.p * ld,
+                            o + K1 + fi.p * ld});
+          }
         }
         S.nactive = (int)act.size();
         S.npanel = (int)pt.size();
