@@ -21,7 +21,7 @@
 
 namespace snu {
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_STAGES = 6;
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_STAGES = 3;
 constexpr long TC_SPIN_LIMIT = 1L << 24;
 
 struct TcProb {
