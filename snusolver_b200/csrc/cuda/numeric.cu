@@ -701,8 +701,10 @@ class CudaEngine : public Engine {
   }
 
   // Tensor-core eligibility of a problem on the FP32 path.
+  // (tiles past the problem's edge read zeros through TMA and store
+  // nothing; below 64 rows or columns the SIMT kernel is cheaper)
   static bool tc_eligible(const GemmProb& g) {
-    return g.m >= TC_BM && g.n >= TC_BN && g.k >= 16;
+    return g.m >= 64 && g.n >= 64 && g.k >= 16;
   }
 
   int gemm_batch(const std::vector<GemmProb>& probs, GemmBatch& gb) {
