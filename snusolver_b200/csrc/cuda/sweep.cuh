@@ -25,11 +25,12 @@ constexpr int SOLVE_CHUNK = 16; // right-hand sides per solve pass
 constexpr int DIAG_ROWS = 128;  // rows of a pivot-block chunk (= threads)
 constexpr long WAVE_SPIN_LIMIT = 1L << 22;
 
-// Dynamic shared memory of the pivot-block sweeps: the staged factor
-// columns of a chunk [NB][DIAG_ROWS] and one tile inverse [NB][NB].
+// Dynamic shared memory of the pivot-block sweeps: two buffers (the tile
+// being applied and the next one) of the staged factor columns of a chunk
+// [NB][DIAG_ROWS] and a tile inverse [NB][NB].
 template <typename T>
 constexpr size_t sweep_smem() {
-  return (size_t)(NB * DIAG_ROWS + NB * NB) * sizeof(T);
+  return 2 * (size_t)(NB * DIAG_ROWS + NB * NB) * sizeof(T);
 }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -43,6 +44,10 @@ __device__ __forceinline__ void cp_async_commit() {
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+// all but the most recently committed group
+__device__ __forceinline__ void cp_async_wait_prev() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
 // Spins (bounded) until *flag is set; on timeout sets *err and returns false.
@@ -111,6 +116,8 @@ __device__ __forceinline__ void tile_apply(const T* Xs, T (*in)[R],
 // on tasks of lower index; the grid is co-resident (cooperative launch) and
 // every block takes its tasks in ascending order, which rules out a cycle
 // of waits.  Tile s: y_s = Linv_s W[k0:k1]; W[r] -= L[r, k0:k1] y_s, r >= k1.
+// The factor columns and inverse of tile s+1 are staged (double buffer)
+// while tile s waits for its flag and is applied.
 template <typename T, int R>
 __global__ void __launch_bounds__(DIAG_ROWS)
     k_fwd_diag(const SweepTask* __restrict__ tasks, int ntasks,
@@ -119,12 +126,13 @@ __global__ void __launch_bounds__(DIAG_ROWS)
                int nrhs, T* __restrict__ W, T* __restrict__ Y, int* flags,
                int* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ls = reinterpret_cast<T*>(smem_raw);
-  T* Xs = Ls + NB * DIAG_ROWS;
+  T* Ls0 = reinterpret_cast<T*>(smem_raw);  // [2][NB][DIAG_ROWS]
+  T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;         // [2][NB * NB]
   __shared__ T ws[NB][R];
   __shared__ T ys[NB][R];
   __shared__ int bad;
   const int tid = threadIdx.x;
+  constexpr int V = 16 / sizeof(T);
   if (tid == 0) bad = 0;
   __syncthreads();
   for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
@@ -137,16 +145,30 @@ __global__ void __launch_bounds__(DIAG_ROWS)
     T* Wf = W + f.w_off * nrhs;
     T* Yf = Y + f.y_off * nrhs;
     const int row = c0 + tid;
+    // stages tile s into buffer b: the rows of this chunk it updates and,
+    // for the chunk that owns it, its inverse
+    auto stage = [&](int s, int b) {
+      const int k0 = s * NB, kb = min(NB, f.p - k0), k1 = k0 + kb;
+      const int u0 = max(c0, k1);
+      stage_cols(Ls0 + b * NB * DIAG_ROWS, F, f, c0, u0 & ~(V - 1), c1, k0, kb);
+      if (k0 >= c0)
+        stage_inv(Xs0 + b * NB * NB, INV + f.inv_off + (int64_t)s * 2 * NB * NB);
+    };
+    cp_async_wait_all();
+    __syncthreads();
+    stage(0, 0);
+    cp_async_commit();
     for (int s = 0; s < ntiles; s++) {
       const int k0 = s * NB, kb = min(NB, f.p - k0), k1 = k0 + kb;
       if (k0 >= c1) break;  // owned by a later chunk; updates no row of ours
       const bool owner = k0 >= c0;
       const int u0 = max(c0, k1);  // rows [u0, c1) take this tile's update
-      stage_cols(Ls, F, f, c0, u0 & ~(16 / (int)sizeof(T) - 1), c1, k0, kb);
-      if (owner) stage_inv(Xs, INV + f.inv_off + (int64_t)s * 2 * NB * NB);
+      const T* Ls = Ls0 + (s & 1) * NB * DIAG_ROWS;
+      const T* Xs = Xs0 + (s & 1) * NB * NB;
+      if (s + 1 < ntiles && (s + 1) * NB < c1) stage(s + 1, (s + 1) & 1);
       cp_async_commit();
       if (!owner && tid == 0 && !wait_flag(fl + s, err)) bad = 1;
-      cp_async_wait_all();
+      cp_async_wait_prev();  // tile s staged (tile s+1 may still be in flight)
       __syncthreads();
       if (bad) return;
       for (int r0 = 0; r0 < nrhs; r0 += R) {
@@ -189,12 +211,14 @@ __global__ void __launch_bounds__(DIAG_ROWS)
       }
     }
   }
+  cp_async_wait_all();
 }
 
 // Backward sweep of the pivot blocks of one level (after W[0:p] -= U12 x_Q).
 // Tasks list the chunks of a front from the last to the first, so again
 // every wait is on a task of lower index.  Tile s (from the last):
-// x_s = Uinv_s W[k0:k1]; W[r] -= U[r, k0:k1] x_s for r < k0.
+// x_s = Uinv_s W[k0:k1]; W[r] -= U[r, k0:k1] x_s for r < k0.  Staging of
+// tile s-1 overlaps tile s as in the forward sweep.
 template <typename T, int R>
 __global__ void __launch_bounds__(DIAG_ROWS)
     k_bwd_diag(const SweepTask* __restrict__ tasks, int ntasks,
@@ -203,8 +227,8 @@ __global__ void __launch_bounds__(DIAG_ROWS)
                int nrhs, T* __restrict__ W, T* __restrict__ Y, int* flags,
                int* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ls = reinterpret_cast<T*>(smem_raw);
-  T* Xs = Ls + NB * DIAG_ROWS;
+  T* Ls0 = reinterpret_cast<T*>(smem_raw);
+  T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;
   __shared__ T ws[NB][R];
   __shared__ T xs[NB][R];
   __shared__ int bad;
@@ -221,17 +245,28 @@ __global__ void __launch_bounds__(DIAG_ROWS)
     T* Wf = W + f.w_off * nrhs;
     T* Yf = Y + f.y_off * nrhs;
     const int row = c0 + tid;
+    auto stage = [&](int s, int b) {
+      const int k0 = s * NB, kb = min(NB, f.p - k0);
+      stage_cols(Ls0 + b * NB * DIAG_ROWS, F, f, c0, c0, min(c1, k0), k0, kb);
+      if (k0 < c1)
+        stage_inv(Xs0 + b * NB * NB,
+                  INV + f.inv_off + (int64_t)s * 2 * NB * NB + NB * NB);
+    };
+    cp_async_wait_all();
+    __syncthreads();
+    stage(ntiles - 1, (ntiles - 1) & 1);
+    cp_async_commit();
     for (int s = ntiles - 1; s >= 0; s--) {
       const int k0 = s * NB, kb = min(NB, f.p - k0);
       if (k0 < c0) break;  // tile lies above our rows: nothing left
       const bool owner = k0 < c1;
       const int u1 = min(c1, k0);  // rows [c0, u1) take this tile's update
-      stage_cols(Ls, F, f, c0, c0, u1, k0, kb);
-      if (owner)
-        stage_inv(Xs, INV + f.inv_off + (int64_t)s * 2 * NB * NB + NB * NB);
+      const T* Ls = Ls0 + (s & 1) * NB * DIAG_ROWS;
+      const T* Xs = Xs0 + (s & 1) * NB * NB;
+      if (s >= 1 && (s - 1) * NB >= c0) stage(s - 1, (s - 1) & 1);
       cp_async_commit();
       if (!owner && tid == 0 && !wait_flag(fl + s, err)) bad = 1;
-      cp_async_wait_all();
+      cp_async_wait_prev();
       __syncthreads();
       if (bad) return;
       for (int r0 = 0; r0 < nrhs; r0 += R) {
@@ -274,6 +309,7 @@ __global__ void __launch_bounds__(DIAG_ROWS)
       }
     }
   }
+  cp_async_wait_all();
 }
 
 // Backward start of a front: W[0:p] = Y (the forward result) and
