@@ -41,6 +41,46 @@ constexpr int SB = 16;  // sub-block of the blocked tile factorization
 // fill the off-diagonal blocks by distance from the diagonal.  A tile
 // smaller than NB is padded with the identity, which leaves its factors and
 // inverses unchanged.
+// One distance of stage B of k_diag_lu_inv: the 2 (NB/SB - DIST) blocks of
+// Linv and Uinv at block distance DIST, element (ei, ej) of each per thread.
+// Compile-time trip counts: the products unroll fully and the independent
+// blocks interleave.
+template <typename T, int DIST>
+__device__ __forceinline__ void inv_distance(const T* D, T* XL, T* XU,
+                                             T (*Tb)[SB][SB + 1], int ei,
+                                             int ej) {
+  constexpr int NT = NB / SB - DIST;
+  T acc[2 * NT];
+#pragma unroll
+  for (int t = 0; t < 2 * NT; t++) acc[t] = (T)0;
+#pragma unroll
+  for (int mm = 0; mm < DIST * SB; mm++) {
+#pragma unroll
+    for (int t = 0; t < NT; t++) {  // L(b2, m) Linv(m, b1), m from b1
+      acc[t] += D[(t + DIST) * SB + ei + (t * SB + mm) * TLD] *
+                XL[t * SB + mm + (t * SB + ej) * TLD];
+      // U(b1, m) Uinv(m, b2), m from b1 + 1
+      acc[NT + t] += D[t * SB + ei + ((t + 1) * SB + mm) * TLD] *
+                     XU[(t + 1) * SB + mm + ((t + DIST) * SB + ej) * TLD];
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 2 * NT; t++) Tb[t][ei][ej] = acc[t];
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < NT; t++) {
+    T al = (T)0, au = (T)0;
+#pragma unroll
+    for (int m = 0; m < SB; m++) {
+      al -= XL[(t + DIST) * SB + ei + ((t + DIST) * SB + m) * TLD] * Tb[t][m][ej];
+      au -= XU[t * SB + ei + (t * SB + m) * TLD] * Tb[NT + t][m][ej];
+    }
+    XL[(t + DIST) * SB + ei + (t * SB + ej) * TLD] = al;
+    XU[t * SB + ei + ((t + DIST) * SB + ej) * TLD] = au;
+  }
+  __syncthreads();
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_diag_lu_inv(const int* __restrict__ active,
@@ -192,44 +232,9 @@ __global__ void __launch_bounds__(256)
   //   Linv(b2,b1) = -Linv(b2,b2) * sum_{m=b1}^{b2-1} L(b2,m) Linv(m,b1)
   //   Uinv(b1,b2) = -Uinv(b1,b1) * sum_{m=b1+1}^{b2} U(b1,m) Uinv(m,b2)
   const int ei = tid & 15, ej = tid >> 4;
-  for (int d = 1; d < NB / SB; d++) {
-    const int nt = NB / SB - d;  // blocks at distance d, per triangle
-    for (int t = 0; t < 2 * nt; t++) {
-      const bool low = t < nt;
-      const int b1 = low ? t : t - nt, b2 = b1 + d;
-      T acc = (T)0;
-      if (low) {
-        const int r = b2 * SB + ei, c = b1 * SB + ej;
-        for (int m = b1 * SB; m < b2 * SB; m++)
-          acc += D[r + m * TLD] * XL[m + c * TLD];
-      } else {
-        const int r = b1 * SB + ei, c = b2 * SB + ej;
-        for (int m = (b1 + 1) * SB; m < (b2 + 1) * SB; m++)
-          acc += D[r + m * TLD] * XU[m + c * TLD];
-      }
-      Tb[t][ei][ej] = acc;
-    }
-    __syncthreads();
-    for (int t = 0; t < 2 * nt; t++) {
-      const bool low = t < nt;
-      const int b1 = low ? t : t - nt, b2 = b1 + d;
-      T acc = (T)0;
-      if (low) {
-        const int r = b2 * SB + ei;
-#pragma unroll
-        for (int m = 0; m < SB; m++)
-          acc -= XL[r + (b2 * SB + m) * TLD] * Tb[t][m][ej];
-        XL[r + (b1 * SB + ej) * TLD] = acc;
-      } else {
-        const int r = b1 * SB + ei;
-#pragma unroll
-        for (int m = 0; m < SB; m++)
-          acc -= XU[r + (b1 * SB + m) * TLD] * Tb[t][m][ej];
-        XU[r + (b2 * SB + ej) * TLD] = acc;
-      }
-    }
-    __syncthreads();
-  }
+  inv_distance<T, 1>(D, XL, XU, Tb, ei, ej);
+  inv_distance<T, 2>(D, XL, XU, Tb, ei, ej);
+  inv_distance<T, 3>(D, XL, XU, Tb, ei, ej);
   T* inv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
   for (int e = tid; e < NB * NB; e += 256) {
     const int i = e & (NB - 1), j = e / NB;
