@@ -29,6 +29,8 @@ struct TcProb {
   int64_t a, b, c;  // element offsets of A, B, C in the front arena
   int lda, ldb, ldc;
   int64_t apack, bpack;  // element offsets of A', B' in the pack workspace
+  int64_t pc, rel;       // Schur scatter into the parent (see GemmProb)
+  int pld, pad;
 };
 
 struct TcTile {
@@ -186,7 +188,7 @@ __global__ void __launch_bounds__(128, 1)
     k_gemm_tc(const TcTile* __restrict__ tiles, const TcProb* __restrict__ probs,
               const CUtensorMap* __restrict__ amaps,
               const CUtensorMap* __restrict__ bmaps, float* __restrict__ F,
-              int* err) {
+              int* err, const int* __restrict__ rel_base) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES], acc_bar;
   __shared__ uint32_t tmem_base_s;
@@ -295,9 +297,20 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
         for (int j = 0; j < 32; j++)
           cv[j] = j < ncol ? cp[(int64_t)j * pr.ldc] : 0.f;
+        if (pr.pc >= 0) {
+          // extend-add fused: the child's update goes straight to the parent
+          const int* rel = rel_base + pr.rel;
+          float* prow = F + pr.pc + rel[row];
 #pragma unroll
-        for (int j = 0; j < 32; j++)
-          if (j < ncol) cp[(int64_t)j * pr.ldc] = cv[j] - __uint_as_float(v[j]);
+          for (int j = 0; j < 32; j++)
+            if (j < ncol)
+              atomicAdd(prow + (int64_t)rel[colbase + j] * pr.pld,
+                        cv[j] - __uint_as_float(v[j]));
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; j++)
+            if (j < ncol) cp[(int64_t)j * pr.ldc] = cv[j] - __uint_as_float(v[j]);
+        }
       }
     }
   }

@@ -28,6 +28,11 @@ struct GemmProb {
   int m, n, k;
   int lda, ldb, ldc;
   int64_t a, b, c;  // element offsets from the A, B, C base pointers
+  // Schur updates scatter into the parent instead of writing C:
+  // parent[rel[i] + rel[j] * pld] += C[i, j] - (A B)[i, j]  (pc >= 0;
+  // pc = the parent's offset, rel = offset of the child's map in rel_base)
+  int64_t pc = -1, rel = 0;
+  int pld = 0, pad = 0;
 };
 
 struct GemmTile {
@@ -88,7 +93,8 @@ template <typename T, int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
     k_gemm(const GemmTile* __restrict__ tiles,
            const GemmProb* __restrict__ probs, const T* __restrict__ Abase,
-           const T* __restrict__ Bbase, T* __restrict__ Cbase, int mode) {
+           const T* __restrict__ Bbase, T* __restrict__ Cbase, int mode,
+           const int* __restrict__ rel_base) {
   constexpr int NX = BM / TM, NY = BN / TN, NT = NX * NY;
   __shared__ T As[BK][BM + 1];
   __shared__ T Bs[BK][BN + 1];
@@ -128,6 +134,7 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
     }
     __syncthreads();
   }
+  const int* rel = rel_base + P.rel;
 #pragma unroll
   for (int j = 0; j < TN; j++) {
     int gj = n0 + ty + j * NY;
@@ -137,7 +144,11 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
       int gi = m0 + tx + i * NX;
       if (gi >= P.m) continue;
       T* c = C + gi + (int64_t)gj * P.ldc;
-      *c = mode ? acc[i][j] : *c - acc[i][j];
+      if (P.pc >= 0)  // extend-add fused: the update goes to the parent
+        atomicAdd(Cbase + P.pc + rel[gi] + (int64_t)rel[gj] * P.pld,
+                  *c - acc[i][j]);
+      else
+        *c = mode ? acc[i][j] : *c - acc[i][j];
     }
   }
 }

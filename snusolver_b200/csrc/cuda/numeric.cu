@@ -732,6 +732,7 @@ class CudaEngine : public Engine {
       t.m = g.m, t.n = g.n, t.k = g.k, t.kpad = (g.k + TC_BK - 1) / TC_BK * TC_BK;
       t.a = g.a, t.b = g.b, t.c = g.c;
       t.lda = g.lda, t.ldb = g.ldb, t.ldc = g.ldc;
+      t.pc = g.pc, t.rel = g.rel, t.pld = g.pld, t.pad = 0;
       t.apack = apos;
       apos += (int64_t)g.m * 3 * t.kpad;
       apos = (apos + 63) / 64 * 64;
@@ -918,10 +919,16 @@ class CudaEngine : public Engine {
       std::vector<GemmProb> f22;
       for (int f = L.f0; f < L.f1; f++) {
         const FrontInfo& fi = fp.fronts[f];
-        if (fi.p == 0 || fi.q == 0) continue;
+        // (a front without pivots passes its update matrix on: k = 0)
+        if (fi.q == 0) continue;
         int64_t o = fi.offset, ld = fi.ld;
-        f22.push_back({fi.q, fi.q, fi.p, fi.ld, fi.ld, fi.ld, o + fi.p,
-                       o + fi.p * ld, o + fi.p + fi.p * ld});
+        GemmProb g{fi.q, fi.q, fi.p, fi.ld, fi.ld, fi.ld, o + fi.p,
+                   o + fi.p * ld, o + fi.p + fi.p * ld};
+        const FrontInfo& par = fp.fronts[fi.parent];
+        g.pc = par.offset;
+        g.pld = par.ld;
+        g.rel = fi.rel_offset;
+        f22.push_back(g);
       }
       if ((rc = gemm_batch(f22, L.f22))) return rc;
       // solve sweeps; fronts with the longest tile chains first
@@ -1006,7 +1013,7 @@ class CudaEngine : public Engine {
     if (gb.ntiles == 0) return ENG_OK;
     int pi = prof_begin(fam, st);
     k_gemm<T, GBM, GBN, 16, 4, 4><<<gb.ntiles, 256, 0, st>>>(
-        gb.tiles, gb.probs, A, B, C, mode);
+        gb.tiles, gb.probs, A, B, C, mode, d_rel_);
     CKL();
     prof_end(pi, fam, st, gb.flops, gb.elems * sizeof(T));
     return ENG_OK;
@@ -1028,11 +1035,12 @@ class CudaEngine : public Engine {
     k_tc_pack_b<<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
     CKL();
     k_gemm_tc<<<gb.ntct, 128, tc_smem_bytes(), st>>>(gb.tct, gb.tcp, gb.amaps,
-                                                    gb.bmaps, F, d_flags_ + 2);
+                                                    gb.bmaps, F, d_flags_ + 2,
+                                                    d_rel_);
     CKL();
     if (gb.nrtiles) {
       k_gemm<float, GBM, GBN, 16, 4, 4><<<gb.nrtiles, 256, 0, st>>>(
-          gb.rtiles, gb.rprobs, F, F, F, 0);
+          gb.rtiles, gb.rprobs, F, F, F, 0, d_rel_);
       CKL();
     }
     prof_end(pi, fam, st, gb.flops, gb.elems * sizeof(float));
@@ -1044,30 +1052,24 @@ class CudaEngine : public Engine {
     cudaStream_t st = stream_;
     const double es = sizeof(T);
     int rc;
+    // every front zeroed and assembled first: children's Schur updates add
+    // into their parents directly (extend-add fused into the Schur GEMM)
+    {
+      const int64_t na = fp_->asm_level[nlevels_];
+      int pi = prof_begin(KF_ASSEMBLE, st);
+      CK(cudaMemsetAsync(F, 0, sizeof(T) * arena_, st));
+      if (na > 0) {
+        int blocks = (int)std::min<int64_t>((na + 255) / 256, 148 * 16);
+        k_assemble<T><<<blocks, 256, 0, st>>>(d_asm_pos_, d_asm_val_, d_vals_,
+                                              F, na);
+        CKL();
+      }
+      prof_end(pi, KF_ASSEMBLE, st, 0, es * arena_ + (20.0 + es) * na);
+    }
     for (int l = 0; l < nlevels_; l++) {
       LevelSched& L = lv_[l];
       cur_level_ = l;
-      int64_t na = L.asm1 - L.asm0;
-      int pi = prof_begin(KF_ASSEMBLE, st);
-      if (L.mem1 > L.mem0)
-        CK(cudaMemsetAsync(F + L.mem0, 0, sizeof(T) * (L.mem1 - L.mem0), st));
-      if (na > 0) {
-        int blocks = (int)std::min<int64_t>((na + 255) / 256, 148 * 16);
-        k_assemble<T><<<blocks, 256, 0, st>>>(d_asm_pos_ + L.asm0,
-                                              d_asm_val_ + L.asm0, d_vals_, F,
-                                              na);
-        CKL();
-      }
-      prof_end(pi, KF_ASSEMBLE, st, 0,
-               es * (L.mem1 - L.mem0) + (20.0 + es) * na);
-      for (size_t r = 0; r < L.ea.size(); r++) {
-        if (!L.nea[r]) continue;
-        pi = prof_begin(KF_EXTEND_ADD, st);
-        k_extend_add<T><<<L.nea[r], 128, 0, st>>>(L.ea[r], d_fr_, d_rel_, F);
-        CKL();
-        prof_end(pi, KF_EXTEND_ADD, st, L.ea_elems[r],
-                 L.ea_elems[r] * (3 * es + 4));
-      }
+      int pi;
       for (Step& S : L.steps) {
         pi = prof_begin(KF_DIAG_LU, st);
         k_diag_lu_inv<T><<<S.nactive, 256, diag_smem<T>(), st>>>(

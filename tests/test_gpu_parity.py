@@ -148,7 +148,9 @@ def test_multiple_rhs_and_refactor(gpu):
     s.refactor(v2)
     X2 = s.solve(B)
     fresh = snu.Solver(nleaves=8).construct(rp, ci, v2).factorize()
-    _close(X2, fresh.solve(B), 1e-13, "refactor vs fresh")
+    # sibling fronts add their updates into a parent with atomics, so two
+    # factorizations of the same values agree to rounding, not bit for bit
+    _close(X2, fresh.solve(B), 1e-11, "refactor vs fresh")
     for r in range(5):
         assert rel_resid(rp, ci, v2, X2[:, r], B[:, r]) <= 1e-12
 
