@@ -86,7 +86,9 @@ typedef struct snu_stats {
   int fp64_fallback;        /* 1 if the last solve fell back to FP64 factors */
   double backward_error;    /* last solve: max over columns of the relative residual */
   int tiny_pivots;          /* leaf pivots replaced by +-pivot_eps */
-  int reserved[7];
+  int factor_launches;      /* kernels of the last factorization */
+  int solve_launches;       /* kernels of the last solve (all chunks) */
+  int reserved[5];
 } snu_stats;
 
 typedef struct snu_handle snu_handle;

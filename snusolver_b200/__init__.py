@@ -60,7 +60,8 @@ class _Stats(C.Structure):
                 ("solve_s", C.c_double), ("factor_flops", C.c_double),
                 ("ir_iters", C.c_int), ("fp64_fallback", C.c_int),
                 ("backward_error", C.c_double), ("tiny_pivots", C.c_int),
-                ("reserved", C.c_int * 7)]
+                ("factor_launches", C.c_int), ("solve_launches", C.c_int),
+                ("reserved", C.c_int * 5)]
 
 
 class _KStat(C.Structure):

@@ -251,6 +251,11 @@ SNU_API snu_status snu_factorize(snu_handle* h) {
     return from_engine(h, rc);
   }
   h->stats.factor_s = sec;
+  {
+    int64_t fl = 0, sl = 0;
+    h->eng->launch_counts(&fl, &sl);
+    h->stats.factor_launches = (int)fl;
+  }
   h->state = 3;
   return SNU_OK;
 }
@@ -281,6 +286,11 @@ SNU_API snu_status snu_solve_device(snu_handle* h, const double* dB,
   h->stats.fp64_fallback = rep.fp64_fallback;
   h->stats.backward_error = rep.backward_error;
   h->stats.device_bytes = h->eng->device_bytes();
+  {
+    int64_t fl = 0, sl = 0;
+    h->eng->launch_counts(&fl, &sl);
+    h->stats.solve_launches = (int)sl;
+  }
   if (prec == 1 && !(rep.backward_error <= h->opts.ir_tol))
     return fail(h, SNU_ENOTCONV,
                 "refinement stopped at backward error " +

@@ -63,6 +63,7 @@ namespace {
 
 #define CKL()                                                            \
   do {                                                                   \
+    ++launches_;                                                         \
     cudaError_t e_ = cudaGetLastError();                                 \
     if (e_ != cudaSuccess) {                                             \
       err_ = std::string("kernel launch: ") + cudaGetErrorString(e_);    \
@@ -182,6 +183,8 @@ class CudaEngine : public Engine {
     {
       const char* e = getenv("SNU_TC_GEMM");
       use_tc_ = !(e && e[0] == '0');
+      const char* g = getenv("SNU_GRAPHS");
+      use_graphs_ = !(g && g[0] == '0');
     }
     {
       int rc2;
@@ -219,6 +222,10 @@ class CudaEngine : public Engine {
     trace_.clear();
   }
   const std::vector<LaunchRec>& trace() const override { return trace_; }
+  void launch_counts(int64_t* factor, int64_t* solve) const override {
+    *factor = last_factor_launches_;
+    *solve = last_solve_launches_;
+  }
   int64_t device_bytes() const override { return bytes_; }
   int tiny_pivots() const override { return tiny_; }
 
@@ -350,9 +357,40 @@ class CudaEngine : public Engine {
     }
     CK(cudaMemsetAsync(d_flags_, 0, 4 * sizeof(int), stream_));
     CK(cudaEventRecord(ev0_, stream_));
-    rc = precision == 0 ? run_factor<double>(d_F64_, d_I64_)
-                        : run_factor<float>(d_F32_, d_I32_);
-    if (rc) return rc;
+    const int64_t l0 = launches_;
+    if (use_graphs_ && !prof_mask_ && stream_) {
+      // the schedule is fixed after set-up: captured once per precision and
+      // replayed (one launch instead of ~1000)
+      cudaGraphExec_t& ex = factor_graph_[precision ? 1 : 0];
+      if (!ex) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        rc = precision == 0 ? run_factor<double>(d_F64_, d_I64_)
+                            : run_factor<float>(d_F32_, d_I32_);
+        cudaError_t ce = cudaStreamEndCapture(stream_, &g);
+        if (rc) {
+          if (g) cudaGraphDestroy(g);
+          return rc;
+        }
+        CK(ce);
+        cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+          cudaGetLastError();
+          ex = nullptr;
+          err_ = std::string("graph instantiate: ") + cudaGetErrorString(ie);
+          return ENG_ECUDA;
+        }
+      }
+      if (launches_ > l0) graph_launches_[precision ? 1 : 0] = launches_ - l0;
+      CK(cudaGraphLaunch(ex, stream_));
+      last_factor_launches_ = graph_launches_[precision ? 1 : 0];
+    } else {
+      rc = precision == 0 ? run_factor<double>(d_F64_, d_I64_)
+                          : run_factor<float>(d_F32_, d_I32_);
+      if (rc) return rc;
+      last_factor_launches_ = launches_ - l0;
+    }
     CK(cudaEventRecord(ev1_, stream_));
     int flags[4];
     CK(cudaMemcpyAsync(flags, d_flags_, sizeof flags, cudaMemcpyDeviceToHost,
@@ -409,6 +447,7 @@ class CudaEngine : public Engine {
     cudaStream_t st = stream ? (cudaStream_t)stream : stream_;
     int rc;
     if ((rc = ensure_solve(nrhs, precision == 0))) return rc;
+    const int64_t l0 = launches_;
     bnorm_.clear();
     CK(cudaMemsetAsync(d_flags_ + 4, 0, sizeof(int), st));
     CK(cudaEventRecord(sev0_, st));
@@ -422,6 +461,7 @@ class CudaEngine : public Engine {
       if ((rc = refine(dB, ldb, dX, ldb, nrhs, st, &r))) return rc;
     }
     CK(cudaEventRecord(sev1_, st));
+    last_solve_launches_ = launches_ - l0;
     if ((rc = sweep_status(st))) return rc;
     prof_collect();
     float ms = 0;
@@ -555,6 +595,7 @@ class CudaEngine : public Engine {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int* fl = d_tflags_ + (fwd ? 0 : ntileflags_);
+    ++launches_;
     CK(cudaLaunchKernelEx(&cfg, k, tasks, ntasks, (const FrontDev*)d_fr_, F, I,
                           (const int64_t*)d_flag_off_, nrhs, W, Y, fl,
                           d_flags_ + 4));
@@ -666,6 +707,11 @@ class CudaEngine : public Engine {
   }
   void release() {
     if (stream_) cudaStreamSynchronize(stream_);
+    for (auto& ex : factor_graph_)
+      if (ex) {
+        cudaGraphExecDestroy(ex);
+        ex = nullptr;
+      }
     for (void* p : ptrs_) cudaFree(p);
     ptrs_.clear();
     sizes_.clear();
@@ -1412,6 +1458,11 @@ class CudaEngine : public Engine {
   int64_t pack_need_ = 0;
   std::vector<GemmBatch*> tc_batches_;
   bool use_tc_ = true;
+  bool use_graphs_ = true;
+  int64_t launches_ = 0;  // kernels launched (counted at every launch site)
+  int64_t graph_launches_[2] = {0, 0};
+  int64_t last_factor_launches_ = 0, last_solve_launches_ = 0;
+  cudaGraphExec_t factor_graph_[2] = {nullptr, nullptr};
   double* d_I64_ = nullptr;  // diagonal-tile inverses (FP64 factors)
   float* d_I32_ = nullptr;   // diagonal-tile inverses (FP32 factors)
   double* d_Y64_ = nullptr;

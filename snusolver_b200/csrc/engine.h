@@ -72,6 +72,8 @@ class Engine {
   virtual void reset_profile() = 0;
   // Per-launch records kept while the trace bit (1u << 31) is set.
   virtual const std::vector<LaunchRec>& trace() const = 0;
+  // Kernels launched by the last factorization and the last solve.
+  virtual void launch_counts(int64_t* factor, int64_t* solve) const = 0;
   // Stream for all work of the handle (nullptr: the engine's own stream).
   virtual int set_stream(void* stream) = 0;
   virtual void* stream() const = 0;  // the stream work goes to
