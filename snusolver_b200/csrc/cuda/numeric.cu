@@ -13,6 +13,7 @@
 
 #include "../engine.h"
 #include "kernels.cuh"
+#include "panel_block.cuh"
 #include "panel.cuh"
 #include "sweep.cuh"
 #include "gemm_tc.cuh"
@@ -113,7 +114,18 @@ struct Step {
   double panel_flops = 0, panel_elems = 0;  // L / U panel solves
 };
 
+// One outer block of a level on the fused path: the cooperative panel
+// kernel's tasks and the rank-(K1-K0) update of the rest.
+struct OuterBlock {
+  int K0 = 0;
+  BlockTask* tasks = nullptr;
+  int ntasks = 0;
+  GemmBatch outer;
+  double flops = 0, elems = 0;
+};
+
 struct LevelSched {
+  std::vector<OuterBlock> ob;
   int f0 = 0, f1 = 0;  // fronts [f0, f1)
   int64_t mem0 = 0, mem1 = 0;
   int64_t asm0 = 0, asm1 = 0;
@@ -145,7 +157,7 @@ struct LevelSched {
 
 constexpr int GBM = 64, GBN = 64;
 // outer block of the two-level blocked partial LU (a multiple of NB)
-constexpr int OB = 256;
+constexpr int OB = OB_COLS;
 
 #define SNU_LAUNCH_(K, T, R, CFG, ARGS) K<T, R><<<SNU_UNPACK CFG>>> ARGS
 #define SNU_UNPACK(...) __VA_ARGS__
@@ -185,6 +197,8 @@ class CudaEngine : public Engine {
       use_tc_ = !(e && e[0] == '0');
       const char* g = getenv("SNU_GRAPHS");
       use_graphs_ = !(g && g[0] == '0');
+      const char* pbk = getenv("SNU_PANEL_BLOCK");
+      use_block_ = !(pbk && pbk[0] == '0');
     }
     {
       int rc2;
@@ -194,6 +208,14 @@ class CudaEngine : public Engine {
           (rc2 = sweep_attr<float, 2>()) || (rc2 = sweep_attr<float, 4>()) ||
           (rc2 = sweep_attr<float, 8>()) || (rc2 = sweep_attr<float, 16>()))
         return rc2;
+    }
+    {
+      int sms = 0;
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount,
+                                opt_.device));
+      int rc3;
+      if ((rc3 = block_attr<double>(sms)) || (rc3 = block_attr<float>(sms)))
+        return rc3;
     }
     CK(cudaFuncSetAttribute(k_panel_apply<double>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -280,6 +302,7 @@ class CudaEngine : public Engine {
       ntileflags_ = std::max<int64_t>(acc, 1);
       if ((rc = upload(d_flag_off_, fo))) return rc;
       if ((rc = alloc(d_tflags_, (size_t)(2 * ntileflags_)))) return rc;
+      if ((rc = alloc(d_fflags_, (size_t)ntileflags_))) return rc;
     }
     if ((rc = upload(d_fr_, frh_))) return rc;
     if ((rc = upload(d_gidx_, fp.gidx))) return rc;
@@ -356,6 +379,7 @@ class CudaEngine : public Engine {
       if (!d_I32_ && (rc = alloc(d_I32_, (size_t)invtot_))) return rc;
     }
     CK(cudaMemsetAsync(d_flags_, 0, 4 * sizeof(int), stream_));
+    CK(cudaMemsetAsync(d_flags_ + 5, 0, sizeof(int), stream_));
     CK(cudaEventRecord(ev0_, stream_));
     const int64_t l0 = launches_;
     if (use_graphs_ && !prof_mask_ && stream_) {
@@ -392,7 +416,7 @@ class CudaEngine : public Engine {
       last_factor_launches_ = launches_ - l0;
     }
     CK(cudaEventRecord(ev1_, stream_));
-    int flags[4];
+    int flags[8];
     CK(cudaMemcpyAsync(flags, d_flags_, sizeof flags, cudaMemcpyDeviceToHost,
                        stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -407,6 +431,10 @@ class CudaEngine : public Engine {
       have32_ = true;
     if (flags[2]) {
       err_ = "tensor-core GEMM pipeline wait timed out";
+      return ENG_ETIMEOUT;
+    }
+    if (flags[5]) {
+      err_ = "panel kernel wait for a diagonal tile timed out";
       return ENG_ETIMEOUT;
     }
     if (flags[1]) {
@@ -559,6 +587,43 @@ class CudaEngine : public Engine {
   }
 
  private:
+  template <typename T>
+  int block_attr(int sms) {
+    auto k = k_panel_block<T>;
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)block_smem<T>()));
+    int nb = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 256,
+                                                     block_smem<T>()));
+    if (nb < 1) {
+      err_ = "panel kernel does not fit on an SM";
+      return ENG_ECUDA;
+    }
+    coop_cap_[(const void*)k] = nb * sms;
+    return ENG_OK;
+  }
+  // One cooperative launch of the fused panel kernel for an outer block.
+  template <typename T>
+  int block_launch(const OuterBlock& O, T* F, T* I, cudaStream_t st) {
+    auto k = k_panel_block<T>;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(std::min(O.ntasks, coop_cap_[(const void*)k]));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = block_smem<T>();
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    ++launches_;
+    CK(cudaLaunchKernelEx(&cfg, k, (const BlockTask*)O.tasks, O.ntasks,
+                          (const FrontDev*)d_fr_, F, I, O.K0, opt_.pivot_eps,
+                          d_flags_, d_fflags_, (const int64_t*)d_flag_off_,
+                          d_flags_ + 5));
+    return ENG_OK;
+  }
+
   template <typename T, int R>
   int sweep_attr() {
     int sms = 0;
@@ -977,6 +1042,50 @@ class CudaEngine : public Engine {
         f22.push_back(g);
       }
       if ((rc = gemm_batch(f22, L.f22))) return rc;
+      // fused path: per outer block the cooperative panel tasks and the
+      // rank-(K1-K0) update of the rest of the pivot rows and columns
+      const int nob = (maxp + OB - 1) / OB;
+      L.ob.assign(nob, OuterBlock());
+      for (int b = 0; b < nob; b++) {
+        OuterBlock& O = L.ob[b];
+        O.K0 = b * OB;
+        std::vector<BlockTask> bt;
+        std::vector<GemmProb> og;
+        int maxrows = 0;
+        for (int f = L.f0; f < L.f1; f++) {
+          const FrontInfo& fi = fp.fronts[f];
+          if (fi.p > O.K0)
+            maxrows = std::max(maxrows, (fi.p + fi.q - O.K0 + NB - 1) / NB);
+        }
+        for (int r = 0; r < maxrows; r++)
+          for (int f = L.f0; f < L.f1; f++) {
+            const FrontInfo& fi = fp.fronts[f];
+            if (fi.p > O.K0 && O.K0 + r * NB < fi.p + fi.q) bt.push_back({f, 0, r});
+          }
+        for (int f = L.f0; f < L.f1; f++) {
+          const FrontInfo& fi = fp.fronts[f];
+          if (fi.p <= O.K0) continue;
+          const int K0 = O.K0, K1 = std::min(K0 + OB, fi.p), dim = fi.p + fi.q;
+          for (int c = 0; K1 + c * NB < dim; c++) bt.push_back({f, 1, c});
+          const int64_t o = fi.offset, ld = fi.ld;
+          const int kk = K1 - K0;
+          if (dim - K1 > 0 && fi.p - K1 > 0)  // rows K1..dim, cols K1..p
+            og.push_back({dim - K1, fi.p - K1, kk, fi.ld, fi.ld, fi.ld,
+                          o + K1 + K0 * ld, o + K0 + K1 * ld, o + K1 + K1 * ld});
+          if (fi.p - K1 > 0 && fi.q > 0)  // rows K1..p, cols p..dim
+            og.push_back({fi.p - K1, fi.q, kk, fi.ld, fi.ld, fi.ld,
+                          o + K1 + K0 * ld, o + K0 + fi.p * ld,
+                          o + K1 + fi.p * ld});
+          // diagonal tiles + L blocks + in-block updates + U12 blocks
+          const double rows = dim - K0, cols = dim - K1;
+          O.flops += kk * (2.0 / 3.0 * NB * NB + 2.0 * rows * NB) +
+                     2.0 * rows * kk * kk / 2 + 2.0 * cols * kk * kk;
+          O.elems += 2.0 * rows * kk + 2.0 * cols * kk;
+        }
+        O.ntasks = (int)bt.size();
+        if (!bt.empty() && (rc = upload(O.tasks, bt))) return rc;
+        if ((rc = gemm_batch(og, O.outer))) return rc;
+      }
       // solve sweeps; fronts with the longest tile chains first
       std::vector<int> byp;
       for (int f = L.f0; f < L.f1; f++)
@@ -1104,6 +1213,7 @@ class CudaEngine : public Engine {
       const int64_t na = fp_->asm_level[nlevels_];
       int pi = prof_begin(KF_ASSEMBLE, st);
       CK(cudaMemsetAsync(F, 0, sizeof(T) * arena_, st));
+      CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * ntileflags_, st));
       if (na > 0) {
         int blocks = (int)std::min<int64_t>((na + 255) / 256, 148 * 16);
         k_assemble<T><<<blocks, 256, 0, st>>>(d_asm_pos_, d_asm_val_, d_vals_,
@@ -1116,6 +1226,18 @@ class CudaEngine : public Engine {
       LevelSched& L = lv_[l];
       cur_level_ = l;
       int pi;
+      if (use_block_) {
+        for (const OuterBlock& O : L.ob) {
+          if (O.ntasks) {
+            pi = prof_begin(KF_PANEL_BLOCK, st);
+            if ((rc = block_launch<T>(O, F, I, st))) return rc;
+            prof_end(pi, KF_PANEL_BLOCK, st, O.flops, O.elems * es);
+          }
+          if ((rc = factor_gemm(O.outer, F, st, KF_GEMM_TRAIL))) return rc;
+        }
+        if ((rc = factor_gemm(L.f22, F, st, KF_GEMM_SCHUR))) return rc;
+        continue;
+      }
       for (Step& S : L.steps) {
         pi = prof_begin(KF_DIAG_LU, st);
         k_diag_lu_inv<T><<<S.nactive, 256, diag_smem<T>(), st>>>(
@@ -1450,6 +1572,7 @@ class CudaEngine : public Engine {
   // pivot-block sweep flags (forward, then backward) and per-front offsets
   int64_t* d_flag_off_ = nullptr;
   int* d_tflags_ = nullptr;
+  int* d_fflags_ = nullptr;  // diagonal tiles done (fused panel path)
   int64_t ntileflags_ = 0;
   // co-resident grid size of each pivot-block sweep kernel
   std::map<const void*, int> coop_cap_;
@@ -1459,6 +1582,7 @@ class CudaEngine : public Engine {
   std::vector<GemmBatch*> tc_batches_;
   bool use_tc_ = true;
   bool use_graphs_ = true;
+  bool use_block_ = true;  // fused outer-block panels (else per-step kernels)
   int64_t launches_ = 0;  // kernels launched (counted at every launch site)
   int64_t graph_launches_[2] = {0, 0};
   int64_t last_factor_launches_ = 0, last_solve_launches_ = 0;
@@ -1502,7 +1626,8 @@ class CudaEngine : public Engine {
 const char* kernel_family_name(int f) {
   static const char* names[KF_COUNT] = {
       "assemble", "extend_add", "diag_lu", "panel_trsm", "gemm_trail",
-      "gemm_schur", "solve_diag", "solve_gemm", "solve_misc", "residual"};
+      "gemm_schur", "solve_diag", "solve_gemm", "solve_misc", "residual",
+      "panel_block"};
   return (f >= 0 && f < KF_COUNT) ? names[f] : "?";
 }
 

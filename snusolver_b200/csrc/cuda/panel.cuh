@@ -81,19 +81,17 @@ __device__ __forceinline__ void inv_distance(const T* D, T* XL, T* XU,
   __syncthreads();
 }
 
+// The tile factorization of one front by the whole CTA (256 threads); D,
+// XL, XU: 3 NB x TLD shared-memory tiles.  On return XL / XU hold Linv /
+// Uinv (also written to INV) and the factored tile is back in F.
 template <typename T>
-__global__ void __launch_bounds__(256)
-    k_diag_lu_inv(const int* __restrict__ active,
-                  const FrontDev* __restrict__ fr, T* __restrict__ F,
-                  T* __restrict__ INV, int k0, int step, double eps,
-                  int* flags) {
-  extern __shared__ unsigned char smem_raw[];
-  T* D = reinterpret_cast<T*>(smem_raw);
-  T* XL = D + NB * TLD;
-  T* XU = XL + NB * TLD;
+__device__ __forceinline__ void diag_tile(const FrontDev& f,
+                                          T* __restrict__ F,
+                                          T* __restrict__ INV, int k0,
+                                          int step, double eps, int* flags,
+                                          T* D, T* XL, T* XU) {
   __shared__ T rdiag[NB];  // 1 / U[i][i]
   __shared__ T Tb[6][SB][SB + 1];
-  const FrontDev f = fr[active[blockIdx.x]];
   const int kb = min(NB, f.p - k0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   T* base = F + f.off + k0 + (int64_t)k0 * f.ld;
@@ -241,6 +239,19 @@ __global__ void __launch_bounds__(256)
     inv[e] = XL[i + j * TLD];
     inv[NB * NB + e] = XU[i + j * TLD];
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_diag_lu_inv(const int* __restrict__ active,
+                  const FrontDev* __restrict__ fr, T* __restrict__ F,
+                  T* __restrict__ INV, int k0, int step, double eps,
+                  int* flags) {
+  extern __shared__ unsigned char smem_raw[];
+  T* D = reinterpret_cast<T*>(smem_raw);
+  const FrontDev f = fr[active[blockIdx.x]];
+  diag_tile<T>(f, F, INV, k0, step, eps, flags, D, D + NB * TLD,
+               D + 2 * NB * TLD);
 }
 
 // Dynamic shared memory of k_panel_apply: the panel tile and the inverse.

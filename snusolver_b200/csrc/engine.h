@@ -48,6 +48,7 @@ enum KernelFamily {
   KF_SOLVE_GEMM,     // GEMM updates of the sweeps
   KF_SOLVE_MISC,     // gathers, scatters and extend-adds of the sweeps
   KF_RESIDUAL,       // FP64 residual, norms and solution updates
+  KF_PANEL_BLOCK,    // fused outer-block panels (tiles, L/U blocks, updates)
   KF_COUNT
 };
 const char* kernel_family_name(int f);
