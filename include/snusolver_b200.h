@@ -309,6 +309,14 @@ SNU_API snu_status snu_read_mtx(const char* path, int expand_symmetric,
                                 double** vals);
 SNU_API void snu_free(void* p);
 
+/* ---- self-test (no reference counterpart) ---- */
+/* Every device-side wait of this library (inter-block flags, mbarriers) is
+   bounded: after its iteration limit it records an error, the kernel
+   returns and the call reports SNU_ETIMEOUT.  This runs one such wait on a
+   flag that nothing sets and returns its status: SNU_ETIMEOUT (after well
+   under a second) is the expected answer; the device stays usable. */
+SNU_API snu_status snu_selftest_wait_timeout(int device);
+
 #ifdef __cplusplus
 }
 #endif

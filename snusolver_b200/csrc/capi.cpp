@@ -13,6 +13,16 @@
 
 #include "handle.h"
 
+// NVTX ranges around the phases (header-only; visible in Nsight tools)
+#include <nvtx3/nvToolsExt.h>
+
+namespace {
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+}  // namespace
+
 // CUDA runtime calls used directly here (host staging for snu_solve).
 #include <cuda_runtime_api.h>
 
@@ -127,6 +137,7 @@ SNU_API const char* snu_last_error(const snu_handle* h) {
 
 SNU_API snu_status snu_analyze(snu_handle* h, int n, int nnz,
                                const int* rowptr, const int* colidx) {
+  NvtxRange r("snu_analyze");
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
   std::string why;
   if (!valid_csr(n, nnz, rowptr, colidx, why)) return fail(h, SNU_EINVAL, why);
@@ -239,6 +250,7 @@ SNU_API snu_status snu_construct_batch(snu_handle* h, int nmat,
 }
 
 SNU_API snu_status snu_factorize(snu_handle* h) {
+  NvtxRange r("snu_factorize");
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
   if (h->state < 2) return fail(h, SNU_ESTATE, "factorize before construct");
   double sec = 0;
@@ -277,6 +289,7 @@ SNU_API snu_status snu_solve_device(snu_handle* h, const double* dB,
   if (h->state < 3) return fail(h, SNU_ESTATE, "solve before factorize");
   if (!dB || !dX || nrhs <= 0 || ldb < h->S.n)
     return fail(h, SNU_EINVAL, "bad right-hand side arguments");
+  NvtxRange r("snu_solve_device");
   snu::SolveReport rep;
   int prec = h->opts.precision == SNU_FP64 ? 0 : 1;
   int rc = h->eng->solve(dB, dX, nrhs, ldb, stream, prec, &rep);
@@ -553,11 +566,24 @@ SNU_API snu_status snu_read_mtx(const char* path, int expand_symmetric,
 
 SNU_API void snu_free(void* p) { std::free(p); }
 
+SNU_API snu_status snu_selftest_wait_timeout(int device) {
+  std::string err;
+  int rc = snu::wait_selftest(device, err);
+  g_err = err;
+  switch (rc) {
+    case snu::ENG_OK: return SNU_OK;
+    case snu::ENG_ETIMEOUT: return SNU_ETIMEOUT;
+    case snu::ENG_ENOMEM: return SNU_ENOMEM;
+    default: return SNU_ECUDA;
+  }
+}
+
 }  // extern "C"
 
 namespace snu {
 
 snu_status finish_construct(snu_handle* h, const double* vals, bool have_plan) {
+  NvtxRange r("snu_construct_device");
   double t0 = now_s();
   std::string err;
   if (!have_plan) {

@@ -1623,6 +1623,42 @@ class CudaEngine : public Engine {
 
 }  // namespace
 
+// Self-test of the bounded device waits: one block waits on a flag that
+// nothing sets; the wait gives up after its iteration limit and records the
+// timeout, and the kernel returns normally.
+__global__ void k_wait_selftest(const int* flag, int* err) {
+  if (threadIdx.x == 0) wait_flag(flag, err);
+}
+
+int wait_selftest(int device, std::string& err) {
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    err = "cannot select the device";
+    return ENG_ECUDA;
+  }
+  int* d = nullptr;
+  if (cudaMalloc((void**)&d, 2 * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    err = "cudaMalloc failed";
+    return ENG_ENOMEM;
+  }
+  int h[2] = {0, 0};
+  cudaMemset(d, 0, 2 * sizeof(int));
+  k_wait_selftest<<<1, 32>>>(d, d + 1);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    err = cudaGetErrorString(e);
+    return ENG_ECUDA;
+  }
+  if (h[1]) {
+    err = "wait on an unset flag gave up after its iteration limit";
+    return ENG_ETIMEOUT;
+  }
+  return ENG_OK;
+}
+
 const char* kernel_family_name(int f) {
   static const char* names[KF_COUNT] = {
       "assemble", "extend_add", "diag_lu", "panel_trsm", "gemm_trail",

@@ -52,6 +52,9 @@ enum KernelFamily {
   KF_COUNT
 };
 const char* kernel_family_name(int f);
+// Runs the bounded-wait self-test on a device (ENG_ETIMEOUT when the wait
+// ran out as it must).
+int wait_selftest(int device, std::string& err);
 
 struct KernelStat {
   int64_t launches = 0;

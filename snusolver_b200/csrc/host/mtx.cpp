@@ -73,6 +73,11 @@ int read_mtx(const char* path, Csr& A, bool expand_symmetric, std::string& err) 
     err = "bad MatrixMarket size line";
     return HOST_EINVAL;
   }
+  if (M != N) {  // only square systems are solved (the CSR keeps n = rows)
+    std::fclose(f);
+    err = "MatrixMarket matrix is not square";
+    return HOST_EINVAL;
+  }
   std::vector<int> I, J;
   std::vector<double> V;
   I.reserve(nz), J.reserve(nz), V.reserve(nz);

@@ -90,3 +90,18 @@ def test_duplicates_analyzed_but_rejected_numerically():
         snu.Solver(nleaves=2).construct(rp2, ci2, v2)
     assert e.value.status == 1
     assert "duplicate" in str(e.value)
+
+
+@pytest.mark.parametrize("body,why", [
+    ("3 3 4\n1 1 2\n2 2 3\n", "truncated"),
+    ("3 3 2\n1 1 2\n4 2 3\n", "out of range"),
+    ("3 3 2\n1 1 abc\n2 2 3\n", "truncated"),
+    ("3 2 2\n1 1 1\n2 2 3\n", "not square"),
+    ("x y z\n", "size line"),
+])
+def test_read_mtx_rejects_corrupt_files(tmp_path, body, why):
+    p = tmp_path / "bad.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate real general\n" + body)
+    with pytest.raises(snu.SnuError) as e:
+        snu.read_matrix(str(p))
+    assert e.value.status == 1 and why in str(e.value)
