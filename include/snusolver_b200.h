@@ -158,6 +158,16 @@ SNU_API snu_status snu_solve_device_noalloc(snu_handle* h, const double* dB,
    handle's own stream).  Takes effect now, or at snu_construct. */
 SNU_API snu_status snu_set_stream(snu_handle* h, void* stream);
 
+/* Autotuner (no reference counterpart): at the next FP32 factorization,
+   time both tensor-core GEMM kernels (one CTA per tile / persistent and
+   warp-specialised) for every GEMM batch of the schedule -- two extra
+   factorizations -- and keep the faster one per batch.  cache_path (may be
+   NULL) is a text file of choices keyed by the sparsity pattern: a pattern
+   found there is not timed again.  Off by default (a per-batch heuristic
+   on the tiles' K picks the variant). */
+SNU_API snu_status snu_set_autotune(snu_handle* h, int enable,
+                                    const char* cache_path);
+
 typedef struct snu_kernel_stat {
   const char* name;   /* kernel family */
   int64_t launches;   /* launches timed */

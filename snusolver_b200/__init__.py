@@ -111,6 +111,7 @@ _EXPORTS = {
     "snu_free": (None, [C.c_void_p]),
     "snu_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "snu_set_profiling": (C.c_int, [C.c_void_p, C.c_uint]),
+    "snu_set_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p]),
     "snu_get_trace": (C.c_int, [C.c_void_p, C.POINTER(_LaunchRec), C.c_int,
                                 C.POINTER(C.c_int)]),
     "snu_get_profile": (C.c_int, [C.c_void_p, C.POINTER(_KStat), C.c_int,
@@ -269,6 +270,13 @@ class Solver:
     def set_stream(self, stream):
         """CUDA stream (integer handle, 0 = the handle's own) for all work."""
         self._check(self._lib.snu_set_stream(self._h, C.c_void_p(stream or None)))
+        return self
+
+    def set_autotune(self, enable=True, cache_path=None):
+        """Tune the tensor-core GEMM variant per batch at the next FP32
+        factorization (see ``snu_set_autotune``)."""
+        self._check(self._lib.snu_set_autotune(
+            self._h, int(enable), cache_path.encode() if cache_path else None))
         return self
 
     def set_profiling(self, families=(), trace=False):

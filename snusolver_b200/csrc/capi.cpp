@@ -58,6 +58,20 @@ double now_s() {
       .count();
 }
 
+// FNV-1a over the pattern and the leaf count: the autotuner's cache key.
+uint64_t pattern_key(const snu_handle* h) {
+  uint64_t k = 1469598103934665603ull;
+  auto mix = [&](const void* p, size_t bytes) {
+    const unsigned char* c = (const unsigned char*)p;
+    for (size_t i = 0; i < bytes; i++) k = (k ^ c[i]) * 1099511628211ull;
+  };
+  mix(&h->opts.nleaves, sizeof h->opts.nleaves);
+  mix(&h->batch, sizeof h->batch);
+  mix(h->rowptr.data(), h->rowptr.size() * sizeof(int));
+  mix(h->colidx.data(), h->colidx.size() * sizeof(int));
+  return k;
+}
+
 bool valid_csr(int n, int nnz, const int* rowptr, const int* colidx,
                std::string& why) {
   if (n <= 0) return why = "n must be positive", false;
@@ -399,6 +413,16 @@ SNU_API snu_status snu_set_stream(snu_handle* h, void* stream) {
   return SNU_OK;
 }
 
+SNU_API snu_status snu_set_autotune(snu_handle* h, int enable,
+                                    const char* cache_path) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  h->autotune = enable ? 1 : 0;
+  h->tune_path = cache_path ? cache_path : "";
+  if (h->eng) h->eng->set_autotune(enable != 0, h->tune_path.c_str(),
+                                   pattern_key(h));
+  return SNU_OK;
+}
+
 SNU_API snu_status snu_set_profiling(snu_handle* h, unsigned mask) {
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
   h->prof_mask = mask;
@@ -605,6 +629,8 @@ snu_status finish_construct(snu_handle* h, const double* vals, bool have_plan) {
   if (rc) return from_engine(h, rc);
   h->eng->set_profiling(h->prof_mask);
   rc = h->eng->setup(h->S, h->FP, h->rowptr.data(), h->colidx.data());
+  if (!rc && h->autotune)
+    h->eng->set_autotune(true, h->tune_path.c_str(), pattern_key(h));
   if (rc) return from_engine(h, rc);
   if (h->batch) {
     rc = h->eng->set_segments(h->batch_rows);

@@ -326,4 +326,197 @@ __global__ void __launch_bounds__(128, 1)
                  "r"(TC_BN));
 }
 
+// ------------------------------------------------------ persistent GEMM
+//
+// The same tiles, but each CTA loops over tiles (stride gridDim.x) with its
+// warps specialised: warp 0 issues the TMA loads through the stage ring,
+// warp 1 issues the MMAs, warps 2-5 run the epilogue.  Two TMEM
+// accumulators (2 x 128 columns) let the epilogue of tile i overlap the
+// MMAs of tile i+1; acc_full[a] (MMA -> epilogue, tcgen05.commit) and
+// acc_empty[a] (four epilogue warps -> MMA) hand each accumulator back and
+// forth.  Every wait is bounded; on a timeout the CTA raises a shared abort
+// flag, the other roles give up too, the MMA warp waits for its own MMAs
+// and the producer for its own loads before TMEM is freed.
+constexpr int TCP_THREADS = 192;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
+__global__ void __launch_bounds__(TCP_THREADS, 1)
+    k_gemm_tcp(const TcTile* __restrict__ tiles, int ntiles,
+               const TcProb* __restrict__ probs,
+               const CUtensorMap* __restrict__ amaps,
+               const CUtensorMap* __restrict__ bmaps, float* __restrict__ F,
+               int* err, const int* __restrict__ rel_base) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES];
+  __shared__ uint64_t acc_full[2], acc_empty[2], drain_bar;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ volatile int abort_s;
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  float* As = (float*)smem;
+  float* Bs = As + (size_t)TC_STAGES * TC_BM * TC_BK;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    abort_s = 0;
+    for (int s = 0; s < TC_STAGES; s++) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int a = 0; a < 2; a++) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], 4);
+    }
+    mbar_init(&drain_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile(
+        "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+            smem_addr(&tmem_base_s)),
+        "r"(2 * TC_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_s;
+
+  if (warp == 0 && lane == 0) {
+    // producer
+    int g = 0;
+    for (int t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x) {
+      const TcTile tl = tiles[t];
+      const TcProb pr = probs[tl.prob];
+      const CUtensorMap* am = amaps + tl.prob;
+      const CUtensorMap* bm = bmaps + tl.prob;
+      const int nk = 3 * pr.kpad / TC_BK;
+      for (int kb = 0; kb < nk; kb++, g++) {
+        const int s = g % TC_STAGES;
+        if (g >= TC_STAGES &&
+            !mbar_wait(&empty_bar[s], ((g / TC_STAGES) - 1) & 1, err)) {
+          abort_s = 1;
+          break;
+        }
+        mbar_expect_tx(&full_bar[s], (TC_BM + TC_BN) * TC_BK * sizeof(float));
+        tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * TC_BK,
+                    tl.tm * TC_BM, &full_bar[s]);
+        tma_load_2d(Bs + (size_t)s * TC_BN * TC_BK, bm, kb * TC_BK,
+                    tl.tn * TC_BN, &full_bar[s]);
+      }
+    }
+    // every issued load has landed before the CTA may exit
+    for (int q = g > TC_STAGES ? g - TC_STAGES : 0; q < g; q++)
+      mbar_wait(&full_bar[q % TC_STAGES], (q / TC_STAGES) & 1, err);
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    const uint32_t idesc = tc_idesc(TC_BN);
+    int g = 0, i = 0;
+    for (int t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x, i++) {
+      const int a = i & 1;
+      if (i >= 2 && !mbar_wait(&acc_empty[a], ((i >> 1) - 1) & 1, err)) {
+        abort_s = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const TcProb pr = probs[tiles[t].prob];
+      const int nk = 3 * pr.kpad / TC_BK;
+      const uint32_t d = tmem + (uint32_t)(a * TC_BN);
+      bool ok = true;
+      for (int kb = 0; kb < nk; kb++, g++) {
+        const int s = g % TC_STAGES;
+        if (!mbar_wait(&full_bar[s], (g / TC_STAGES) & 1, err)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_addr(As + (size_t)s * TC_BM * TC_BK);
+        const uint32_t b0 = smem_addr(Bs + (size_t)s * TC_BN * TC_BK);
+#pragma unroll
+        for (int kk = 0; kk < TC_BK / 8; kk++)
+          tc_mma(d, umma_desc(a0 + kk * 32), umma_desc(b0 + kk * 32), idesc,
+                 (kb > 0 || kk > 0) ? 1u : 0u);
+        tc_commit(&empty_bar[s]);
+      }
+      if (!ok) {
+        abort_s = 1;
+        break;
+      }
+      tc_commit(&acc_full[a]);
+    }
+    // all of this thread's MMAs complete before TMEM can be freed
+    tc_commit(&drain_bar);
+    mbar_wait(&drain_bar, 0, err);
+  } else if (warp >= 2) {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+    const int qtr = warp & 3;
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
+      const int a = i & 1;
+      if (abort_s || !mbar_wait(&acc_full[a], (i >> 1) & 1, err)) {
+        abort_s = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const TcTile tl = tiles[t];
+      const TcProb pr = probs[tl.prob];
+      const int row = tl.tm * TC_BM + qtr * 32 + lane;
+      float* Cc = F + pr.c;
+      for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+        uint32_t v[32];
+        const uint32_t taddr =
+            tmem + (uint32_t)(a * TC_BN + c0) + ((uint32_t)(qtr * 32) << 16);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, "
+            "[%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]),
+              "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]),
+              "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+              "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+              "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+              "=r"(v[30]), "=r"(v[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < pr.m) {
+          const int colbase = tl.tn * TC_BN + c0;
+          float* cp = Cc + row + (int64_t)colbase * pr.ldc;
+          const int ncol = min(32, pr.n - colbase);
+          float cv[32];
+#pragma unroll
+          for (int j = 0; j < 32; j++)
+            cv[j] = j < ncol ? cp[(int64_t)j * pr.ldc] : 0.f;
+          if (pr.pc >= 0) {
+            const int* rel = rel_base + pr.rel;
+            float* prow = F + pr.pc + rel[row];
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+              if (j < ncol)
+                atomicAdd(prow + (int64_t)rel[colbase + j] * pr.pld,
+                          cv[j] - __uint_as_float(v[j]));
+          } else {
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+              if (j < ncol)
+                cp[(int64_t)j * pr.ldc] = cv[j] - __uint_as_float(v[j]);
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[a]);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
+                     tmem),
+                 "r"(2 * TC_BN));
+}
+
 }  // namespace snu

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -94,6 +95,11 @@ struct GemmBatch {
   GemmProb* rprobs = nullptr;  // SIMT remainder of the FP32 path
   GemmTile* rtiles = nullptr;
   int nrtiles = 0;
+  // tensor-core kernel variant: 0 one CTA per tile, 1 persistent and
+  // warp-specialised; a heuristic default (mean K of the tiles) unless the
+  // autotuner timed both
+  int variant = 0;
+  double ktiles = 0;  // sum of kpad over tiles (for the heuristic)
 };
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType,
@@ -192,11 +198,22 @@ class CudaEngine : public Engine {
                             (int)diag_smem<float>()));
     CK(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)tc_smem_bytes()));
+    CK(cudaFuncSetAttribute(k_gemm_tcp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tc_smem_bytes()));
+    {
+      int sms = 0, nb = 0;
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gemm_tcp, TCP_THREADS,
+                                                       tc_smem_bytes()));
+      tcp_cap_ = std::max(1, std::min(nb, 2)) * sms;  // TMEM: 2 x 256 columns
+    }
     {
       const char* e = getenv("SNU_TC_GEMM");
       use_tc_ = !(e && e[0] == '0');
       const char* g = getenv("SNU_GRAPHS");
       use_graphs_ = !(g && g[0] == '0');
+      const char* tp = getenv("SNU_TC_PERSIST");
+      force_tcp_ = tp ? (tp[0] == '0' ? 0 : 1) : -1;
       const char* pbk = getenv("SNU_PANEL_BLOCK");
       use_block_ = !(pbk && pbk[0] == '0');
     }
@@ -377,6 +394,9 @@ class CudaEngine : public Engine {
     } else {
       if (!d_F32_ && (rc = alloc(d_F32_, (size_t)arena_))) return rc;
       if (!d_I32_ && (rc = alloc(d_I32_, (size_t)invtot_))) return rc;
+    }
+    if (precision == 1 && autotune_ && !tuned_ && force_tcp_ < 0) {
+      if ((rc = autotune())) return rc;
     }
     CK(cudaMemsetAsync(d_flags_, 0, 4 * sizeof(int), stream_));
     CK(cudaMemsetAsync(d_flags_ + 5, 0, sizeof(int), stream_));
@@ -584,6 +604,77 @@ class CudaEngine : public Engine {
         out[r + (int64_t)c * m] =
             F[fi.offset + (ro + r) + (int64_t)(co + c) * fi.ld];
     return ENG_OK;
+  }
+
+ private:
+  // Picks the tensor-core kernel variant of every FP32 GEMM batch: from the
+  // cache file when it holds this pattern, else by timing two complete
+  // factorizations (every batch with variant 0, then 1; the factorization
+  // is recomputed from the values each time, so nothing is lost) and
+  // keeping the faster variant per batch.  The choice is baked into the
+  // factorization's CUDA graph.
+  int autotune() {
+    tuned_ = true;
+    const size_t nb = tc_batches_.size();
+    if (nb == 0) return ENG_OK;
+    char keyhex[32];
+    snprintf(keyhex, sizeof keyhex, "%016llx", (unsigned long long)tune_key_);
+    if (!tune_path_.empty()) {
+      if (FILE* f = fopen(tune_path_.c_str(), "r")) {
+        char k[64], v[65536];
+        bool hit = false;
+        while (fscanf(f, "%63s %65535s", k, v) == 2)
+          if (!strcmp(k, keyhex) && strlen(v) == nb) {
+            for (size_t i = 0; i < nb; i++) tc_batches_[i]->variant = v[i] - '0';
+            hit = true;
+          }
+        fclose(f);
+        if (hit) return ENG_OK;
+      }
+    }
+    std::vector<double> t(2 * nb, 0.0);
+    for (int v = 0; v < 2; v++) {
+      for (GemmBatch* gb : tc_batches_) gb->variant = v;
+      tuning_ = true;
+      tune_rec_.clear();
+      CK(cudaMemsetAsync(d_flags_, 0, 8 * sizeof(int), stream_));
+      int rc = run_factor<float>(d_F32_, d_I32_);
+      tuning_ = false;
+      if (rc) return rc;
+      CK(cudaStreamSynchronize(stream_));
+      for (const auto& r : tune_rec_) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, tune_events_[r.second],
+                                tune_events_[r.second + 1]));
+        for (size_t i = 0; i < nb; i++)
+          if (tc_batches_[i] == r.first) t[2 * i + v] += ms;
+      }
+      for (cudaEvent_t e : tune_events_) cudaEventDestroy(e);
+      tune_events_.clear();
+    }
+    std::string choice(nb, '0');
+    for (size_t i = 0; i < nb; i++) {
+      tc_batches_[i]->variant = t[2 * i + 1] < t[2 * i] ? 1 : 0;
+      choice[i] = (char)('0' + tc_batches_[i]->variant);
+    }
+    if (factor_graph_[1]) {
+      cudaGraphExecDestroy(factor_graph_[1]);
+      factor_graph_[1] = nullptr;
+    }
+    if (!tune_path_.empty())
+      if (FILE* f = fopen(tune_path_.c_str(), "a")) {
+        fprintf(f, "%s %s\n", keyhex, choice.c_str());
+        fclose(f);
+      }
+    return ENG_OK;
+  }
+
+ public:
+  void set_autotune(bool on, const char* path, uint64_t key) override {
+    autotune_ = on;
+    tuned_ = false;
+    tune_path_ = path ? path : "";
+    tune_key_ = key;
   }
 
  private:
@@ -909,11 +1000,15 @@ class CudaEngine : public Engine {
           return ENG_ECUDA;
         }
         int tm = (t.m + TC_BM - 1) / TC_BM, tn = (t.n + TC_BN - 1) / TC_BN;
+        gb->ktiles += (double)t.kpad * tm * tn;
         for (int b = 0; b < tn; b++)
           for (int a = 0; a < tm; a++) tiles.push_back({(int)k, a, b});
       }
       gb->ntcp = (int)gb->tc_host.size();
       gb->ntct = (int)tiles.size();
+      // long K per tile: the persistent kernel hides each epilogue behind
+      // the next tile's MMAs; short K: one CTA per tile balances better
+      gb->variant = gb->ktiles / std::max(1, gb->ntct) >= 512 ? 1 : 0;
       if ((rc = upload(gb->tcp, gb->tc_host))) return rc;
       if ((rc = upload(gb->tct, tiles))) return rc;
       if ((rc = upload(gb->amaps, am))) return rc;
@@ -1189,9 +1284,29 @@ class CudaEngine : public Engine {
     dim3 gbp((gb.tc_maxn + 7) / 8, gb.ntcp);
     k_tc_pack_b<<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
     CKL();
-    k_gemm_tc<<<gb.ntct, 128, tc_smem_bytes(), st>>>(gb.tct, gb.tcp, gb.amaps,
-                                                    gb.bmaps, F, d_flags_ + 2,
-                                                    d_rel_);
+    const int variant = force_tcp_ >= 0 ? force_tcp_ : gb.variant;
+    int te = -1;
+    if (tuning_) {  // autotuner: time this launch
+      te = (int)tune_events_.size();
+      for (int q = 0; q < 2; q++) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        tune_events_.push_back(e);
+      }
+      CK(cudaEventRecord(tune_events_[te], st));
+    }
+    if (variant == 1)  // persistent, warp-specialised
+      k_gemm_tcp<<<std::min(gb.ntct, tcp_cap_), TCP_THREADS, tc_smem_bytes(),
+                   st>>>(gb.tct, gb.ntct, gb.tcp, gb.amaps, gb.bmaps, F,
+                         d_flags_ + 2, d_rel_);
+    else
+      k_gemm_tc<<<gb.ntct, 128, tc_smem_bytes(), st>>>(gb.tct, gb.tcp, gb.amaps,
+                                                      gb.bmaps, F, d_flags_ + 2,
+                                                      d_rel_);
+    if (te >= 0) {
+      CK(cudaEventRecord(tune_events_[te + 1], st));
+      tune_rec_.push_back({(const GemmBatch*)&gb, te});
+    }
     CKL();
     if (gb.nrtiles) {
       k_gemm<float, GBM, GBN, 16, 4, 4><<<gb.nrtiles, 256, 0, st>>>(
@@ -1582,7 +1697,15 @@ class CudaEngine : public Engine {
   std::vector<GemmBatch*> tc_batches_;
   bool use_tc_ = true;
   bool use_graphs_ = true;
-  bool use_block_ = true;  // fused outer-block panels (else per-step kernels)
+  bool use_block_ = true;
+  int force_tcp_ = -1;  // tensor-core kernel variant forced (-1: per batch)
+  int tcp_cap_ = 148;
+  // autotuner of the tensor-core kernel variant per GEMM batch
+  bool autotune_ = false, tuned_ = false, tuning_ = false;
+  std::string tune_path_;
+  uint64_t tune_key_ = 0;
+  std::vector<cudaEvent_t> tune_events_;
+  std::vector<std::pair<const GemmBatch*, int>> tune_rec_;  // fused outer-block panels (else per-step kernels)
   int64_t launches_ = 0;  // kernels launched (counted at every launch site)
   int64_t graph_launches_[2] = {0, 0};
   int64_t last_factor_launches_ = 0, last_solve_launches_ = 0;

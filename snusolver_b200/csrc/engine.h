@@ -78,6 +78,9 @@ class Engine {
   virtual const std::vector<LaunchRec>& trace() const = 0;
   // Kernels launched by the last factorization and the last solve.
   virtual void launch_counts(int64_t* factor, int64_t* solve) const = 0;
+  // Autotuning of the tensor-core GEMM variant per batch at the next FP32
+  // factorization (cache file of choices keyed by the pattern, may be null).
+  virtual void set_autotune(bool on, const char* path, uint64_t key) = 0;
   // Stream for all work of the handle (nullptr: the engine's own stream).
   virtual int set_stream(void* stream) = 0;
   virtual void* stream() const = 0;  // the stream work goes to

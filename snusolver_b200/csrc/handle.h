@@ -24,6 +24,8 @@ struct snu_handle {
   size_t dcap = 0;
   void* stream = nullptr;    // user stream (applied at construct)
   unsigned prof_mask = 0;    // profiling families (applied at construct)
+  int autotune = 0;          // tune the GEMM variants at the next factorize
+  std::string tune_path;     // cache file of tuned choices ("" = none)
   int batch = 0;             // matrices of a batch handle (0: one matrix)
   std::vector<int> batch_rows;  // row_start of every matrix (batch + 1)
 };

@@ -196,3 +196,27 @@ def test_solve_device_pointers(gpu):
     torch.cuda.synchronize()
     X = dX.cpu().numpy().T
     _close(X, s.solve(B), 1e-14, "device vs host solve")
+
+
+def test_autotuned_factorization_matches(gpu, tmp_path):
+    # the autotuner times both tensor-core GEMM kernels per batch, keeps the
+    # faster, and records the choice; results stay those of the default
+    rp, ci, v = generators.convdiff3d(20)
+    n = len(rp) - 1
+    B = generators.rhs(n, 2, seed=3)
+    cache = tmp_path / "tune.txt"
+    ref = snu.Solver(nleaves=8, precision=snu.FP32_IR).construct(rp, ci, v)
+    Xr = ref.factorize().solve(B)
+    s = snu.Solver(nleaves=8, precision=snu.FP32_IR).construct(rp, ci, v)
+    s.set_autotune(True, str(cache))
+    X = s.factorize().solve(B)
+    lines = cache.read_text().split()
+    assert len(lines) == 2 and set(lines[1]) <= {"0", "1"}
+    for r in range(2):
+        assert rel_resid(rp, ci, v, X[:, r], B[:, r]) <= 1e-10
+    assert np.abs(X - Xr).max() <= 1e-8 * np.abs(Xr).max()
+    # a second handle on the same pattern reads the cache (no new line)
+    s2 = snu.Solver(nleaves=8, precision=snu.FP32_IR).construct(rp, ci, v)
+    s2.set_autotune(True, str(cache))
+    s2.factorize()
+    assert cache.read_text().split() == lines
