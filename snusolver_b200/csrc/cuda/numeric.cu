@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -214,6 +215,8 @@ class CudaEngine : public Engine {
       use_graphs_ = !(g && g[0] == '0');
       const char* tp = getenv("SNU_TC_PERSIST");
       force_tcp_ = tp ? (tp[0] == '0' ? 0 : 1) : -1;
+      const char* vb = getenv("SNU_VERBOSE");
+      verbose_ = vb && vb[0] == '1';
       const char* pbk = getenv("SNU_PANEL_BLOCK");
       use_block_ = !(pbk && pbk[0] == '0');
     }
@@ -277,6 +280,7 @@ class CudaEngine : public Engine {
     nfronts_ = fp.nfronts;
     nlevels_ = fp.nlevels;
     arena_ = fp.arena;
+    const double t0 = wall_s();
     deferring_ = true;
     fix_.clear();
     blob_.clear();
@@ -333,9 +337,18 @@ class CudaEngine : public Engine {
     if ((rc = alloc(d_vals_, (size_t)std::max(1, nnz_)))) return rc;
     if ((rc = alloc(d_flags_, 8))) return rc;
     if ((rc = alloc(d_norms_, 3 * 64))) return rc;
+    const double t1 = wall_s();
     if ((rc = build_schedule())) return rc;
+    const double t2 = wall_s();
     if ((rc = finalize_tc())) return rc;
+    const double t3 = wall_s();
     if ((rc = flush_uploads())) return rc;
+    const double t4 = wall_s();
+    if (verbose_)
+      fprintf(stderr,
+              "snusolver: set-up %d fronts, %d levels: tables %.3f s, "
+              "schedule %.3f s, tensor maps %.3f s, upload %.3f s\n",
+              nfronts_, nlevels_, t1 - t0, t2 - t1, t3 - t2, t4 - t3);
     have64_ = have32_ = false;
     return ENG_OK;
   }
@@ -760,6 +773,10 @@ class CudaEngine : public Engine {
   template <typename T>
   int diag_sweep(bool fwd, const SweepTask* tasks, int ntasks, const T* F,
                  const T* I, int nrhs, T* W, T* Y, cudaStream_t st) {
+    if (nrhs > RG) {  // the kernels hold a chunk's W rows for <= RG columns
+      err_ = "pivot-block sweep called with more than 16 right-hand sides";
+      return ENG_EINVAL;
+    }
     if (nrhs <= 1) return diag_launch<T, 1>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
     if (nrhs <= 2) return diag_launch<T, 2>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
     if (nrhs <= 4) return diag_launch<T, 4>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
@@ -1374,6 +1391,21 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
+  // tree_solve over column groups of at most RG right-hand sides (the
+  // pivot-block sweeps hold a chunk's rows for RG columns); W and Y are
+  // reused by every group.
+  template <typename T>
+  int tree_solve_cols(const T* F, const T* I, T* W, T* Y, const double* B,
+                      int ldb, double* X, int ldx, int nrhs, cudaStream_t st) {
+    for (int c0 = 0; c0 < nrhs; c0 += RG) {
+      int rc = tree_solve<T>(F, I, W, Y, B + (size_t)c0 * ldb, ldb,
+                             X + (size_t)c0 * ldx, ldx,
+                             std::min(RG, nrhs - c0), st);
+      if (rc) return rc;
+    }
+    return ENG_OK;
+  }
+
   template <typename T>
   int tree_solve(const T* F, const T* I, T* W, T* Y, const double* B, int ldb,
                  double* X, int ldx, int nrhs, cudaStream_t st) {
@@ -1565,16 +1597,17 @@ class CudaEngine : public Engine {
     do {
       if ((rc = colmax(dB, ldb, nrhs, st, bn))) break;
       if (precision == 0) {
-        if ((rc = tree_solve<double>(d_F64_, d_I64_, (double*)pW, (double*)pY,
-                                     dB, ldb, dX, ldb, nrhs, st)))
+        if ((rc = tree_solve_cols<double>(d_F64_, d_I64_, (double*)pW,
+                                          (double*)pY, dB, ldb, dX, ldb, nrhs,
+                                          st)))
           break;
         rc = berr(dX);
         break;
       }
       float* W = (float*)pW;
       float* Y = (float*)pY;
-      if ((rc = tree_solve<float>(d_F32_, d_I32_, W, Y, dB, ldb, dX, ldb, nrhs,
-                                  st)))
+      if ((rc = tree_solve_cols<float>(d_F32_, d_I32_, W, Y, dB, ldb, dX, ldb,
+                                       nrhs, st)))
         break;
       double prev = INFINITY;
       int it = 0, stagnant = 0;
@@ -1590,8 +1623,8 @@ class CudaEngine : public Engine {
         }
         stagnant = r.backward_error > 0.5 * prev ? stagnant + 1 : 0;
         prev = r.backward_error;
-        if ((rc = tree_solve<float>(d_F32_, d_I32_, W, Y, R, n_, D, n_, nrhs,
-                                    st)))
+        if ((rc = tree_solve_cols<float>(d_F32_, d_I32_, W, Y, R, n_, D, n_,
+                                         nrhs, st)))
           break;
         k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, D, n_, dX, ldb);
         CKL();
@@ -1698,6 +1731,12 @@ class CudaEngine : public Engine {
   bool use_tc_ = true;
   bool use_graphs_ = true;
   bool use_block_ = true;
+  bool verbose_ = false;  // SNU_VERBOSE=1: set-up phase timings on stderr
+  static double wall_s() {
+    return std::chrono::duration<double>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+  }
   int force_tcp_ = -1;  // tensor-core kernel variant forced (-1: per batch)
   int tcp_cap_ = 148;
   // autotuner of the tensor-core kernel variant per GEMM batch

@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(DIAG_ROWS)
   T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;         // [2][NB * NB]
   __shared__ T ws[NB][R];
   __shared__ T ys[NB][R];
+  __shared__ T Wc[R][DIAG_ROWS];  // this chunk's rows of W (nrhs <= R)
   __shared__ int bad;
   const int tid = threadIdx.x;
   constexpr int V = 16 / sizeof(T);
@@ -158,6 +159,11 @@ __global__ void __launch_bounds__(DIAG_ROWS)
     __syncthreads();
     stage(0, 0);
     cp_async_commit();
+    // the pivot rows of W are dead after this sweep (Y carries the result),
+    // so the chunk keeps its rows in shared memory and never writes them back
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      Wc[r][tid] = (row < c1 && r < nrhs) ? Wf[row + (int64_t)r * dim] : (T)0;
     for (int s = 0; s < ntiles; s++) {
       const int k0 = s * NB, kb = min(NB, f.p - k0), k1 = k0 + kb;
       if (k0 >= c1) break;  // owned by a later chunk; updates no row of ours
@@ -176,13 +182,11 @@ __global__ void __launch_bounds__(DIAG_ROWS)
         if (owner) {
           for (int e = tid; e < NB * R; e += blockDim.x) {
             const int i = e % NB, r = e / NB;
-            ws[i][r] = (i < kb && r < nr) ? Wf[k0 + i + (int64_t)(r0 + r) * dim]
-                                          : (T)0;
+            ws[i][r] = (i < kb && r < nr) ? Wc[r0 + r][k0 - c0 + i] : (T)0;
           }
           __syncthreads();
           tile_apply<T, R>(Xs, ws, ys, Yf, f.p, k0, kb, r0, nr);
-          __threadfence();  // publish this thread's Y stores device-wide
-          __syncthreads();
+          __syncthreads();  // raise_flag's fence publishes the CTA's Y stores
           if (tid == 0 && r0 + R >= nrhs) raise_flag(fl + s);
         } else {
           for (int e = tid; e < NB * R; e += blockDim.x) {
@@ -205,7 +209,7 @@ __global__ void __launch_bounds__(DIAG_ROWS)
           }
 #pragma unroll
           for (int r = 0; r < R; r++)
-            if (r < nr) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
+            if (r < nr) Wc[r0 + r][tid] -= acc[r];
         }
         __syncthreads();
       }
@@ -231,6 +235,7 @@ __global__ void __launch_bounds__(DIAG_ROWS)
   T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;
   __shared__ T ws[NB][R];
   __shared__ T xs[NB][R];
+  __shared__ T Wc[R][DIAG_ROWS];  // this chunk's rows of W (nrhs <= R)
   __shared__ int bad;
   const int tid = threadIdx.x;
   if (tid == 0) bad = 0;
@@ -256,6 +261,9 @@ __global__ void __launch_bounds__(DIAG_ROWS)
     __syncthreads();
     stage(ntiles - 1, (ntiles - 1) & 1);
     cp_async_commit();
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      Wc[r][tid] = (row < c1 && r < nrhs) ? Wf[row + (int64_t)r * dim] : (T)0;
     for (int s = ntiles - 1; s >= 0; s--) {
       const int k0 = s * NB, kb = min(NB, f.p - k0);
       if (k0 < c0) break;  // tile lies above our rows: nothing left
@@ -274,12 +282,10 @@ __global__ void __launch_bounds__(DIAG_ROWS)
         if (owner) {
           for (int e = tid; e < NB * R; e += blockDim.x) {
             const int i = e % NB, r = e / NB;
-            ws[i][r] = (i < kb && r < nr) ? Wf[k0 + i + (int64_t)(r0 + r) * dim]
-                                          : (T)0;
+            ws[i][r] = (i < kb && r < nr) ? Wc[r0 + r][k0 - c0 + i] : (T)0;
           }
           __syncthreads();
           tile_apply<T, R>(Xs, ws, xs, Yf, f.p, k0, kb, r0, nr);
-          __threadfence();
           __syncthreads();
           if (tid == 0 && r0 + R >= nrhs) raise_flag(fl + s);
         } else {
@@ -303,7 +309,7 @@ __global__ void __launch_bounds__(DIAG_ROWS)
           }
 #pragma unroll
           for (int r = 0; r < R; r++)
-            if (r < nr) Wf[row + (int64_t)(r0 + r) * dim] -= acc[r];
+            if (r < nr) Wc[r0 + r][tid] -= acc[r];
         }
         __syncthreads();
       }
