@@ -323,7 +323,7 @@ class CudaEngine : public Engine {
       ntileflags_ = std::max<int64_t>(acc, 1);
       if ((rc = upload(d_flag_off_, fo))) return rc;
       if ((rc = alloc(d_tflags_, (size_t)(2 * ntileflags_)))) return rc;
-      if ((rc = alloc(d_fflags_, (size_t)ntileflags_))) return rc;
+      if ((rc = alloc(d_fflags_, (size_t)(2 * ntileflags_)))) return rc;
     }
     if ((rc = upload(d_fr_, frh_))) return rc;
     if ((rc = upload(d_gidx_, fp.gidx))) return rc;
@@ -1345,7 +1345,7 @@ class CudaEngine : public Engine {
       const int64_t na = fp_->asm_level[nlevels_];
       int pi = prof_begin(KF_ASSEMBLE, st);
       CK(cudaMemsetAsync(F, 0, sizeof(T) * arena_, st));
-      CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * ntileflags_, st));
+      CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 2 * ntileflags_, st));
       if (na > 0) {
         int blocks = (int)std::min<int64_t>((na + 255) / 256, 148 * 16);
         k_assemble<T><<<blocks, 256, 0, st>>>(d_asm_pos_, d_asm_val_, d_vals_,

@@ -95,12 +95,22 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
   const int kb = min(NB, f.p - k0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   T* base = F + f.off + k0 + (int64_t)k0 * f.ld;
-  for (int e = tid; e < NB * NB; e += 256) {
-    const int i = e & (NB - 1), j = e / NB;
-    D[i + j * TLD] = (i < kb && j < kb) ? base[i + (int64_t)j * f.ld]
-                                        : (i == j ? (T)1 : (T)0);
-    XL[i + j * TLD] = (T)0;
-    XU[i + j * TLD] = (T)0;
+  {
+    // all 16 loads of a thread in flight before the shared-memory stores
+    T v[NB * NB / 256];
+#pragma unroll
+    for (int q = 0; q < NB * NB / 256; q++) {
+      const int e = tid + 256 * q, i = e & (NB - 1), j = e / NB;
+      v[q] = (i < kb && j < kb) ? __ldcg(base + i + (int64_t)j * f.ld)
+                                : (i == j ? (T)1 : (T)0);
+    }
+#pragma unroll
+    for (int q = 0; q < NB * NB / 256; q++) {
+      const int e = tid + 256 * q, i = e & (NB - 1), j = e / NB;
+      D[i + j * TLD] = v[q];
+      XL[i + j * TLD] = (T)0;
+      XU[i + j * TLD] = (T)0;
+    }
   }
   __syncthreads();
   const T teps = (T)eps;

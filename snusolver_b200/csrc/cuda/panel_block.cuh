@@ -41,10 +41,18 @@ struct BlockTask {
 template <typename T>
 __device__ __forceinline__ void pb_load(T* S, const T* src, int64_t ld, int nr,
                                         int nc) {
-  for (int e = threadIdx.x; e < NB * NB; e += 256) {
-    const int i = e & (NB - 1), j = e / NB;
-    // through L2: tiles written by other blocks of this launch
-    S[i + j * TLD] = (i < nr && j < nc) ? __ldcg(src + i + j * ld) : (T)0;
+  // all 16 loads of a thread in flight before any shared-memory store
+  // (through L2: tiles written by other blocks of this launch)
+  T v[NB * NB / 256];
+#pragma unroll
+  for (int q = 0; q < NB * NB / 256; q++) {
+    const int e = threadIdx.x + 256 * q, i = e & (NB - 1), j = e / NB;
+    v[q] = (i < nr && j < nc) ? __ldcg(src + i + j * ld) : (T)0;
+  }
+#pragma unroll
+  for (int q = 0; q < NB * NB / 256; q++) {
+    const int e = threadIdx.x + 256 * q, i = e & (NB - 1), j = e / NB;
+    S[i + j * TLD] = v[q];
   }
 }
 
@@ -78,6 +86,16 @@ __device__ __forceinline__ void pb_store(T* dst, int64_t ld, int nr, int nc,
                                          const T (&acc)[4][4], bool sub,
                                          T* S) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  T old[4][4];
+  if (sub) {  // the 16 reads in flight together
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int i = tx + 16 * a, j = ty + 16 * b;
+        old[a][b] = (i < nr && j < nc) ? __ldcg(dst + i + j * ld) : (T)0;
+      }
+  }
 #pragma unroll
   for (int b = 0; b < 4; b++) {
     const int j = ty + 16 * b;
@@ -85,7 +103,7 @@ __device__ __forceinline__ void pb_store(T* dst, int64_t ld, int nr, int nc,
     for (int a = 0; a < 4; a++) {
       const int i = tx + 16 * a;
       if (i < nr && j < nc) {
-        T v = sub ? dst[i + j * ld] - acc[a][b] : acc[a][b];
+        T v = sub ? old[a][b] - acc[a][b] : acc[a][b];
         dst[i + j * ld] = v;
         if (S) S[i + j * TLD] = v;
       } else if (S) {
@@ -103,7 +121,7 @@ constexpr size_t block_smem() {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(256, 2)
     k_panel_block(const BlockTask* __restrict__ tasks, int ntasks,
                   const FrontDev* __restrict__ fr, T* __restrict__ F,
                   T* __restrict__ INV, int K0, double eps, int* dflags,
@@ -122,18 +140,40 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
     const int dim = f.p + f.q;
     const int K1 = min(K0 + OB_COLS, f.p);
     const int nt = (K1 - K0 + NB - 1) / NB;
-    int* fl = tflags + flag_off[tk.front];
+    // two flags per tile: [2 s] tile factored and its first U chunk (the
+    // next tile's columns) written, [2 s + 1] all its U rows written
+    int* fl = tflags + 2 * flag_off[tk.front];
     T* Fo = F + f.off;
     const int64_t ld = f.ld;
     if (tk.kind == 0) {
       const int R0 = K0 + NB * tk.chunk, nr = min(NB, dim - R0);
+      int deferred = -1;  // step whose remaining column chunks wait
       for (int t = 0; t < nt; t++) {
         const int k0 = K0 + NB * t, kb = min(NB, f.p - k0), k1 = k0 + kb;
         const int step = k0 / NB;
         if (tk.chunk == t) {
-          // owner: the diagonal tile, then its U rows inside the block
+          // owner: the diagonal tile (its columns are up to date)
           diag_tile<T>(f, F, INV, k0, step, eps, dflags, S0, S1, S2);
           __syncthreads();
+          if (deferred >= 0) {
+            // the previous step's update of our rows right of this tile
+            const int pk0 = K0 + NB * deferred, pstep = pk0 / NB;
+            if (threadIdx.x == 0 && !wait_flag(fl + 2 * pstep + 1, err)) bad = 1;
+            __syncthreads();
+            if (bad) return;
+            for (int c0 = k1; c0 < K1; c0 += NB) {
+              const int nc = min(NB, K1 - c0);
+              pb_load(S0, Fo + R0 + pk0 * ld, ld, nr, NB);  // our L block
+              pb_load(S2, Fo + pk0 + c0 * ld, ld, NB, nc);  // its U rows
+              __syncthreads();
+              T acc[4][4];
+              pb_mm(acc, S0, S2, NB);
+              pb_store(Fo + R0 + c0 * ld, ld, nr, nc, acc, true, (T*)nullptr);
+              __syncthreads();
+            }
+          }
+          // U rows inside the block: the first chunk (the next tile's
+          // columns) is published on its own, the next owner needs only it
           for (int c0 = k1; c0 < K1; c0 += NB) {
             const int nc = min(NB, K1 - c0);
             pb_load(S0, Fo + k0 + c0 * ld, ld, kb, nc);
@@ -142,24 +182,32 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
             pb_mm(acc, S1, S0, kb);  // Linv A
             pb_store(Fo + k0 + c0 * ld, ld, kb, nc, acc, false, (T*)nullptr);
             __syncthreads();
+            if (c0 == k1 && threadIdx.x == 0) raise_flag(fl + 2 * step);
           }
-          __threadfence();
-          __syncthreads();
-          if (threadIdx.x == 0) raise_flag(fl + step);
+          if (threadIdx.x == 0) {
+            if (k1 >= K1) raise_flag(fl + 2 * step);
+            raise_flag(fl + 2 * step + 1);
+          }
           // a partial last tile: the chunk's rows past it are L rows
-          // (L = A Uinv, Uinv still in S2); nothing is right of the block
+          // (L = A Uinv); nothing is right of the block
           if (k1 < R0 + nr) {
+            pb_load(S1, INV + f.inv_off + (int64_t)step * 2 * NB * NB + NB * NB,
+                    (int64_t)NB, NB, NB);
             pb_load(S0, Fo + k1 + k0 * ld, ld, R0 + nr - k1, kb);
             __syncthreads();
             T acc[4][4];
-            pb_mm(acc, S0, S2, kb);
+            pb_mm(acc, S0, S1, kb);
             pb_store(Fo + k1 + k0 * ld, ld, R0 + nr - k1, kb, acc, false,
                      (T*)nullptr);
             __syncthreads();
           }
           break;  // the owner's rows are complete in this block
         }
-        if (threadIdx.x == 0 && !wait_flag(fl + step, err)) bad = 1;
+        // the next tile's owner only needs this tile's first U chunk now
+        const bool next_owner = tk.chunk == t + 1;
+        if (threadIdx.x == 0 &&
+            !wait_flag(fl + 2 * step + (next_owner ? 0 : 1), err))
+          bad = 1;
         __syncthreads();
         if (bad) return;
         // L block of our rows: A Uinv_t
@@ -173,7 +221,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
         pb_store(Fo + R0 + k0 * ld, ld, nr, kb, acc, false, S0);  // S0 = L
         __syncthreads();
         // rank-64 update of our rows inside the block: columns [k1, K1)
+        // (the next owner takes the first chunk now, the rest after its tile)
         for (int c0 = k1; c0 < K1; c0 += NB) {
+          if (next_owner && c0 > k1) {
+            deferred = t;
+            break;
+          }
           const int nc = min(NB, K1 - c0);
           pb_load(S2, Fo + k0 + c0 * ld, ld, kb, nc);  // U (from the owner)
           __syncthreads();
@@ -187,7 +240,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
       for (int t = 0; t < nt; t++) {
         const int k0 = K0 + NB * t, kb = min(NB, f.p - k0);
         const int step = k0 / NB;
-        if (threadIdx.x == 0 && !wait_flag(fl + step, err)) bad = 1;
+        if (threadIdx.x == 0 && !wait_flag(fl + 2 * step + 1, err)) bad = 1;
         __syncthreads();
         if (bad) return;
         // S2 = A_t - sum_{s<t} L_ts U_s  (our columns)
