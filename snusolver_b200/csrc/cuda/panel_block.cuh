@@ -66,6 +66,7 @@ __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b < 4; b++) acc[a][b] = (T)0;
+#pragma unroll 8
   for (int m = 0; m < kk; m++) {
     T av[4], bv[4];
 #pragma unroll
