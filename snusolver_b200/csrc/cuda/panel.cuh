@@ -38,45 +38,132 @@ constexpr int SB = 16;  // sub-block of the blocked tile factorization
 // of it inside the tile are finished by substitution (one thread per row /
 // column), and the rest of the tile takes a rank-SB update.  The inverses
 // start from the SB x SB diagonal-block inverses (eight warps at once) and
-// fill the off-diagonal blocks by distance from the diagonal.  A tile
-// smaller than NB is padded with the identity, which leaves its factors and
-// inverses unchanged.
-// One distance of stage B of k_diag_lu_inv: the 2 (NB/SB - DIST) blocks of
-// Linv and Uinv at block distance DIST, element (ei, ej) of each per thread.
-// Compile-time trip counts: the products unroll fully and the independent
-// blocks interleave.
-template <typename T, int DIST>
-__device__ __forceinline__ void inv_distance(const T* D, T* XL, T* XU,
-                                             T (*Tb)[SB][SB + 1], int ei,
-                                             int ej) {
-  constexpr int NT = NB / SB - DIST;
-  T acc[2 * NT];
+// are joined by recursive doubling (inv_join).  A tile smaller than NB is
+// padded with the identity, which leaves its factors and inverses unchanged.
+
+// acc(r, c) += sum_{m0 <= m < m1} A[r + m lda] B[m + c ldb]: an R x C
+// register tile of a product of two shared-memory operands.
+template <typename T, int R, int C>
+__device__ __forceinline__ void tile_mm(const T* A, int lda, const T* B,
+                                        int ldb, int m0, int m1,
+                                        T (&acc)[R][C]) {
+#pragma unroll 4
+  for (int m = m0; m < m1; m++) {
+    T a[R], b[C];
 #pragma unroll
-  for (int t = 0; t < 2 * NT; t++) acc[t] = (T)0;
+    for (int r = 0; r < R; r++) a[r] = A[r + m * lda];
 #pragma unroll
-  for (int mm = 0; mm < DIST * SB; mm++) {
+    for (int c = 0; c < C; c++) b[c] = B[m + c * ldb];
 #pragma unroll
-    for (int t = 0; t < NT; t++) {  // L(b2, m) Linv(m, b1), m from b1
-      acc[t] += D[(t + DIST) * SB + ei + (t * SB + mm) * TLD] *
-                XL[t * SB + mm + (t * SB + ej) * TLD];
-      // U(b1, m) Uinv(m, b2), m from b1 + 1
-      acc[NT + t] += D[t * SB + ei + ((t + 1) * SB + mm) * TLD] *
-                     XU[(t + 1) * SB + mm + ((t + DIST) * SB + ej) * TLD];
-    }
+    for (int r = 0; r < R; r++)
+#pragma unroll
+      for (int c = 0; c < C; c++) acc[r][c] += a[r] * b[c];
   }
+}
+
+// Stage B of the tile inverses, by recursive doubling: level 1 joins the
+// SB x SB diagonal-block inverses into 2SB x 2SB ones, level 2 joins those
+// into the NB x NB inverses,
+//   Linv21 = -Linv22 (L21 Linv11),   Uinv12 = -Uinv11 (U12 Uinv22).
+// The first products go to the zero triangles (XL's upper right and XU's
+// lower left NB/2 x NB/2 blocks), which are cleared again at the end.  A
+// thread holds a 2 x 2 (level 1) or 2 x 4 (level 2) register tile; the
+// tiles of one warp share their columns (first product) or rows (second
+// product), so the triangular factor bounds the inner loop per warp.
+template <typename T>
+__device__ __forceinline__ void inv_join(const T* D, T* XL, T* XU, int tid) {
+  constexpr int H = NB / 2;
+  T* TL = XL + H * TLD;  // XL(0:H, H:NB)
+  T* TU = XU + H;        // XU(H:NB, 0:H)
+  const int lane = tid & 31;
+  {
+    // level 1: join pair P of the diagonal blocks, of L (isU 0) or U
+    const int pr = tid >> 6, P = pr & 1, isU = pr >> 1, wp = (tid >> 5) & 1;
+    const int b1 = 2 * P * SB, b2 = b1 + SB;
+    T* Tp = TL + P * SB + isU * SB * TLD;
+    {
+      const int i = 2 * (lane & 7), j = 2 * (wp * 4 + (lane >> 3));
+      T acc[2][2] = {};
+      if (!isU)  // L21 Linv11: Linv11(m, j) = 0 for m < j
+        tile_mm<T, 2, 2>(D + b2 + i + b1 * TLD, TLD, XL + b1 + (b1 + j) * TLD,
+                         TLD, 8 * wp, SB, acc);
+      else       // U12 Uinv22: Uinv22(m, j) = 0 for m > j
+        tile_mm<T, 2, 2>(D + b1 + i + b2 * TLD, TLD, XU + b2 + (b2 + j) * TLD,
+                         TLD, 0, 8 * wp + 8, acc);
 #pragma unroll
-  for (int t = 0; t < 2 * NT; t++) Tb[t][ei][ej] = acc[t];
-  __syncthreads();
+      for (int r = 0; r < 2; r++)
 #pragma unroll
-  for (int t = 0; t < NT; t++) {
-    T al = (T)0, au = (T)0;
-#pragma unroll
-    for (int m = 0; m < SB; m++) {
-      al -= XL[(t + DIST) * SB + ei + ((t + DIST) * SB + m) * TLD] * Tb[t][m][ej];
-      au -= XU[t * SB + ei + (t * SB + m) * TLD] * Tb[NT + t][m][ej];
+        for (int c = 0; c < 2; c++) Tp[i + r + (j + c) * TLD] = acc[r][c];
     }
-    XL[(t + DIST) * SB + ei + (t * SB + ej) * TLD] = al;
-    XU[t * SB + ei + ((t + DIST) * SB + ej) * TLD] = au;
+    __syncthreads();
+    {
+      const int i = 2 * (wp * 4 + (lane >> 3)), j = 2 * (lane & 7);
+      T acc[2][2] = {};
+      if (!isU) {  // Linv22 (i, m) = 0 for m > i
+        tile_mm<T, 2, 2>(XL + b2 + i + b2 * TLD, TLD, Tp + j * TLD, TLD, 0,
+                         8 * wp + 8, acc);
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+          for (int c = 0; c < 2; c++)
+            XL[b2 + i + r + (b1 + j + c) * TLD] = -acc[r][c];
+      } else {     // Uinv11 (i, m) = 0 for m < i
+        tile_mm<T, 2, 2>(XU + b1 + i + b1 * TLD, TLD, Tp + j * TLD, TLD,
+                         8 * wp, SB, acc);
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+          for (int c = 0; c < 2; c++)
+            XU[b1 + i + r + (b2 + j + c) * TLD] = -acc[r][c];
+      }
+    }
+    __syncthreads();
+  }
+  {
+    // level 2: join the two H x H inverses of L (isU 0) or U
+    const int isU = tid >> 7, wq = (tid >> 5) & 3;
+    {
+      const int i = 2 * (lane & 15), j = 4 * (wq * 2 + (lane >> 4));
+      T acc[2][4] = {};
+      T* out;
+      if (!isU) {
+        tile_mm<T, 2, 4>(D + H + i, TLD, XL + j * TLD, TLD, 8 * wq, H, acc);
+        out = TL;
+      } else {
+        tile_mm<T, 2, 4>(D + i + H * TLD, TLD, XU + H + (H + j) * TLD, TLD, 0,
+                         8 * wq + 8, acc);
+        out = TU;
+      }
+#pragma unroll
+      for (int r = 0; r < 2; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) out[i + r + (j + c) * TLD] = acc[r][c];
+    }
+    __syncthreads();
+    {
+      const int i = 2 * (wq * 4 + (lane >> 3)), j = 4 * (lane & 7);
+      T acc[2][4] = {};
+      if (!isU) {
+        tile_mm<T, 2, 4>(XL + H + i + H * TLD, TLD, TL + j * TLD, TLD, 0,
+                         8 * wq + 8, acc);
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) XL[H + i + r + (j + c) * TLD] = -acc[r][c];
+      } else {
+        tile_mm<T, 2, 4>(XU + i, TLD, TU + j * TLD, TLD, 8 * wq, H, acc);
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) XU[i + r + (H + j + c) * TLD] = -acc[r][c];
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < H * H; e += 256) {
+    const int i = e & (H - 1), j = e / H;
+    TL[i + j * TLD] = (T)0;
+    TU[i + j * TLD] = (T)0;
   }
   __syncthreads();
 }
@@ -91,7 +178,6 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
                                           int step, double eps, int* flags,
                                           T* D, T* XL, T* XU) {
   __shared__ T rdiag[NB];  // 1 / U[i][i]
-  __shared__ T Tb[6][SB][SB + 1];
   const int kb = min(NB, f.p - k0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   T* base = F + f.off + k0 + (int64_t)k0 * f.ld;
@@ -122,17 +208,23 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
       T v[SB];
 #pragma unroll
       for (int j = 0; j < SB; j++) v[j] = D[r + (s0 + j) * TLD];
+      // the pivot is warp-uniform: the replaced-pivot count and the
+      // zero / non-finite test are kept in registers and published once
+      // after the sub-block (a global atomic inside the loop costs a warp
+      // divergence per pivot)
+      int nguard = 0;
+      bool bad = false;
 #pragma unroll
       for (int k = 0; k < SB; k++) {
         T rowk[SB];
 #pragma unroll
         for (int j = k; j < SB; j++) rowk[j] = __shfl_sync(0xffffffffu, v[j], k);
         T piv = rowk[k];
-        bool guarded = false;
         if (f.guard && s0 + k < kb && piv < teps && piv > -teps) {
           piv = piv < (T)0 ? -teps : teps;
-          guarded = true;
+          nguard++;
         }
+        if (s0 + k < kb && (!(piv != (T)0) || !isfinite(piv))) bad = true;
         const T rp = recip_rn(piv);
         if (lane == k) v[k] = piv;
         if (lane > k && lane < SB) {
@@ -141,13 +233,11 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
 #pragma unroll
           for (int j = k + 1; j < SB; j++) v[j] -= l * rowk[j];
         }
-        if (lane == 0) {
-          rdiag[s0 + k] = rp;
-          if (s0 + k < kb) {
-            if (guarded) atomicAdd(flags, 1);
-            if (!(piv != (T)0) || !isfinite((double)piv)) flags[1] = 1;
-          }
-        }
+        if (lane == 0) rdiag[s0 + k] = rp;
+      }
+      if (lane == 0) {
+        if (nguard) atomicAdd(flags, nguard);
+        if (bad) flags[1] = 1;
       }
       if (lane < SB)
 #pragma unroll
@@ -236,13 +326,8 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
     }
   }
   __syncthreads();
-  // stage B: off-diagonal blocks by distance d from the diagonal
-  //   Linv(b2,b1) = -Linv(b2,b2) * sum_{m=b1}^{b2-1} L(b2,m) Linv(m,b1)
-  //   Uinv(b1,b2) = -Uinv(b1,b1) * sum_{m=b1+1}^{b2} U(b1,m) Uinv(m,b2)
-  const int ei = tid & 15, ej = tid >> 4;
-  inv_distance<T, 1>(D, XL, XU, Tb, ei, ej);
-  inv_distance<T, 2>(D, XL, XU, Tb, ei, ej);
-  inv_distance<T, 3>(D, XL, XU, Tb, ei, ej);
+  // stage B: the off-diagonal blocks
+  inv_join<T>(D, XL, XU, tid);
   T* inv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
   for (int e = tid; e < NB * NB; e += 256) {
     const int i = e & (NB - 1), j = e / NB;
