@@ -214,25 +214,28 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
       // divergence per pivot)
       int nguard = 0;
       bool bad = false;
+      const bool guard = f.guard != 0;
 #pragma unroll
       for (int k = 0; k < SB; k++) {
         T rowk[SB];
 #pragma unroll
         for (int j = k; j < SB; j++) rowk[j] = __shfl_sync(0xffffffffu, v[j], k);
         T piv = rowk[k];
-        if (f.guard && s0 + k < kb && piv < teps && piv > -teps) {
-          piv = piv < (T)0 ? -teps : teps;
-          nguard++;
-        }
-        if (s0 + k < kb && (!(piv != (T)0) || !isfinite(piv))) bad = true;
+        // branch-free: the guard, the test and the update are selects, so
+        // the warp never diverges inside the pivot chain
+        const bool live = s0 + k < kb;
+        const bool g = guard & live & (piv < teps) & (piv > -teps);
+        piv = g ? (piv < (T)0 ? -teps : teps) : piv;
+        nguard += g;
+        bad |= live & (!(piv != (T)0) | !isfinite(piv));
         const T rp = recip_rn(piv);
-        if (lane == k) v[k] = piv;
-        if (lane > k && lane < SB) {
-          const T l = v[k] * rp;
-          v[k] = l;
+        // lanes below row k take the multiplier and the update (lanes
+        // 16-31 hold copies of the rows and are never stored)
+        const bool upd = lane > k;
+        const T l = v[k] * rp;
+        v[k] = upd ? l : (lane == k ? piv : v[k]);
 #pragma unroll
-          for (int j = k + 1; j < SB; j++) v[j] -= l * rowk[j];
-        }
+        for (int j = k + 1; j < SB; j++) v[j] = upd ? v[j] - l * rowk[j] : v[j];
         if (lane == 0) rdiag[s0 + k] = rp;
       }
       if (lane == 0) {
