@@ -1198,6 +1198,23 @@ class CudaEngine : public Engine {
         if (!bt.empty() && (rc = upload(O.tasks, bt))) return rc;
         if ((rc = gemm_batch(og, O.outer))) return rc;
       }
+      if (verbose_) {
+        int nf = 0, pmax = 0, qmax = 0;
+        double ps = 0, qs = 0;
+        for (int f = L.f0; f < L.f1; f++) {
+          const FrontInfo& fi = fp.fronts[f];
+          nf++;
+          pmax = std::max(pmax, fi.p);
+          qmax = std::max(qmax, fi.q);
+          ps += fi.p;
+          qs += fi.q;
+        }
+        fprintf(stderr,
+                "snusolver: level %d: %d fronts, p max %d avg %.0f, q max %d "
+                "avg %.0f, outer blocks %d, tasks of the first %d\n",
+                l, nf, pmax, nf ? ps / nf : 0.0, qmax, nf ? qs / nf : 0.0, nob,
+                nob ? L.ob[0].ntasks : 0);
+      }
       // solve sweeps; fronts with the longest tile chains first
       std::vector<int> byp;
       for (int f = L.f0; f < L.f1; f++)

@@ -199,7 +199,7 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
     }
   }
   __syncthreads();
-  const T teps = (T)eps;
+  const T teps = (T)eps, rteps = recip_rn(teps);
   for (int b = 0; b < NB / SB; b++) {
     const int s0 = b * SB;
     // (1) diagonal sub-block by warp 0; lane l (< SB) owns row s0 + l
@@ -223,12 +223,15 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
         T piv = rowk[k];
         // branch-free: the guard, the test and the update are selects, so
         // the warp never diverges inside the pivot chain
+        // the guard is a select after the reciprocal, off the pivot chain
+        // (1 / +-eps is +-rteps exactly)
         const bool live = s0 + k < kb;
         const bool g = guard & live & (piv < teps) & (piv > -teps);
+        const T rraw = recip_rn(piv);
+        const T rp = g ? (piv < (T)0 ? -rteps : rteps) : rraw;
         piv = g ? (piv < (T)0 ? -teps : teps) : piv;
         nguard += g;
         bad |= live & (!(piv != (T)0) | !isfinite(piv));
-        const T rp = recip_rn(piv);
         // lanes below row k take the multiplier and the update (lanes
         // 16-31 hold copies of the rows and are never stored)
         const bool upd = lane > k;
