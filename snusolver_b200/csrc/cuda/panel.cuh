@@ -69,19 +69,25 @@ __device__ __forceinline__ void tile_mm(const T* A, int lda, const T* B,
 // lower left NB/2 x NB/2 blocks), which are cleared again at the end.  A
 // thread holds a 2 x 2 (level 1) or 2 x 4 (level 2) register tile; the
 // tiles of one warp share their columns (first product) or rows (second
-// product), so the triangular factor bounds the inner loop per warp.
+// product), so the triangular factor bounds the inner loop per warp.  nbk:
+// the sub-blocks that hold the tile; the rest is identity padding, whose
+// joins are zero and are skipped.
 template <typename T>
-__device__ __forceinline__ void inv_join(const T* D, T* XL, T* XU, int tid) {
+__device__ __forceinline__ void inv_join(const T* D, T* XL, T* XU, int tid,
+                                         int nbk) {
   constexpr int H = NB / 2;
   T* TL = XL + H * TLD;  // XL(0:H, H:NB)
   T* TU = XU + H;        // XU(H:NB, 0:H)
   const int lane = tid & 31;
+  if (nbk < 2) return;  // one block: nothing off the diagonal
   {
-    // level 1: join pair P of the diagonal blocks, of L (isU 0) or U
+    // level 1: join pair P of the diagonal blocks, of L (isU 0) or U (pair
+    // 1 only when its second block is not identity padding)
     const int pr = tid >> 6, P = pr & 1, isU = pr >> 1, wp = (tid >> 5) & 1;
     const int b1 = 2 * P * SB, b2 = b1 + SB;
+    const bool work = P == 0 || nbk == NB / SB;
     T* Tp = TL + P * SB + isU * SB * TLD;
-    {
+    if (work) {
       const int i = 2 * (lane & 7), j = 2 * (wp * 4 + (lane >> 3));
       T acc[2][2] = {};
       if (!isU)  // L21 Linv11: Linv11(m, j) = 0 for m < j
@@ -96,7 +102,7 @@ __device__ __forceinline__ void inv_join(const T* D, T* XL, T* XU, int tid) {
         for (int c = 0; c < 2; c++) Tp[i + r + (j + c) * TLD] = acc[r][c];
     }
     __syncthreads();
-    {
+    if (work) {
       const int i = 2 * (wp * 4 + (lane >> 3)), j = 2 * (lane & 7);
       T acc[2][2] = {};
       if (!isU) {  // Linv22 (i, m) = 0 for m > i
@@ -119,7 +125,7 @@ __device__ __forceinline__ void inv_join(const T* D, T* XL, T* XU, int tid) {
     }
     __syncthreads();
   }
-  {
+  if (nbk > 2) {
     // level 2: join the two H x H inverses of L (isU 0) or U
     const int isU = tid >> 7, wq = (tid >> 5) & 3;
     {
@@ -180,6 +186,10 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
   __shared__ T rdiag[NB];  // 1 / U[i][i]
   const int kb = min(NB, f.p - k0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // sub-blocks past the tile (identity padding) need no factorization:
+  // their pivots are 1
+  const int nbk = (kb + SB - 1) / SB, kbp = nbk * SB;
+  if (tid >= kbp && tid < NB) rdiag[tid] = (T)1;
   T* base = F + f.off + k0 + (int64_t)k0 * f.ld;
   {
     // all 16 loads of a thread in flight before the shared-memory stores
@@ -200,7 +210,7 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
   }
   __syncthreads();
   const T teps = (T)eps, rteps = recip_rn(teps);
-  for (int b = 0; b < NB / SB; b++) {
+  for (int b = 0; b < nbk; b++) {
     const int s0 = b * SB;
     // (1) diagonal sub-block by warp 0; lane l (< SB) owns row s0 + l
     if (warp == 0) {
@@ -250,7 +260,7 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
         for (int j = 0; j < SB; j++) D[r + (s0 + j) * TLD] = v[j];
     }
     __syncthreads();
-    const int rem = NB - s0 - SB;
+    const int rem = kbp - s0 - SB;
     if (rem > 0) {
       // (2) rows below: x Ubb = a; columns right: Lbb y = a (unit lower)
       if (tid < rem) {
@@ -333,7 +343,7 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
   }
   __syncthreads();
   // stage B: the off-diagonal blocks
-  inv_join<T>(D, XL, XU, tid);
+  inv_join<T>(D, XL, XU, tid, nbk);
   T* inv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
   for (int e = tid; e < NB * NB; e += 256) {
     const int i = e & (NB - 1), j = e / NB;
