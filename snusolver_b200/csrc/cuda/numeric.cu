@@ -125,6 +125,7 @@ struct Step {
 // kernel's tasks and the rank-(K1-K0) update of the rest.
 struct OuterBlock {
   int K0 = 0;
+  int ctr = 0;  // its task counter (index past the tile flags)
   BlockTask* tasks = nullptr;
   int ntasks = 0;
   GemmBatch outer;
@@ -323,7 +324,9 @@ class CudaEngine : public Engine {
       ntileflags_ = std::max<int64_t>(acc, 1);
       if ((rc = upload(d_flag_off_, fo))) return rc;
       if ((rc = alloc(d_tflags_, (size_t)(2 * ntileflags_)))) return rc;
-      if ((rc = alloc(d_fflags_, (size_t)(2 * ntileflags_)))) return rc;
+      // fused panel path: two flags per tile, then one task counter per
+      // outer-block launch (a level has no more outer blocks than tiles)
+      if ((rc = alloc(d_fflags_, (size_t)(3 * ntileflags_)))) return rc;
     }
     if ((rc = upload(d_fr_, frh_))) return rc;
     if ((rc = upload(d_gidx_, fp.gidx))) return rc;
@@ -724,7 +727,7 @@ class CudaEngine : public Engine {
     CK(cudaLaunchKernelEx(&cfg, k, (const BlockTask*)O.tasks, O.ntasks,
                           (const FrontDev*)d_fr_, F, I, O.K0, opt_.pivot_eps,
                           d_flags_, d_fflags_, (const int64_t*)d_flag_off_,
-                          d_flags_ + 5));
+                          d_fflags_ + 2 * ntileflags_ + O.ctr, d_flags_ + 5));
     return ENG_OK;
   }
 
@@ -1039,6 +1042,7 @@ class CudaEngine : public Engine {
     lv_.assign(nlevels_, LevelSched());
     int mc = fp.max_children;
     int rc;
+    int obc = 0;  // outer-block launches so far (task counters)
     for (int l = 0; l < nlevels_; l++) {
       LevelSched& L = lv_[l];
       L.f0 = fp.level_start[l];
@@ -1161,6 +1165,7 @@ class CudaEngine : public Engine {
       for (int b = 0; b < nob; b++) {
         OuterBlock& O = L.ob[b];
         O.K0 = b * OB;
+        O.ctr = obc++;
         std::vector<BlockTask> bt;
         std::vector<GemmProb> og;
         int maxrows = 0;
@@ -1362,7 +1367,7 @@ class CudaEngine : public Engine {
       const int64_t na = fp_->asm_level[nlevels_];
       int pi = prof_begin(KF_ASSEMBLE, st);
       CK(cudaMemsetAsync(F, 0, sizeof(T) * arena_, st));
-      CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 2 * ntileflags_, st));
+      CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 3 * ntileflags_, st));
       if (na > 0) {
         int blocks = (int)std::min<int64_t>((na + 255) / 256, 148 * 16);
         k_assemble<T><<<blocks, 256, 0, st>>>(d_asm_pos_, d_asm_val_, d_vals_,

@@ -21,10 +21,11 @@
 // Schur update at the end.  Tasks are listed row chunk 0 of every front,
 // then row chunk 1 of every front, ..., then the column tasks, so every wait
 // (on the owner of a tile, row chunk t < ours, or on any owner for a column
-// task) is on a task of lower index; the grid is co-resident and blocks
-// take tasks in ascending order, so the lowest unfinished task never waits
-// on an unfinished one.  Every wait is bounded (error flag, then the block
-// returns).
+// task) is on a task of lower index; the grid is co-resident and tasks
+// start in ascending order, so the lowest unfinished task never waits on an
+// unfinished one.  Blocks take the next task from a counter as they
+// come free, so tasks start in ascending order.  Every wait is bounded
+// (error flag, then the block returns).
 #pragma once
 #include "panel.cuh"
 #include "sweep.cuh"
@@ -127,15 +128,21 @@ __global__ void __launch_bounds__(256, 2)
                   const FrontDev* __restrict__ fr, T* __restrict__ F,
                   T* __restrict__ INV, int K0, double eps, int* dflags,
                   int* tflags, const int64_t* __restrict__ flag_off,
-                  int* err) {
+                  int* next_task, int* err) {
   extern __shared__ unsigned char smem_raw[];
   T* S0 = reinterpret_cast<T*>(smem_raw);
   T* S1 = S0 + NB * TLD;
   T* S2 = S1 + NB * TLD;
-  __shared__ int bad;
+  __shared__ int bad, s_task;
   if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+  for (;;) {
+    // tasks are handed out in ascending order as blocks come free (a block
+    // behind a long tile chain takes no further tasks meanwhile)
+    __syncthreads();
+    if (threadIdx.x == 0) s_task = atomicAdd(next_task, 1);
+    __syncthreads();
+    const int task = s_task;
+    if (task >= ntasks) break;
     const BlockTask tk = tasks[task];
     const FrontDev f = fr[tk.front];
     const int dim = f.p + f.q;
