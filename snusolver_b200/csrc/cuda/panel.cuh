@@ -12,6 +12,23 @@ namespace snu {
 // Shared-memory tile, column-major with one element of padding per column.
 constexpr int TLD = NB + 1;
 
+// Product tiles (the operands and results of the 64 x 64 products) are
+// column-major with leading dimension PLD: a multiple of 16 bytes, so a
+// thread reads four rows of a column, or two rows of a column, as one
+// vector; 68 (FP32) and 66 (FP64) also keep the eight columns a warp reads
+// at once in distinct banks.  The tile factorization keeps its own odd
+// stride (TLD) and hands Linv over in this layout.
+template <typename T>
+constexpr int pld() {
+  return sizeof(T) == 4 ? NB + 4 : NB + 2;
+}
+// Elements per tile buffer (the larger of the two layouts).
+template <typename T>
+constexpr int tile_elems() {
+  return NB * (pld<T>() > TLD ? pld<T>() : TLD);
+}
+
+
 // Correctly rounded reciprocal (CUDA intrinsics): multipliers are formed as
 // x * (1/p) instead of x / p, one reciprocal per pivot.
 __device__ __forceinline__ float recip_rn(float x) { return __frcp_rn(x); }
@@ -176,13 +193,15 @@ __device__ __forceinline__ void inv_join(const T* D, T* XL, T* XU, int tid,
 
 // The tile factorization of one front by the whole CTA (256 threads); D,
 // XL, XU: 3 NB x TLD shared-memory tiles.  On return XL / XU hold Linv /
-// Uinv (also written to INV) and the factored tile is back in F.
+// Uinv (also written to INV), the factored tile is back in F and, when LP
+// is given (it may be D), Linv is also in LP with leading dimension PLD.
 template <typename T>
 __device__ __forceinline__ void diag_tile(const FrontDev& f,
                                           T* __restrict__ F,
                                           T* __restrict__ INV, int k0,
                                           int step, double eps, int* flags,
-                                          T* D, T* XL, T* XU) {
+                                          T* D, T* XL, T* XU,
+                                          T* LP = nullptr) {
   __shared__ T rdiag[NB];  // 1 / U[i][i]
   const int kb = min(NB, f.p - k0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -347,8 +366,10 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
   T* inv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
   for (int e = tid; e < NB * NB; e += 256) {
     const int i = e & (NB - 1), j = e / NB;
-    inv[e] = XL[i + j * TLD];
+    const T l = XL[i + j * TLD];
+    inv[e] = l;
     inv[NB * NB + e] = XU[i + j * TLD];
+    if (LP) LP[i + j * pld<T>()] = l;  // D is free by now
   }
 }
 

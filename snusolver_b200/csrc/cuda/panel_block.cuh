@@ -38,88 +38,180 @@ struct BlockTask {
   int front, kind, chunk;  // kind 0: row chunk, 1: column chunk
 };
 
-// S(i, j) = src(i, j) for i < nr, j < nc, zero elsewhere (NB x NB tile).
+// Register tile of a thread in the 64 x 64 products: rows r0 + a (four
+// contiguous rows), columns c0 + 8 b.  A warp covers 16 rows x 32 columns.
+__device__ __forceinline__ int pb_r0() {
+  return ((threadIdx.x >> 5) & 3) * 16 + (threadIdx.x & 3) * 4;
+}
+__device__ __forceinline__ int pb_c0() {
+  return (threadIdx.x >> 7) * 32 + ((threadIdx.x >> 2) & 7);
+}
+
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
+  const double2 t0 = *reinterpret_cast<const double2*>(p);
+  const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = t0.x, v[1] = t0.y, v[2] = t1.x, v[3] = t1.y;
+}
+__device__ __forceinline__ void ld2(const float* p, float& x, float& y) {
+  const float2 t = *reinterpret_cast<const float2*>(p);
+  x = t.x, y = t.y;
+}
+__device__ __forceinline__ void ld2(const double* p, double& x, double& y) {
+  const double2 t = *reinterpret_cast<const double2*>(p);
+  x = t.x, y = t.y;
+}
+// four contiguous values from global memory through L2 (16-byte aligned)
+__device__ __forceinline__ void ldg4(const float* p, float (&v)[4]) {
+  const float4 t = __ldcg(reinterpret_cast<const float4*>(p));
+  v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+}
+__device__ __forceinline__ void ldg4(const double* p, double (&v)[4]) {
+  const double2 t0 = __ldcg(reinterpret_cast<const double2*>(p));
+  const double2 t1 = __ldcg(reinterpret_cast<const double2*>(p + 2));
+  v[0] = t0.x, v[1] = t0.y, v[2] = t1.x, v[3] = t1.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+template <typename T>
+__device__ __forceinline__ bool aligned16(const T* p) {
+  return (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+}
+
+// S(i, j) = src(i, j) for i < nr, j < nc, zero elsewhere (NB x NB tile,
+// leading dimension PLD).  Through L2: tiles written by other blocks of
+// this launch.  Four rows per vector load when the column starts are
+// 16-byte aligned, else one element per load; all loads of a thread are in
+// flight before its shared-memory stores.
 template <typename T>
 __device__ __forceinline__ void pb_load(T* S, const T* src, int64_t ld, int nr,
                                         int nc) {
-  // all 16 loads of a thread in flight before any shared-memory store
-  // (through L2: tiles written by other blocks of this launch)
-  T v[NB * NB / 256];
+  constexpr int P = pld<T>();
+  if (aligned16(src) && (ld & 3) == 0) {
+    T v[4][4];
 #pragma unroll
-  for (int q = 0; q < NB * NB / 256; q++) {
-    const int e = threadIdx.x + 256 * q, i = e & (NB - 1), j = e / NB;
-    v[q] = (i < nr && j < nc) ? __ldcg(src + i + j * ld) : (T)0;
-  }
+    for (int q = 0; q < 4; q++) {
+      const int e = threadIdx.x + 256 * q, i = (e & 15) * 4, j = e >> 4;
+      if (j < nc && i + 3 < nr) {
+        ldg4(src + i + j * ld, v[q]);
+      } else {
 #pragma unroll
-  for (int q = 0; q < NB * NB / 256; q++) {
-    const int e = threadIdx.x + 256 * q, i = e & (NB - 1), j = e / NB;
-    S[i + j * TLD] = v[q];
-  }
-}
-
-// acc = A B for NB x NB shared tiles (inner dimension kk); thread (tx, ty)
-// holds rows tx + 16 a, columns ty + 16 b.
-template <typename T>
-__device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
-                                      int kk) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b] = (T)0;
-#pragma unroll 8
-  for (int m = 0; m < kk; m++) {
-    T av[4], bv[4];
-#pragma unroll
-    for (int a = 0; a < 4; a++) av[a] = A[tx + 16 * a + m * TLD];
-#pragma unroll
-    for (int b = 0; b < 4; b++) bv[b] = B[m + (ty + 16 * b) * TLD];
-#pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-      for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
-  }
-}
-
-// dst(i, j) = acc (sub = false) or dst(i, j) -= acc (sub = true), i < nr,
-// j < nc; optionally the result also into the shared tile S.
-template <typename T>
-__device__ __forceinline__ void pb_store(T* dst, int64_t ld, int nr, int nc,
-                                         const T (&acc)[4][4], bool sub,
-                                         T* S) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  T old[4][4];
-  if (sub) {  // the 16 reads in flight together
-#pragma unroll
-    for (int b = 0; b < 4; b++)
-#pragma unroll
-      for (int a = 0; a < 4; a++) {
-        const int i = tx + 16 * a, j = ty + 16 * b;
-        old[a][b] = (i < nr && j < nc) ? __ldcg(dst + i + j * ld) : (T)0;
+        for (int a = 0; a < 4; a++)
+          v[q][a] = (j < nc && i + a < nr) ? __ldcg(src + i + a + j * ld) : (T)0;
       }
-  }
+    }
 #pragma unroll
-  for (int b = 0; b < 4; b++) {
-    const int j = ty + 16 * b;
+    for (int q = 0; q < 4; q++) {
+      const int e = threadIdx.x + 256 * q, i = (e & 15) * 4, j = e >> 4;
+      st4(S + i + j * P, v[q]);
+    }
+  } else {
+    T v[NB * NB / 256];
 #pragma unroll
-    for (int a = 0; a < 4; a++) {
-      const int i = tx + 16 * a;
-      if (i < nr && j < nc) {
-        T v = sub ? old[a][b] - acc[a][b] : acc[a][b];
-        dst[i + j * ld] = v;
-        if (S) S[i + j * TLD] = v;
-      } else if (S) {
-        S[i + j * TLD] = (T)0;
-      }
+    for (int q = 0; q < NB * NB / 256; q++) {
+      const int e = threadIdx.x + 256 * q, i = e & (NB - 1), j = e / NB;
+      v[q] = (i < nr && j < nc) ? __ldcg(src + i + j * ld) : (T)0;
+    }
+#pragma unroll
+    for (int q = 0; q < NB * NB / 256; q++) {
+      const int e = threadIdx.x + 256 * q, i = e & (NB - 1), j = e / NB;
+      S[i + j * P] = v[q];
     }
   }
 }
 
-// Dynamic shared memory: three NB x TLD tiles (the diagonal-tile
-// factorization's D / Linv / Uinv, reused as work tiles).
+// acc = A B for NB x NB shared tiles (leading dimension PLD, inner
+// dimension kk).  A is read four rows at a time, B two k at a time; the
+// operands are zero (or finite identity padding against zeros) past kk, so
+// the loop runs to kk rounded up to 8.
+template <typename T>
+__device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
+                                      int kk) {
+  constexpr int P = pld<T>();
+  const int r0 = pb_r0(), c0 = pb_c0();
+  const T* Ar = A + r0;
+  const T* Bc = B + c0 * P;
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = (T)0;
+  const int k8 = (kk + 7) & ~7;
+#pragma unroll 2
+  for (int m = 0; m < k8; m += 2) {
+    T a0[4], a1[4], b0[4], b1[4];
+    ld4(Ar + m * P, a0);
+    ld4(Ar + (m + 1) * P, a1);
+#pragma unroll
+    for (int b = 0; b < 4; b++) ld2(Bc + m + 8 * b * P, b0[b], b1[b]);
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        acc[a][b] += a0[a] * b0[b];
+        acc[a][b] += a1[a] * b1[b];
+      }
+  }
+}
+
+// dst(i, j) = acc (sub = false) or dst(i, j) -= acc (sub = true), i < nr,
+// j < nc; optionally the result also into the shared tile S (zero outside
+// nr x nc).  A thread's four rows of a column go as one vector when they
+// are all inside and 16-byte aligned.
+template <typename T>
+__device__ __forceinline__ void pb_store(T* dst, int64_t ld, int nr, int nc,
+                                         const T (&acc)[4][4], bool sub,
+                                         T* S) {
+  constexpr int P = pld<T>();
+  const int r0 = pb_r0(), c0 = pb_c0();
+  const bool vec = aligned16(dst + r0) && (ld & 3) == 0 && r0 + 3 < nr;
+  T v[4][4];  // [b][a]
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    const int j = c0 + 8 * b;
+    if (sub) {  // all reads in flight together
+      if (vec && j < nc) {
+        ldg4(dst + r0 + j * ld, v[b]);
+      } else {
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+          v[b][a] = (r0 + a < nr && j < nc) ? __ldcg(dst + r0 + a + j * ld) : (T)0;
+      }
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    const int j = c0 + 8 * b;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const bool in = r0 + a < nr && j < nc;
+      v[b][a] = in ? (sub ? v[b][a] - acc[a][b] : acc[a][b]) : (T)0;
+    }
+    if (j < nc) {
+      if (vec) {
+        st4(dst + r0 + j * ld, v[b]);
+      } else {
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+          if (r0 + a < nr) dst[r0 + a + j * ld] = v[b][a];
+      }
+    }
+    if (S) st4(S + r0 + j * P, v[b]);
+  }
+}
+
+// Dynamic shared memory: three tile buffers (the diagonal-tile
+// factorization's D / Linv / Uinv, reused as product tiles).
 template <typename T>
 constexpr size_t block_smem() {
-  return 3 * (size_t)NB * TLD * sizeof(T);
+  return 3 * (size_t)tile_elems<T>() * sizeof(T);
 }
 
 template <typename T>
@@ -129,10 +221,10 @@ __global__ void __launch_bounds__(256, 2)
                   T* __restrict__ INV, int K0, double eps, int* dflags,
                   int* tflags, const int64_t* __restrict__ flag_off,
                   int* next_task, int* err) {
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S0 = reinterpret_cast<T*>(smem_raw);
-  T* S1 = S0 + NB * TLD;
-  T* S2 = S1 + NB * TLD;
+  T* S1 = S0 + tile_elems<T>();
+  T* S2 = S1 + tile_elems<T>();
   __shared__ int bad, s_task;
   if (threadIdx.x == 0) bad = 0;
   for (;;) {
@@ -161,7 +253,8 @@ __global__ void __launch_bounds__(256, 2)
         const int step = k0 / NB;
         if (tk.chunk == t) {
           // owner: the diagonal tile (its columns are up to date)
-          diag_tile<T>(f, F, INV, k0, step, eps, dflags, S0, S1, S2);
+          // (Linv comes back in S0, product layout)
+          diag_tile<T>(f, F, INV, k0, step, eps, dflags, S0, S1, S2, S0);
           __syncthreads();
           if (deferred >= 0) {
             // the previous step's update of our rows right of this tile
@@ -171,11 +264,11 @@ __global__ void __launch_bounds__(256, 2)
             if (bad) return;
             for (int c0 = k1; c0 < K1; c0 += NB) {
               const int nc = min(NB, K1 - c0);
-              pb_load(S0, Fo + R0 + pk0 * ld, ld, nr, NB);  // our L block
+              pb_load(S1, Fo + R0 + pk0 * ld, ld, nr, NB);  // our L block
               pb_load(S2, Fo + pk0 + c0 * ld, ld, NB, nc);  // its U rows
               __syncthreads();
               T acc[4][4];
-              pb_mm(acc, S0, S2, NB);
+              pb_mm(acc, S1, S2, NB);
               pb_store(Fo + R0 + c0 * ld, ld, nr, nc, acc, true, (T*)nullptr);
               __syncthreads();
             }
@@ -184,10 +277,10 @@ __global__ void __launch_bounds__(256, 2)
           // columns) is published on its own, the next owner needs only it
           for (int c0 = k1; c0 < K1; c0 += NB) {
             const int nc = min(NB, K1 - c0);
-            pb_load(S0, Fo + k0 + c0 * ld, ld, kb, nc);
+            pb_load(S1, Fo + k0 + c0 * ld, ld, kb, nc);
             __syncthreads();
             T acc[4][4];
-            pb_mm(acc, S1, S0, kb);  // Linv A
+            pb_mm(acc, S0, S1, kb);  // Linv A
             pb_store(Fo + k0 + c0 * ld, ld, kb, nc, acc, false, (T*)nullptr);
             __syncthreads();
             if (c0 == k1 && threadIdx.x == 0) raise_flag(fl + 2 * step);
@@ -261,12 +354,12 @@ __global__ void __launch_bounds__(256, 2)
           __syncthreads();
           T acc[4][4];
           pb_mm(acc, S0, S1, NB);
-          const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+          const int r0 = pb_r0(), c0 = pb_c0();
 #pragma unroll
           for (int b = 0; b < 4; b++)
 #pragma unroll
             for (int a = 0; a < 4; a++)
-              S2[tx + 16 * a + (ty + 16 * b) * TLD] -= acc[a][b];
+              S2[r0 + a + (c0 + 8 * b) * pld<T>()] -= acc[a][b];
           __syncthreads();
         }
         // U_t = Linv_t S2
