@@ -13,14 +13,14 @@ namespace snu {
 constexpr int TLD = NB + 1;
 
 // Product tiles (the operands and results of the 64 x 64 products) are
-// column-major with leading dimension PLD: a multiple of 16 bytes, so a
-// thread reads four rows of a column, or two rows of a column, as one
-// vector; 68 (FP32) and 66 (FP64) also keep the eight columns a warp reads
-// at once in distinct banks.  The tile factorization keeps its own odd
-// stride (TLD) and hands Linv over in this layout.
+// column-major with leading dimension PLD.  FP32: 68, a multiple of 16
+// bytes, so a thread reads four rows of a column, or two rows of a column,
+// as one vector, and the eight columns a warp reads at once sit in
+// distinct banks.  FP64: the odd stride TLD (scalar loads).  The tile
+// factorization keeps TLD and hands Linv over in this layout.
 template <typename T>
 constexpr int pld() {
-  return sizeof(T) == 4 ? NB + 4 : NB + 2;
+  return sizeof(T) == 4 ? NB + 4 : TLD;
 }
 // Elements per tile buffer (the larger of the two layouts).
 template <typename T>

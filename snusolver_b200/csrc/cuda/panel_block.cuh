@@ -38,14 +38,25 @@ struct BlockTask {
   int front, kind, chunk;  // kind 0: row chunk, 1: column chunk
 };
 
-// Register tile of a thread in the 64 x 64 products: rows r0 + a (four
-// contiguous rows), columns c0 + 8 b.  A warp covers 16 rows x 32 columns.
-__device__ __forceinline__ int pb_r0() {
-  return ((threadIdx.x >> 5) & 3) * 16 + (threadIdx.x & 3) * 4;
-}
-__device__ __forceinline__ int pb_c0() {
-  return (threadIdx.x >> 7) * 32 + ((threadIdx.x >> 2) & 7);
-}
+// Register tile of a thread in the 64 x 64 products: rows r0 + RS a,
+// columns c0 + CS b (a, b < 4).  FP32: four contiguous rows (one vector
+// load), columns 8 apart, a warp covers 16 rows x 32 columns.  FP64 keeps
+// scalar loads (the products are bound by the FP64 pipe, not by shared
+// memory): rows 16 apart, columns 16 apart.
+template <typename T>
+struct PbMap {
+  static constexpr int RS = sizeof(T) == 4 ? 1 : 16;
+  static constexpr int CS = sizeof(T) == 4 ? 8 : 16;
+  __device__ __forceinline__ static int r0() {
+    return sizeof(T) == 4
+               ? ((threadIdx.x >> 5) & 3) * 16 + (threadIdx.x & 3) * 4
+               : (threadIdx.x & 15);
+  }
+  __device__ __forceinline__ static int c0() {
+    return sizeof(T) == 4 ? (threadIdx.x >> 7) * 32 + ((threadIdx.x >> 2) & 7)
+                          : (threadIdx.x >> 4);
+  }
+};
 
 __device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
   const float4 t = *reinterpret_cast<const float4*>(p);
@@ -95,7 +106,7 @@ template <typename T>
 __device__ __forceinline__ void pb_load(T* S, const T* src, int64_t ld, int nr,
                                         int nc) {
   constexpr int P = pld<T>();
-  if (aligned16(src) && (ld & 3) == 0) {
+  if (sizeof(T) == 4 && aligned16(src) && (ld & 3) == 0) {
     T v[4][4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -136,13 +147,28 @@ template <typename T>
 __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
                                       int kk) {
   constexpr int P = pld<T>();
-  const int r0 = pb_r0(), c0 = pb_c0();
+  const int r0 = PbMap<T>::r0(), c0 = PbMap<T>::c0();
   const T* Ar = A + r0;
   const T* Bc = B + c0 * P;
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b < 4; b++) acc[a][b] = (T)0;
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll 8
+    for (int m = 0; m < kk; m++) {
+      T av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; a++) av[a] = Ar[16 * a + m * P];
+#pragma unroll
+      for (int b = 0; b < 4; b++) bv[b] = Bc[m + 16 * b * P];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
+    }
+    return;
+  }
   const int k8 = (kk + 7) & ~7;
 #pragma unroll 2
   for (int m = 0; m < k8; m += 2) {
@@ -169,29 +195,32 @@ template <typename T>
 __device__ __forceinline__ void pb_store(T* dst, int64_t ld, int nr, int nc,
                                          const T (&acc)[4][4], bool sub,
                                          T* S) {
-  constexpr int P = pld<T>();
-  const int r0 = pb_r0(), c0 = pb_c0();
-  const bool vec = aligned16(dst + r0) && (ld & 3) == 0 && r0 + 3 < nr;
+  constexpr int P = pld<T>(), RS = PbMap<T>::RS, CS = PbMap<T>::CS;
+  const int r0 = PbMap<T>::r0(), c0 = PbMap<T>::c0();
+  const bool vec =
+      RS == 1 && aligned16(dst + r0) && (ld & 3) == 0 && r0 + 3 < nr;
   T v[4][4];  // [b][a]
 #pragma unroll
   for (int b = 0; b < 4; b++) {
-    const int j = c0 + 8 * b;
+    const int j = c0 + CS * b;
     if (sub) {  // all reads in flight together
       if (vec && j < nc) {
         ldg4(dst + r0 + j * ld, v[b]);
       } else {
 #pragma unroll
-        for (int a = 0; a < 4; a++)
-          v[b][a] = (r0 + a < nr && j < nc) ? __ldcg(dst + r0 + a + j * ld) : (T)0;
+        for (int a = 0; a < 4; a++) {
+          const int i = r0 + RS * a;
+          v[b][a] = (i < nr && j < nc) ? __ldcg(dst + i + j * ld) : (T)0;
+        }
       }
     }
   }
 #pragma unroll
   for (int b = 0; b < 4; b++) {
-    const int j = c0 + 8 * b;
+    const int j = c0 + CS * b;
 #pragma unroll
     for (int a = 0; a < 4; a++) {
-      const bool in = r0 + a < nr && j < nc;
+      const bool in = r0 + RS * a < nr && j < nc;
       v[b][a] = in ? (sub ? v[b][a] - acc[a][b] : acc[a][b]) : (T)0;
     }
     if (j < nc) {
@@ -200,10 +229,17 @@ __device__ __forceinline__ void pb_store(T* dst, int64_t ld, int nr, int nc,
       } else {
 #pragma unroll
         for (int a = 0; a < 4; a++)
-          if (r0 + a < nr) dst[r0 + a + j * ld] = v[b][a];
+          if (r0 + RS * a < nr) dst[r0 + RS * a + j * ld] = v[b][a];
       }
     }
-    if (S) st4(S + r0 + j * P, v[b]);
+    if (S) {
+      if (RS == 1) {
+        st4(S + r0 + j * P, v[b]);
+      } else {
+#pragma unroll
+        for (int a = 0; a < 4; a++) S[r0 + RS * a + j * P] = v[b][a];
+      }
+    }
   }
 }
 
@@ -354,12 +390,13 @@ __global__ void __launch_bounds__(256, 2)
           __syncthreads();
           T acc[4][4];
           pb_mm(acc, S0, S1, NB);
-          const int r0 = pb_r0(), c0 = pb_c0();
+          const int r0 = PbMap<T>::r0(), c0 = PbMap<T>::c0();
 #pragma unroll
           for (int b = 0; b < 4; b++)
 #pragma unroll
             for (int a = 0; a < 4; a++)
-              S2[r0 + a + (c0 + 8 * b) * pld<T>()] -= acc[a][b];
+              S2[r0 + PbMap<T>::RS * a + (c0 + PbMap<T>::CS * b) * pld<T>()] -=
+                  acc[a][b];
           __syncthreads();
         }
         // U_t = Linv_t S2
