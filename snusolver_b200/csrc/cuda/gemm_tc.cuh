@@ -184,6 +184,17 @@ constexpr size_t tc_smem_bytes() {
 
 // ----------------------------------------------------------------- GEMM
 
+// Bulk prefetch into L2 of n floats from p (rounded out to 16 bytes; the
+// callers' spans are front columns, whose starts and ends at ld are
+// 16-byte aligned).
+__device__ __forceinline__ void prefetch_l2_span(const float* p, int n) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)15;
+  const uintptr_t e = (reinterpret_cast<uintptr_t>(p + n) + 15) & ~(uintptr_t)15;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a),
+               "r"((uint32_t)(e - a))
+               : "memory");
+}
+
 __global__ void __launch_bounds__(128, 1)
     k_gemm_tc(const TcTile* __restrict__ tiles, const TcProb* __restrict__ probs,
               const CUtensorMap* __restrict__ amaps,
@@ -193,6 +204,7 @@ __global__ void __launch_bounds__(128, 1)
   __shared__ uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES], acc_bar;
   __shared__ uint32_t tmem_base_s;
   __shared__ int failed_s;
+  __shared__ int rel_r[TC_BM], rel_c[TC_BN];  // scatter map of the tile
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   float* As = (float*)smem;                                   // [STAGES][BM*BK]
   float* Bs = As + (size_t)TC_STAGES * TC_BM * TC_BK;         // [STAGES][BN*BK]
@@ -260,6 +272,19 @@ __global__ void __launch_bounds__(128, 1)
       tc_commit(&empty_bar[s]);
     }
     tc_commit(&acc_bar);  // also after an early exit: drains issued MMAs
+  } else if (warp >= 2) {
+    // while the main loop runs: the tile's columns of C into L2 and the
+    // scatter map into shared memory, for the epilogue
+    const int t = threadIdx.x - 64;
+    const int r0 = tl.tm * TC_BM, c0 = tl.tn * TC_BN;
+    const int nr = min(TC_BM, pr.m - r0), ncl = min(TC_BN, pr.n - c0);
+    for (int c = t; c < ncl; c += 64)
+      prefetch_l2_span(F + pr.c + r0 + (int64_t)(c0 + c) * pr.ldc, nr);
+    if (pr.pc >= 0) {
+      const int* rel = rel_base + pr.rel;
+      for (int i = t; i < TC_BM; i += 64) rel_r[i] = i < nr ? rel[r0 + i] : 0;
+      for (int j = t; j < TC_BN; j += 64) rel_c[j] = j < ncl ? rel[c0 + j] : 0;
+    }
   }
   __syncthreads();  // every role has finished issuing
 
@@ -299,12 +324,11 @@ __global__ void __launch_bounds__(128, 1)
           cv[j] = j < ncol ? cp[(int64_t)j * pr.ldc] : 0.f;
         if (pr.pc >= 0) {
           // extend-add fused: the child's update goes straight to the parent
-          const int* rel = rel_base + pr.rel;
-          float* prow = F + pr.pc + rel[row];
+          float* prow = F + pr.pc + rel_r[warp * 32 + lane];
 #pragma unroll
           for (int j = 0; j < 32; j++)
             if (j < ncol)
-              atomicAdd(prow + (int64_t)rel[colbase + j] * pr.pld,
+              atomicAdd(prow + (int64_t)rel_c[c0 + j] * pr.pld,
                         cv[j] - __uint_as_float(v[j]));
         } else {
 #pragma unroll
