@@ -479,13 +479,21 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
     int i = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
       const int a = i & 1;
+      const TcTile tl = tiles[t];
+      const TcProb pr = probs[tl.prob];
+      {
+        // this warp's rows of C into L2 while the tile's MMAs run
+        const int r0 = tl.tm * TC_BM + qtr * 32, ct = tl.tn * TC_BN;
+        const int nr = min(32, pr.m - r0), ncl = min(TC_BN, pr.n - ct);
+        if (nr > 0)
+          for (int c = lane; c < ncl; c += 32)
+            prefetch_l2_span(F + pr.c + r0 + (int64_t)(ct + c) * pr.ldc, nr);
+      }
       if (abort_s || !mbar_wait(&acc_full[a], (i >> 1) & 1, err)) {
         abort_s = 1;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const TcTile tl = tiles[t];
-      const TcProb pr = probs[tl.prob];
       const int row = tl.tm * TC_BM + qtr * 32 + lane;
       float* Cc = F + pr.c;
       for (int c0 = 0; c0 < TC_BN; c0 += 32) {
