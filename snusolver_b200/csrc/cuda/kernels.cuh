@@ -180,22 +180,29 @@ __global__ void k_solve_init(const int* __restrict__ list,
 
 // Update vectors of children (their Q rows after the forward sweep) are
 // added into the parent's work vector; all children of a level in one
-// launch, siblings meeting on a parent row add with atomics.
+// launch, one block per 256 Q rows of a child (task.j = the first row),
+// one thread per row for all right-hand sides; siblings meeting on a parent
+// row add with atomics.  nrhs <= 16 (the tree solve's column group).
 template <typename T>
-__global__ void k_solve_ea(const int* __restrict__ list,
-                           const FrontDev* __restrict__ fr,
-                           const int* __restrict__ rel, int nrhs,
-                           T* __restrict__ W) {
-  const FrontDev c = fr[list[blockIdx.x]];
+__global__ void __launch_bounds__(256)
+    k_solve_ea(const EaTask* __restrict__ tasks,
+               const FrontDev* __restrict__ fr, const int* __restrict__ rel,
+               int nrhs, T* __restrict__ W) {
+  const EaTask t = tasks[blockIdx.x];
+  const FrontDev c = fr[t.child];
+  const int i = t.j + threadIdx.x;
+  if (i >= c.q) return;
   const FrontDev pf = fr[c.parent];
   const int dimc = c.p + c.q, dimp = pf.p + pf.q;
-  const T* src = W + c.w_off * nrhs;
-  T* dst = W + pf.w_off * nrhs;
-  const int* r = rel + c.rel_off;
-  for (int e = threadIdx.x; e < c.q * nrhs; e += blockDim.x) {
-    int i = e % c.q, k = e / c.q;
-    atomicAdd(dst + r[i] + (int64_t)k * dimp, src[c.p + i + (int64_t)k * dimc]);
-  }
+  const T* src = W + c.w_off * nrhs + c.p + i;
+  T* dst = W + pf.w_off * nrhs + rel[c.rel_off + i];
+  T v[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++)
+    if (k < nrhs) v[k] = src[(int64_t)k * dimc];
+#pragma unroll
+  for (int k = 0; k < 16; k++)
+    if (k < nrhs) atomicAdd(dst + (int64_t)k * dimp, v[k]);
 }
 
 // ------------------------------------------------ FP64 refinement helpers

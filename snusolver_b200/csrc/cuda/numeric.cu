@@ -139,8 +139,8 @@ struct LevelSched {
   int64_t asm0 = 0, asm1 = 0;
   std::vector<EaTask*> ea;  // per child rank
   std::vector<int> nea;
-  int* ea_kids = nullptr;  // children of the level's fronts (solve)
-  int nea_kids = 0;
+  EaTask* ea_kids = nullptr;  // (child, first of 256 Q rows) of the level's
+  int nea_kids = 0;           // fronts' children (solve extend-add)
   int* list = nullptr;  // fronts of the level
   int* listq = nullptr; // fronts of the level with q > 0
   int nlistq = 0;
@@ -323,7 +323,10 @@ class CudaEngine : public Engine {
       }
       ntileflags_ = std::max<int64_t>(acc, 1);
       if ((rc = upload(d_flag_off_, fo))) return rc;
-      if ((rc = alloc(d_tflags_, (size_t)(2 * ntileflags_)))) return rc;
+      // solve sweeps: one flag per tile and direction, then one task
+      // counter per level and direction
+      if ((rc = alloc(d_tflags_, (size_t)(2 * ntileflags_ + 2 * nlevels_ + 2))))
+        return rc;
       // fused panel path: two flags per tile, then one task counter per
       // outer-block launch (a level has no more outer blocks than tiles)
       if ((rc = alloc(d_fflags_, (size_t)(3 * ntileflags_)))) return rc;
@@ -767,9 +770,11 @@ class CudaEngine : public Engine {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int* fl = d_tflags_ + (fwd ? 0 : ntileflags_);
+    int* ctr = d_tflags_ + 2 * ntileflags_ + 2 * std::max(cur_level_, 0) +
+               (fwd ? 0 : 1);
     ++launches_;
     CK(cudaLaunchKernelEx(&cfg, k, tasks, ntasks, (const FrontDev*)d_fr_, F, I,
-                          (const int64_t*)d_flag_off_, nrhs, W, Y, fl,
+                          (const int64_t*)d_flag_off_, nrhs, W, Y, fl, ctr,
                           d_flags_ + 4));
     return ENG_OK;
   }
@@ -1068,13 +1073,13 @@ class CudaEngine : public Engine {
       L.ea_elems.assign(mc, 0.0);
       for (int f = L.f0; f < L.f1; f++)
         L.solve_elems += fp.fronts[f].p + fp.fronts[f].q;
-      std::vector<int> kids;
+      std::vector<EaTask> kids;
       for (int r = 0; r < mc; r++) {
         int b0 = fp.ea_ptr[(size_t)l * mc + r], b1 = fp.ea_ptr[(size_t)l * mc + r + 1];
         std::vector<EaTask> tasks;
         for (int k = b0; k < b1; k++) {
           int c = fp.ea_child[k];
-          kids.push_back(c);
+          for (int i0 = 0; i0 < fp.fronts[c].q; i0 += 256) kids.push_back({c, i0});
           for (int j = 0; j < fp.fronts[c].q; j++) tasks.push_back({c, j});
           L.ea_elems[r] += (double)fp.fronts[c].q * fp.fronts[c].q;
         }
@@ -1433,7 +1438,12 @@ class CudaEngine : public Engine {
                  double* X, int ldx, int nrhs, cudaStream_t st) {
     const double es = sizeof(T);
     int pi, rc;
-    CK(cudaMemsetAsync(d_tflags_, 0, sizeof(int) * 2 * ntileflags_, st));
+    if (nrhs < 1 || nrhs > RG) {  // the kernels hold at most RG columns
+      err_ = "tree solve of more than 16 columns at once";
+      return ENG_EINVAL;
+    }
+    CK(cudaMemsetAsync(d_tflags_, 0,
+                       sizeof(int) * (2 * ntileflags_ + 2 * nlevels_ + 2), st));
     for (int l = 0; l < nlevels_; l++) {
       LevelSched& L = lv_[l];
       cur_level_ = l;

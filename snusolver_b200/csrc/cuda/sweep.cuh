@@ -114,8 +114,8 @@ __device__ __forceinline__ void tile_apply(const T* Xs, T (*in)[R],
 // Forward sweep of the pivot blocks of one level.  Tasks are (front, chunk)
 // with the chunks of a front in ascending order, so every chunk waits only
 // on tasks of lower index; the grid is co-resident (cooperative launch) and
-// every block takes its tasks in ascending order, which rules out a cycle
-// of waits.  Tile s: y_s = Linv_s W[k0:k1]; W[r] -= L[r, k0:k1] y_s, r >= k1.
+// blocks take tasks from a counter as they come free, so tasks start in
+// ascending order, which rules out a cycle of waits.  Tile s: y_s = Linv_s W[k0:k1]; W[r] -= L[r, k0:k1] y_s, r >= k1.
 // The factor columns and inverse of tile s+1 are staged (double buffer)
 // while tile s waits for its flag and is applied.
 template <typename T, int R>
@@ -124,19 +124,24 @@ __global__ void __launch_bounds__(DIAG_ROWS)
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                const T* __restrict__ INV, const int64_t* __restrict__ flag_off,
                int nrhs, T* __restrict__ W, T* __restrict__ Y, int* flags,
-               int* err) {
+               int* next_task, int* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls0 = reinterpret_cast<T*>(smem_raw);  // [2][NB][DIAG_ROWS]
   T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;         // [2][NB * NB]
   __shared__ T ws[NB][R];
   __shared__ T ys[NB][R];
   __shared__ T Wc[R][DIAG_ROWS];  // this chunk's rows of W (nrhs <= R)
-  __shared__ int bad;
+  __shared__ int bad, s_task;
   const int tid = threadIdx.x;
   constexpr int V = 16 / sizeof(T);
   if (tid == 0) bad = 0;
-  __syncthreads();
-  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+  for (;;) {
+    // tasks start in ascending order as blocks come free
+    __syncthreads();
+    if (tid == 0) s_task = atomicAdd(next_task, 1);
+    __syncthreads();
+    const int task = s_task;
+    if (task >= ntasks) break;
     const SweepTask t = tasks[task];
     const FrontDev f = fr[t.front];
     const int dim = f.p + f.q;
@@ -229,18 +234,22 @@ __global__ void __launch_bounds__(DIAG_ROWS)
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                const T* __restrict__ INV, const int64_t* __restrict__ flag_off,
                int nrhs, T* __restrict__ W, T* __restrict__ Y, int* flags,
-               int* err) {
+               int* next_task, int* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls0 = reinterpret_cast<T*>(smem_raw);
   T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;
   __shared__ T ws[NB][R];
   __shared__ T xs[NB][R];
   __shared__ T Wc[R][DIAG_ROWS];  // this chunk's rows of W (nrhs <= R)
-  __shared__ int bad;
+  __shared__ int bad, s_task;
   const int tid = threadIdx.x;
   if (tid == 0) bad = 0;
-  __syncthreads();
-  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_task = atomicAdd(next_task, 1);
+    __syncthreads();
+    const int task = s_task;
+    if (task >= ntasks) break;
     const SweepTask t = tasks[task];
     const FrontDev f = fr[t.front];
     const int dim = f.p + f.q;
