@@ -360,7 +360,13 @@ __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
                                          const T* __restrict__ F, int nrhs,
                                          T* __restrict__ W,
                                          const T* __restrict__ Y) {
-  __shared__ T red[4][GEMV_ROWS][R + 1];
+  // the block's slice of the source vector, then (after the products) the
+  // reduction of the four k-groups, in one buffer
+  constexpr size_t YS = sizeof(T) * GEMV_K * R,
+                   RED = sizeof(T) * 4 * GEMV_ROWS * (R + 1);
+  __shared__ __align__(16) unsigned char smb[YS > RED ? YS : RED];
+  T(*ys)[R] = reinterpret_cast<T(*)[R]>(smb);
+  T(*red)[GEMV_ROWS][R + 1] = reinterpret_cast<T(*)[GEMV_ROWS][R + 1]>(smb);
   const SweepTask t = tasks[blockIdx.x];
   const FrontDev f = fr[t.front];
   const int dim = f.p + f.q;
@@ -375,6 +381,14 @@ __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
   T* dst = FWD ? Wf + f.p : Wf;
   for (int r0 = 0; r0 < nrhs; r0 += R) {
     const int nr = min(R, nrhs - r0);
+    __syncthreads();  // the previous pass's reduction is read
+    for (int e = threadIdx.x; e < GEMV_K * R; e += blockDim.x) {
+      const int k = e % GEMV_K, r = e / GEMV_K;
+      ys[k][r] = (kc0 + k < kc1 && r < nr)
+                     ? src[kc0 + k + (int64_t)(r0 + r) * lds]
+                     : (T)0;
+    }
+    __syncthreads();
     T acc[R];
 #pragma unroll
     for (int r = 0; r < R; r++) acc[r] = (T)0;
@@ -387,9 +401,7 @@ __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
           const int k = k0 + 4 * u;
           av[u] = k < kc1 ? a[(int64_t)k * f.ld] : (T)0;
 #pragma unroll
-          for (int r = 0; r < R; r++)
-            wv[u][r] = (k < kc1 && r < nr) ? src[k + (int64_t)(r0 + r) * lds]
-                                           : (T)0;
+          for (int r = 0; r < R; r++) wv[u][r] = ys[min(k, kc1 - 1) - kc0][r];
         }
 #pragma unroll
         for (int u = 0; u < UB; u++)
@@ -397,6 +409,7 @@ __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
           for (int r = 0; r < R; r++) acc[r] += av[u] * wv[u][r];
       }
     }
+    __syncthreads();  // ys is read
 #pragma unroll
     for (int r = 0; r < R; r++) red[g][threadIdx.x & 63][r] = acc[r];
     __syncthreads();
