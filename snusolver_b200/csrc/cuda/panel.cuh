@@ -195,13 +195,16 @@ __device__ __forceinline__ void inv_join(const T* D, T* XL, T* XU, int tid,
 // XL, XU: 3 NB x TLD shared-memory tiles.  On return XL / XU hold Linv /
 // Uinv (also written to INV), the factored tile is back in F and, when LP
 // is given (it may be D), Linv is also in LP with leading dimension PLD.
+// pre: the tile already in shared memory (leading dimension PLD), instead
+// of loading it from the front.
 template <typename T>
 __device__ __forceinline__ void diag_tile(const FrontDev& f,
                                           T* __restrict__ F,
                                           T* __restrict__ INV, int k0,
                                           int step, double eps, int* flags,
                                           T* D, T* XL, T* XU,
-                                          T* LP = nullptr) {
+                                          T* LP = nullptr,
+                                          const T* pre = nullptr) {
   __shared__ T rdiag[NB];  // 1 / U[i][i]
   const int kb = min(NB, f.p - k0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -211,14 +214,18 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
   if (tid >= kbp && tid < NB) rdiag[tid] = (T)1;
   T* base = F + f.off + k0 + (int64_t)k0 * f.ld;
   {
-    // all 16 loads of a thread in flight before the shared-memory stores
+    // all 16 loads of a thread in flight before the shared-memory stores;
+    // the tile comes from the front, or from pre (leading dimension PLD)
+    // when the caller already holds it (pre may alias XL or XU)
     T v[NB * NB / 256];
 #pragma unroll
     for (int q = 0; q < NB * NB / 256; q++) {
       const int e = tid + 256 * q, i = e & (NB - 1), j = e / NB;
-      v[q] = (i < kb && j < kb) ? __ldcg(base + i + (int64_t)j * f.ld)
-                                : (i == j ? (T)1 : (T)0);
+      v[q] = (i < kb && j < kb)
+                 ? (pre ? pre[i + j * pld<T>()] : __ldcg(base + i + (int64_t)j * f.ld))
+                 : (i == j ? (T)1 : (T)0);
     }
+    if (pre) __syncthreads();
 #pragma unroll
     for (int q = 0; q < NB * NB / 256; q++) {
       const int e = tid + 256 * q, i = e & (NB - 1), j = e / NB;

@@ -284,39 +284,45 @@ __global__ void __launch_bounds__(256, 2)
     if (tk.kind == 0) {
       const int R0 = K0 + NB * tk.chunk, nr = min(NB, dim - R0);
       int deferred = -1;  // step whose remaining column chunks wait
+      bool pre = false;   // S1 holds our updated diagonal tile
       for (int t = 0; t < nt; t++) {
         const int k0 = K0 + NB * t, kb = min(NB, f.p - k0), k1 = k0 + kb;
         const int step = k0 / NB;
         if (tk.chunk == t) {
           // owner: the diagonal tile (its columns are up to date)
-          // (Linv comes back in S0, product layout)
-          diag_tile<T>(f, F, INV, k0, step, eps, dflags, S0, S1, S2, S0);
+          // (Linv comes back in S0, product layout; the tile from S1 when
+          // our update of the previous step left it there)
+          diag_tile<T>(f, F, INV, k0, step, eps, dflags, S0, S1, S2, S0,
+                       pre ? S1 : (const T*)nullptr);
           __syncthreads();
+          const int pk0 = K0 + NB * max(deferred, 0);
           if (deferred >= 0) {
             // the previous step's update of our rows right of this tile
-            const int pk0 = K0 + NB * deferred, pstep = pk0 / NB;
-            if (threadIdx.x == 0 && !wait_flag(fl + 2 * pstep + 1, err)) bad = 1;
+            if (threadIdx.x == 0 && !wait_flag(fl + 2 * (pk0 / NB) + 1, err))
+              bad = 1;
             __syncthreads();
             if (bad) return;
-            for (int c0 = k1; c0 < K1; c0 += NB) {
-              const int nc = min(NB, K1 - c0);
-              pb_load(S1, Fo + R0 + pk0 * ld, ld, nr, NB);  // our L block
-              pb_load(S2, Fo + pk0 + c0 * ld, ld, NB, nc);  // its U rows
-              __syncthreads();
-              T acc[4][4];
-              pb_mm(acc, S1, S2, NB);
-              pb_store(Fo + R0 + c0 * ld, ld, nr, nc, acc, true, (T*)nullptr);
-              __syncthreads();
-            }
+            pb_load(S1, Fo + R0 + pk0 * ld, ld, nr, NB);  // our L block
           }
-          // U rows inside the block: the first chunk (the next tile's
-          // columns) is published on its own, the next owner needs only it
+          // per column chunk right of the tile: the deferred update of our
+          // rows, then the U rows (U = Linv A); the first chunk (the next
+          // tile's columns) is published on its own, the next owner needs
+          // only it
           for (int c0 = k1; c0 < K1; c0 += NB) {
             const int nc = min(NB, K1 - c0);
-            pb_load(S1, Fo + k0 + c0 * ld, ld, kb, nc);
-            __syncthreads();
             T acc[4][4];
-            pb_mm(acc, S0, S1, kb);  // Linv A
+            bool have = false;  // S2 holds our updated rows of these columns
+            if (deferred >= 0) {
+              pb_load(S2, Fo + pk0 + c0 * ld, ld, NB, nc);  // its U rows
+              __syncthreads();
+              pb_mm(acc, S1, S2, NB);
+              __syncthreads();
+              pb_store(Fo + R0 + c0 * ld, ld, nr, nc, acc, true, S2);
+              have = kb == NB;  // (a partial tile would hold L rows past kb)
+            }
+            if (!have) pb_load(S2, Fo + k0 + c0 * ld, ld, kb, nc);
+            __syncthreads();
+            pb_mm(acc, S0, S2, kb);  // Linv A
             pb_store(Fo + k0 + c0 * ld, ld, kb, nc, acc, false, (T*)nullptr);
             __syncthreads();
             if (c0 == k1 && threadIdx.x == 0) raise_flag(fl + 2 * step);
@@ -368,7 +374,10 @@ __global__ void __launch_bounds__(256, 2)
           pb_load(S2, Fo + k0 + c0 * ld, ld, kb, nc);  // U (from the owner)
           __syncthreads();
           pb_mm(acc, S0, S2, kb);
-          pb_store(Fo + R0 + c0 * ld, ld, nr, nc, acc, true, (T*)nullptr);
+          // the next owner keeps its updated tile in S1 (free: Uinv is used)
+          pb_store(Fo + R0 + c0 * ld, ld, nr, nc, acc, true,
+                   next_owner ? S1 : (T*)nullptr);
+          pre = next_owner;
           __syncthreads();
         }
       }
