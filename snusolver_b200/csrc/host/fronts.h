@@ -64,8 +64,10 @@ struct FrontPlan {
 struct FrontOptions {
   int relax_small = 16;    // merge child into parent if both fronts' pivot
                            // counts add up to at most this
-  double relax_zeros = 0.15;  // ... or if the merged front adds at most this
-                              // fraction of explicit zeros
+  double relax_zeros = 0.30;  // ... or if the merged front adds at most this
+                              // fraction of explicit zeros (0.30 measured
+                              // best of 0.15-0.5 on 3D and 2D grids: fewer,
+                              // larger leaf fronts for ~1% more flops)
   int relax_max_p = 256;      // never grow a merged front beyond this many pivots
 };
 
