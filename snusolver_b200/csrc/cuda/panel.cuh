@@ -29,6 +29,46 @@ constexpr int tile_elems() {
 }
 
 
+// Vector shared/global accesses of four (or two) contiguous elements.
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
+  const double2 t0 = *reinterpret_cast<const double2*>(p);
+  const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = t0.x, v[1] = t0.y, v[2] = t1.x, v[3] = t1.y;
+}
+__device__ __forceinline__ void ld2(const float* p, float& x, float& y) {
+  const float2 t = *reinterpret_cast<const float2*>(p);
+  x = t.x, y = t.y;
+}
+__device__ __forceinline__ void ld2(const double* p, double& x, double& y) {
+  const double2 t = *reinterpret_cast<const double2*>(p);
+  x = t.x, y = t.y;
+}
+// four contiguous values from global memory through L2 (16-byte aligned)
+__device__ __forceinline__ void ldg4(const float* p, float (&v)[4]) {
+  const float4 t = __ldcg(reinterpret_cast<const float4*>(p));
+  v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+}
+__device__ __forceinline__ void ldg4(const double* p, double (&v)[4]) {
+  const double2 t0 = __ldcg(reinterpret_cast<const double2*>(p));
+  const double2 t1 = __ldcg(reinterpret_cast<const double2*>(p + 2));
+  v[0] = t0.x, v[1] = t0.y, v[2] = t1.x, v[3] = t1.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+template <typename T>
+__device__ __forceinline__ bool aligned16(const T* p) {
+  return (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+}
+
 // Correctly rounded reciprocal (CUDA intrinsics): multipliers are formed as
 // x * (1/p) instead of x / p, one reciprocal per pivot.
 __device__ __forceinline__ float recip_rn(float x) { return __frcp_rn(x); }
@@ -333,10 +373,22 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
       __syncthreads();
     }
   }
-  // factored tile back to the front
-  for (int e = tid; e < NB * NB; e += 256) {
-    const int i = e & (NB - 1), j = e / NB;
-    if (i < kb && j < kb) base[i + (int64_t)j * f.ld] = D[i + j * TLD];
+  // factored tile back to the front (four rows per vector store when the
+  // tile is full and its columns are 16-byte aligned)
+  if (kb == NB && aligned16(base) && (f.ld & 3) == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = tid + 256 * q, i = (e & 15) * 4, j = e >> 4;
+      T v[4];
+#pragma unroll
+      for (int a = 0; a < 4; a++) v[a] = D[i + a + j * TLD];
+      st4(base + i + (int64_t)j * f.ld, v);
+    }
+  } else {
+    for (int e = tid; e < NB * NB; e += 256) {
+      const int i = e & (NB - 1), j = e / NB;
+      if (i < kb && j < kb) base[i + (int64_t)j * f.ld] = D[i + j * TLD];
+    }
   }
   // inverses, stage A: SB x SB diagonal blocks; warps 0-3 Linv, 4-7 Uinv;
   // lane j (< SB) computes column j of its block
@@ -371,12 +423,35 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
   // stage B: the off-diagonal blocks
   inv_join<T>(D, XL, XU, tid, nbk);
   T* inv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
-  for (int e = tid; e < NB * NB; e += 256) {
-    const int i = e & (NB - 1), j = e / NB;
-    const T l = XL[i + j * TLD];
-    inv[e] = l;
-    inv[NB * NB + e] = XU[i + j * TLD];
-    if (LP) LP[i + j * pld<T>()] = l;  // D is free by now
+  if (aligned16(inv)) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = tid + 256 * q, i = (e & 15) * 4, j = e >> 4;
+      T l[4], u[4];
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        l[a] = XL[i + a + j * TLD];
+        u[a] = XU[i + a + j * TLD];
+      }
+      st4(inv + i + j * NB, l);
+      st4(inv + NB * NB + i + j * NB, u);
+      if (LP) {  // D is free by now
+        if (pld<T>() % 4 == 0) {
+          st4(LP + i + j * pld<T>(), l);
+        } else {
+#pragma unroll
+          for (int a = 0; a < 4; a++) LP[i + a + j * pld<T>()] = l[a];
+        }
+      }
+    }
+  } else {
+    for (int e = tid; e < NB * NB; e += 256) {
+      const int i = e & (NB - 1), j = e / NB;
+      const T l = XL[i + j * TLD];
+      inv[e] = l;
+      inv[NB * NB + e] = XU[i + j * TLD];
+      if (LP) LP[i + j * pld<T>()] = l;  // D is free by now
+    }
   }
 }
 

@@ -58,45 +58,6 @@ struct PbMap {
   }
 };
 
-__device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
-  const float4 t = *reinterpret_cast<const float4*>(p);
-  v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
-}
-__device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
-  const double2 t0 = *reinterpret_cast<const double2*>(p);
-  const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
-  v[0] = t0.x, v[1] = t0.y, v[2] = t1.x, v[3] = t1.y;
-}
-__device__ __forceinline__ void ld2(const float* p, float& x, float& y) {
-  const float2 t = *reinterpret_cast<const float2*>(p);
-  x = t.x, y = t.y;
-}
-__device__ __forceinline__ void ld2(const double* p, double& x, double& y) {
-  const double2 t = *reinterpret_cast<const double2*>(p);
-  x = t.x, y = t.y;
-}
-// four contiguous values from global memory through L2 (16-byte aligned)
-__device__ __forceinline__ void ldg4(const float* p, float (&v)[4]) {
-  const float4 t = __ldcg(reinterpret_cast<const float4*>(p));
-  v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
-}
-__device__ __forceinline__ void ldg4(const double* p, double (&v)[4]) {
-  const double2 t0 = __ldcg(reinterpret_cast<const double2*>(p));
-  const double2 t1 = __ldcg(reinterpret_cast<const double2*>(p + 2));
-  v[0] = t0.x, v[1] = t0.y, v[2] = t1.x, v[3] = t1.y;
-}
-__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
-  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-}
-__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
-  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
-  *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
-}
-template <typename T>
-__device__ __forceinline__ bool aligned16(const T* p) {
-  return (reinterpret_cast<uintptr_t>(p) & 15) == 0;
-}
-
 // S(i, j) = src(i, j) for i < nr, j < nc, zero elsewhere (NB x NB tile,
 // leading dimension PLD).  Through L2: tiles written by other blocks of
 // this launch.  Four rows per vector load when the column starts are
