@@ -19,12 +19,12 @@ constexpr int TLD = NB + 1;
 // distinct banks.  FP64: the odd stride TLD (scalar loads).  The tile
 // factorization keeps TLD and hands Linv over in this layout.
 template <typename T>
-constexpr int pld() {
+__host__ __device__ constexpr int pld() {
   return sizeof(T) == 4 ? NB + 4 : TLD;
 }
 // Elements per tile buffer (the larger of the two layouts).
 template <typename T>
-constexpr int tile_elems() {
+__host__ __device__ constexpr int tile_elems() {
   return NB * (pld<T>() > TLD ? pld<T>() : TLD);
 }
 
