@@ -171,10 +171,16 @@ __global__ void k_solve_init(const int* __restrict__ list,
   const int dim = f.p + f.q;
   T* w = W + f.w_off * nrhs;
   const int* g = gidx + f.idx_off;
-  for (int e = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x;
-       e < dim * nrhs; e += SOLVE_SPLIT * blockDim.x) {
-    int t = e % dim, r = e / dim;
-    w[t + (int64_t)r * dim] = t < f.p ? (T)B[g[t] + (int64_t)r * ldb] : (T)0;
+  // one row per thread (its index once), all right-hand sides
+  for (int t = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x; t < dim;
+       t += SOLVE_SPLIT * blockDim.x) {
+    if (t < f.p) {
+      const int64_t gt = g[t];
+      for (int r = 0; r < nrhs; r++)
+        w[t + (int64_t)r * dim] = (T)B[gt + (int64_t)r * ldb];
+    } else {
+      for (int r = 0; r < nrhs; r++) w[t + (int64_t)r * dim] = (T)0;
+    }
   }
 }
 

@@ -340,11 +340,17 @@ __global__ void k_bwd_init(const int* __restrict__ list,
   T* w = W + f.w_off * nrhs;
   const T* y = Y + f.y_off * nrhs;
   const int* g = gidx + f.idx_off;
-  for (int e = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x;
-       e < dim * nrhs; e += SOLVE_SPLIT * blockDim.x) {
-    int t = e % dim, r = e / dim;
-    w[t + (int64_t)r * dim] = t < f.p ? y[t + (int64_t)r * f.p]
-                                      : (T)X[g[t] + (int64_t)r * ldx];
+  // one row per thread (its index once), all right-hand sides
+  for (int t = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x; t < dim;
+       t += SOLVE_SPLIT * blockDim.x) {
+    if (t < f.p) {
+      for (int r = 0; r < nrhs; r++)
+        w[t + (int64_t)r * dim] = y[t + (int64_t)r * f.p];
+    } else {
+      const int64_t gt = g[t];
+      for (int r = 0; r < nrhs; r++)
+        w[t + (int64_t)r * dim] = (T)X[gt + (int64_t)r * ldx];
+    }
   }
 }
 
@@ -450,10 +456,11 @@ __global__ void k_scatter_y(const int* __restrict__ list,
   const FrontDev f = fr[list[blockIdx.x / SOLVE_SPLIT]];
   const T* y = Y + f.y_off * nrhs;
   const int* g = gidx + f.idx_off;
-  for (int e = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x;
-       e < f.p * nrhs; e += SOLVE_SPLIT * blockDim.x) {
-    int t = e % f.p, r = e / f.p;
-    X[g[t] + (int64_t)r * ldx] = (double)y[t + (int64_t)r * f.p];
+  for (int t = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x; t < f.p;
+       t += SOLVE_SPLIT * blockDim.x) {
+    const int64_t gt = g[t];
+    for (int r = 0; r < nrhs; r++)
+      X[gt + (int64_t)r * ldx] = (double)y[t + (int64_t)r * f.p];
   }
 }
 
