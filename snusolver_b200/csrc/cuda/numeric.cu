@@ -904,6 +904,10 @@ class CudaEngine : public Engine {
     sev0_ = sev1_ = nullptr;
     for (cudaEvent_t e : pev_) cudaEventDestroy(e);
     pev_.clear();
+    // autotuner events left by a tuning pass that stopped on an error
+    for (cudaEvent_t e : tune_events_) cudaEventDestroy(e);
+    tune_events_.clear();
+    tune_rec_.clear();
     if (own_stream_) cudaStreamDestroy(own_stream_);
     ev0_ = ev1_ = nullptr;
     stream_ = own_stream_ = nullptr;
