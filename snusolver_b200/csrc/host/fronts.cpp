@@ -3,12 +3,33 @@
 #include "fronts.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <numeric>
+#include <thread>
 
 namespace snu {
 
 namespace {
+
+// fn(i) for i < n on up to 16 host threads (items taken from a counter);
+// fn must only write data owned by item i.
+template <class Fn>
+void parallel_for(int n, Fn fn) {
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nt = std::min({n, hw, 16});
+  if (nt <= 1) {
+    for (int i = 0; i < n; i++) fn(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++)
+    th.emplace_back([&] {
+      for (int i; (i = next.fetch_add(1)) < n;) fn(i);
+    });
+  for (auto& x : th) x.join();
+}
 
 struct Snode {
   std::vector<int> P;  // pivot core indices (ascending)
@@ -139,10 +160,12 @@ int build_front_plan(const Structure& s, const FrontOptions& opt,
   std::vector<std::vector<int>> leaf_roots(np);
   fp.sep_front.assign(2 * np, -1);
 
+  // the leaves' supernodes are independent: built in parallel
+  std::vector<std::vector<Snode>> sns(np);
+  parallel_for(np, [&](int rank) { leaf_supernodes(s.leaves[rank], opt, sns[rank]); });
   for (int rank = 0; rank < np; rank++) {
     const LeafStructure& L = s.leaves[rank];
-    std::vector<Snode> sn;
-    leaf_supernodes(L, opt, sn);
+    std::vector<Snode> sn = std::move(sns[rank]);
     fp.pivot_front[rank].assign(L.leaf_size, -1);
     // core index -> original row index
     auto orig = [&](int j) {
@@ -321,8 +344,7 @@ int build_front_plan(const Structure& s, const FrontOptions& opt,
     int64_t pos;
     int val;
   };
-  std::vector<AE> ae;
-  ae.reserve(s.nnz);
+  std::vector<AE> ae(s.nnz);
   // position lookup inside a separator front: permuted global -> local
   auto sep_local = [&](int i, int g) {
     int off2 = 0;
@@ -333,7 +355,12 @@ int build_front_plan(const Structure& s, const FrontOptions& opt,
     }
     return -1;
   };
-  for (int k = 0; k < s.nnz; k++) {
+  // one lookup per entry, in parallel over chunks of entries
+  constexpr int ACHUNK = 1 << 16;
+  const int nchunk = (s.nnz + ACHUNK - 1) / ACHUNK;
+  std::atomic<int> bad_entry{0};
+  parallel_for(nchunk, [&](int ch) {
+  for (int k = ch * ACHUNK; k < std::min(s.nnz, (ch + 1) * ACHUNK); k++) {
     int p = s.perm_map[k];
     int gi = s.coo_grid_i[p], gj = s.coo_grid_j[p];
     int f, r, c;
@@ -352,15 +379,34 @@ int build_front_plan(const Structure& s, const FrontOptions& opt,
       c = sep_local(i, s.coo_c[p]);
     }
     if (f < 0 || r < 0 || c < 0) {
-      err = "entry outside its front";
-      return HOST_EINVAL;
+      bad_entry = 1;
+      ae[k] = {0, -1, k};
+      continue;
     }
     const FrontInfo& fi = fp.fronts[f];
-    ae.push_back({fi.level, fi.offset + r + (int64_t)c * fi.ld, k});
+    ae[k] = {fi.level, fi.offset + r + (int64_t)c * fi.ld, k};
   }
-  std::sort(ae.begin(), ae.end(), [](const AE& a, const AE& b) {
-    return a.level != b.level ? a.level < b.level : a.pos < b.pos;
   });
+  if (bad_entry) {
+    err = "entry outside its front";
+    return HOST_EINVAL;
+  }
+  // order by (level, position): a stable bucketing by level, then each
+  // level's positions sorted in parallel (the keys are unique, so the order
+  // is the same as one sort by the pair)
+  {
+    std::vector<int64_t> lstart(nlev + 1, 0);
+    for (const AE& a : ae) lstart[a.level + 1]++;
+    for (int l = 0; l < nlev; l++) lstart[l + 1] += lstart[l];
+    std::vector<AE> by(ae.size());
+    std::vector<int64_t> fill(lstart.begin(), lstart.end() - 1);
+    for (const AE& a : ae) by[fill[a.level]++] = a;
+    parallel_for(nlev, [&](int l) {
+      std::sort(by.begin() + lstart[l], by.begin() + lstart[l + 1],
+                [](const AE& a, const AE& b) { return a.pos < b.pos; });
+    });
+    ae.swap(by);
+  }
   for (size_t k = 1; k < ae.size(); k++)
     if (ae[k].pos == ae[k - 1].pos) {
       err = "duplicate (row, column) entries are not supported by the "
