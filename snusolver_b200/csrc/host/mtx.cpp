@@ -5,7 +5,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "structure.h"
 
@@ -15,6 +18,41 @@ namespace {
 std::string lower(std::string s) {
   for (auto& ch : s) ch = (char)std::tolower((unsigned char)ch);
   return s;
+}
+
+// Entries parsed from [b, e) (a whole number of lines): stops at the first
+// entry that does not parse; notes the first entry out of range.
+struct Part {
+  std::vector<int> I, J;
+  std::vector<double> V;
+  bool bad = false;       // an entry did not parse (at index I.size())
+  long long range = -1;   // first entry out of range, -1 if none
+};
+
+void parse_part(const char* b, const char* e, long long M, long long N,
+                Part& out) {
+  const char* p = b;
+  auto skip = [&] {
+    while (p < e && std::isspace((unsigned char)*p)) p++;
+    return p < e;
+  };
+  for (;;) {
+    if (!skip()) return;  // clean end between entries
+    char* q;
+    const long long r = std::strtoll(p, &q, 10);
+    if (q == p || !(p = q, skip())) break;
+    const long long c = std::strtoll(p, &q, 10);
+    if (q == p || !(p = q, skip())) break;
+    const double v = std::strtod(p, &q);
+    if (q == p) break;
+    p = q;
+    if ((r < 1 || r > M || c < 1 || c > N) && out.range < 0)
+      out.range = (long long)out.I.size();
+    out.I.push_back((int)(r - 1));
+    out.J.push_back((int)(c - 1));
+    out.V.push_back(v);
+  }
+  out.bad = true;
 }
 }  // namespace
 
@@ -78,19 +116,85 @@ int read_mtx(const char* path, Csr& A, bool expand_symmetric, std::string& err) 
     err = "MatrixMarket matrix is not square";
     return HOST_EINVAL;
   }
+  // the entry list: the rest of the file read at once and parsed in place
+  // (strtoll / strtod accept what "%lld %lld %lg" accepts, whitespace and
+  // line breaks included)
+  std::string buf;
+  {
+    char chunk[1 << 16];
+    size_t got;
+    while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0) buf.append(chunk, got);
+  }
+  std::fclose(f);
   std::vector<int> I, J;
   std::vector<double> V;
+  // large files: line-aligned chunks parsed on host threads, joined in file
+  // order; the first problem in file order decides, exactly as a
+  // sequential parse would (anything after the nz-th entry is ignored).  A
+  // chunk that fails falls back to the sequential parse below, which also
+  // handles an entry broken over lines at a chunk boundary.
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nt = std::min(hw, 16);
+  if (nt > 1 && buf.size() > ((size_t)16 << 20)) {
+    std::vector<size_t> cut(nt + 1, buf.size());
+    cut[0] = 0;
+    for (int t = 1; t < nt; t++) {
+      size_t x = std::max(cut[t - 1], buf.size() / nt * t);
+      while (x < buf.size() && buf[x] != '\n') x++;
+      cut[t] = std::min(buf.size(), x + 1);
+    }
+    std::vector<Part> parts(nt);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; t++)
+      th.emplace_back([&, t] {
+        parse_part(buf.data() + cut[t], buf.data() + cut[t + 1], M, N, parts[t]);
+      });
+    for (auto& x : th) x.join();
+    long long seen = 0;
+    bool ok = true, range = false;
+    for (const Part& pt : parts) {
+      if (pt.range >= 0 && seen + pt.range < nz) {
+        range = true;
+        break;
+      }
+      seen += (long long)pt.I.size();
+      if (seen >= nz) break;
+      if (pt.bad) {
+        ok = false;
+        break;
+      }
+    }
+    if (range) {
+      err = "MatrixMarket entry out of range";
+      return HOST_EINVAL;
+    }
+    if (ok && seen >= nz) {
+      I.reserve(nz), J.reserve(nz), V.reserve(nz);
+      for (const Part& pt : parts)
+        for (size_t k = 0; k < pt.I.size() && (long long)I.size() < nz; k++) {
+          I.push_back(pt.I[k]);
+          J.push_back(pt.J[k]);
+          V.push_back(pt.V[k]);
+        }
+    }
+  }
+  if ((long long)I.size() < nz) {
+  I.clear(), J.clear(), V.clear();
   I.reserve(nz), J.reserve(nz), V.reserve(nz);
+  const char* p = buf.c_str();
   for (long long k = 0; k < nz; k++) {
-    long long r, c;
-    double v;
-    if (std::fscanf(f, "%lld %lld %lg", &r, &c, &v) != 3) {
-      std::fclose(f);
+    char* e1 = nullptr;
+    char* e2 = nullptr;
+    char* e3 = nullptr;
+    const long long r = std::strtoll(p, &e1, 10);
+    const long long c = e1 != p ? std::strtoll(e1, &e2, 10) : 0;
+    const double v = e1 != p && e2 != e1 ? std::strtod(e2, &e3) : 0.0;
+    if (e1 == p || e2 == e1 || e3 == e2) {
       err = "truncated MatrixMarket entry list";
       return HOST_EINVAL;
     }
+    p = e3;
     if (r < 1 || r > M || c < 1 || c > N) {
-      std::fclose(f);
       err = "MatrixMarket entry out of range";
       return HOST_EINVAL;
     }
@@ -98,7 +202,7 @@ int read_mtx(const char* path, Csr& A, bool expand_symmetric, std::string& err) 
     J.push_back((int)(c - 1));
     V.push_back(v);
   }
-  std::fclose(f);
+  }
   if (symmetric && expand_symmetric) {
     size_t base = I.size();
     for (size_t k = 0; k < base; k++)

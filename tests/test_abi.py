@@ -105,3 +105,56 @@ def test_read_mtx_rejects_corrupt_files(tmp_path, body, why):
     with pytest.raises(snu.SnuError) as e:
         snu.read_matrix(str(p))
     assert e.value.status == 1 and why in str(e.value)
+
+
+def _big_mtx(path, n=200_000, per_row=5, seed=7, broken_every=0, tail="",
+             extra_nz=0, bad_last=False):
+    """A file above the reader's parallel-parse threshold (16 MB); returns the
+    expected CSR (rows keep file order)."""
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(n), per_row)
+    cols = rng.integers(0, n, size=rows.size)
+    vals = rng.standard_normal(rows.size)
+    order = rng.permutation(rows.size)  # entries in random file order
+    rows, cols, vals = rows[order], cols[order], vals[order]
+    lines = []
+    for k, (r, c, v) in enumerate(zip(rows.tolist(), cols.tolist(), vals.tolist())):
+        if bad_last and k == rows.size - 1:
+            r = n  # 0-based n -> 1-based n + 1: out of range
+        sep = "\n" if broken_every and k % broken_every == 0 else " "
+        lines.append(f"{r + 1}{sep}{c + 1}{sep}{v!r}\n")
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n% generated\n")
+        f.write(f"{n} {n} {rows.size + extra_nz}\n")
+        f.write("".join(lines))
+        f.write(tail)
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, rows + 1, 1)
+    rp = np.cumsum(rp)
+    idx = np.argsort(rows, kind="stable")
+    return rp, cols[idx], vals[idx]
+
+
+@pytest.mark.parametrize("broken_every,tail", [(0, ""), (997, ""),
+                                               (0, "1 1 1.0\ngarbage\n")])
+def test_read_mtx_large_files_match_file_order(tmp_path, broken_every, tail):
+    # large files are parsed in line-aligned chunks on host threads; the CSR
+    # must be the sequential parse's (file order kept, entries broken over
+    # lines and text after the last declared entry handled the same way)
+    p = str(tmp_path / "big.mtx")
+    rp, ci, v = _big_mtx(p, broken_every=broken_every, tail=tail)
+    assert os.path.getsize(p) > 16 << 20
+    A = snu.read_matrix(p)
+    assert np.array_equal(np.asarray(A.rowptr), rp)
+    assert np.array_equal(np.asarray(A.colidx), ci)
+    assert np.array_equal(np.asarray(A.data), v)
+
+
+@pytest.mark.parametrize("kw,why", [({"bad_last": True}, "out of range"),
+                                    ({"extra_nz": 3}, "truncated")])
+def test_read_mtx_large_files_rejected(tmp_path, kw, why):
+    p = str(tmp_path / "big_bad.mtx")
+    _big_mtx(p, **kw)
+    with pytest.raises(snu.SnuError) as e:
+        snu.read_matrix(p)
+    assert e.value.status == 1 and why in str(e.value)
