@@ -371,8 +371,30 @@ class Solver:
         return out.reshape((int(bz[i]), int(bz[j])), order="F")
 
 
-def read_matrix(path, expand_symmetric=False) -> CsrMatrix:
-    """MatrixMarket reader with read_matrix.cpp semantics."""
+def read_matrix(path, expand_symmetric=False, cache=None) -> CsrMatrix:
+    """MatrixMarket reader with read_matrix.cpp semantics.
+
+    cache: optional path of a binary CSR copy (numpy .npz).  When it exists,
+    is newer than the .mtx file and was written with the same
+    expand_symmetric, it is loaded instead of parsing; otherwise the file is
+    parsed and the copy (re)written.  Nothing is written without it."""
+    if cache is not None:
+        try:
+            if os.path.getmtime(cache) >= os.path.getmtime(path):
+                with np.load(cache) as z:
+                    if bool(z["expand_symmetric"]) == bool(expand_symmetric):
+                        n = int(z["n"])
+                        return CsrMatrix(n, n, int(z["data"].size),
+                                         z["rowptr"].copy(), z["colidx"].copy(),
+                                         z["data"].copy())
+        except (OSError, KeyError, ValueError):
+            pass  # missing or unreadable copy: parse the file
+        A = read_matrix(path, expand_symmetric)
+        tmp = f"{cache}.tmp.{os.getpid()}.npz"
+        np.savez(tmp, n=np.int64(A.n), rowptr=A.rowptr, colidx=A.colidx,
+                 data=A.data, expand_symmetric=np.bool_(expand_symmetric))
+        os.replace(tmp, cache)  # readers never see a partial copy
+        return A
     lib = load_library()
     n, nnz = C.c_int(), C.c_int()
     rp, ci, v = _I(), _I(), _D()

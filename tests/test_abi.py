@@ -158,3 +158,23 @@ def test_read_mtx_large_files_rejected(tmp_path, kw, why):
     with pytest.raises(snu.SnuError) as e:
         snu.read_matrix(p)
     assert e.value.status == 1 and why in str(e.value)
+
+
+def test_read_mtx_binary_cache(tmp_path):
+    # an opt-in binary CSR copy: reused while newer than the .mtx file and
+    # written with the same expand_symmetric, rebuilt otherwise
+    mtx, cache = tmp_path / "a.mtx", str(tmp_path / "a.csr.npz")
+    hdr = "%%MatrixMarket matrix coordinate real symmetric\n"
+    mtx.write_text(hdr + "3 3 3\n1 1 2.0\n2 1 -1.0\n3 3 4.0\n")
+    A = snu.read_matrix(str(mtx), expand_symmetric=True, cache=cache)
+    assert os.path.exists(cache) and A.nnz == 4
+    # same (older) file name, other contents: the copy is what is read
+    mtx.write_text(hdr + "3 3 1\n1 1 9.0\n")
+    t = os.path.getmtime(cache) - 10
+    os.utime(mtx, (t, t))
+    B = snu.read_matrix(str(mtx), expand_symmetric=True, cache=cache)
+    assert B.nnz == 4 and np.array_equal(B.data, A.data)
+    # another expand_symmetric, or a newer file: parsed again
+    C1 = snu.read_matrix(str(mtx), expand_symmetric=False, cache=cache)
+    assert C1.nnz == 1 and C1.data[0] == 9.0
+    assert snu.read_matrix(str(mtx), cache=cache).nnz == 1
