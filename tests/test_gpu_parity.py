@@ -220,3 +220,37 @@ def test_autotuned_factorization_matches(gpu, tmp_path):
     s2.set_autotune(True, str(cache))
     s2.factorize()
     assert cache.read_text().split() == lines
+
+
+@pytest.mark.parametrize("env", [("SNU_PANEL_BLOCK", "0"), ("SNU_TC_GEMM", "0"),
+                                 ("SNU_TC_PERSIST", "1"), ("SNU_TC_PERSIST", "0"),
+                                 ("SNU_GRAPHS", "0")])
+def test_alternative_paths_match(gpu, monkeypatch, env):
+    # the paths behind the engine switches (read when an engine is made):
+    # per-step panels instead of the fused outer-block kernel, SIMT instead
+    # of tensor-core FP32 GEMMs, the persistent GEMM forced on or off, no
+    # CUDA graph -- each must reproduce the oracle like the default path
+    monkeypatch.setenv(*env)
+    rng = np.random.default_rng(41)
+    rp, ci, v = _random_unsym(rng, 33, 30, 80)
+    b = rng.uniform(-1, 1, len(rp) - 1)
+    s = snu.Solver(nleaves=4).construct(rp, ci, v)
+    x = s.factorize().solve(b)
+    order, sizes = s.ordering()
+    xo, lus, blocks, lib = oracle_solve(rp, ci, v, b, 4, order, sizes)
+    try:
+        _close(x, xo, X_TOL, "x")
+        for r in range(4):
+            _close(s.leaf_factor(r), lus[r], FACTOR_TOL, f"leaf {r}")
+    finally:
+        free_blocks(lib, blocks)
+    # FP32 fronts large enough for the tensor-core GEMMs and several outer
+    # blocks per separator front
+    rp, ci, v = generators.convdiff3d(24)
+    B = generators.rhs(len(rp) - 1, 2, seed=9)
+    s = snu.Solver(nleaves=8, precision=snu.FP32_IR).construct(rp, ci, v)
+    X = s.factorize().solve(B)
+    st = s.stats()
+    assert st["fp64_fallback"] == 0 and st["ir_iters"] <= 3, st
+    for r in range(2):
+        assert rel_resid(rp, ci, v, X[:, r], B[:, r]) <= 1e-10
