@@ -374,7 +374,7 @@ class CudaEngine : public Engine {
         for (int i = row_start[b]; i < row_start[b + 1]; i++) seg[i] = b;
       int rc;
       if ((rc = upload(d_seg_, seg))) return rc;
-      if ((rc = alloc(d_segnorms_, (size_t)ns * 64))) return rc;
+      if ((rc = alloc(d_segnorms_, (size_t)ns * 64 * 2))) return rc;  // two sets
     }
     anorm_seg_.assign(ns, 0.0);
     return ENG_OK;
@@ -1515,24 +1515,35 @@ class CudaEngine : public Engine {
   }
 
   // Max norms of up to 64 columns of M into host out[], per matrix of a
-  // batch (out[b * nc + r]; one matrix: out[r]).
+  // batch (out[b * nc + r]; one matrix: out[r]).  M2 (optional, same
+  // shape): its norms into out2 with the same single read-back.
   int colmax(const double* M, int ld, int nrhs, cudaStream_t st,
-             std::vector<double>& out) {
+             std::vector<double>& out, const double* M2 = nullptr,
+             int ld2 = 0, std::vector<double>* out2 = nullptr) {
     const int nc = std::min(nrhs, 64);
     const size_t cnt = (size_t)nseg_ * nc;
+    const int sets = M2 ? 2 : 1;
     unsigned long long* d = nseg_ > 1 ? d_segnorms_ : d_norms_;
-    CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * cnt, st));
-    if (nseg_ > 1)
-      k_colmax_seg<<<4 * 148, 256, 0, st>>>(n_, nc, M, ld, d_seg_, d);
-    else
-      k_colmax<<<148, 256, 0, st>>>(n_, nc, M, ld, d);
-    CKL();
-    std::vector<unsigned long long> h(cnt);
-    CK(cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long) * cnt,
+    CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * cnt * sets, st));
+    for (int q = 0; q < sets; q++) {
+      const double* A = q ? M2 : M;
+      const int la = q ? ld2 : ld;
+      if (nseg_ > 1)
+        k_colmax_seg<<<4 * 148, 256, 0, st>>>(n_, nc, A, la, d_seg_, d + q * cnt);
+      else
+        k_colmax<<<148, 256, 0, st>>>(n_, nc, A, la, d + q * cnt);
+      CKL();
+    }
+    std::vector<unsigned long long> h(cnt * sets);
+    CK(cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long) * cnt * sets,
                        cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     out.assign(cnt, 0.0);
     for (size_t k = 0; k < cnt; k++) memcpy(&out[k], &h[k], 8);
+    if (M2) {
+      out2->assign(cnt, 0.0);
+      for (size_t k = 0; k < cnt; k++) memcpy(&(*out2)[k], &h[cnt + k], 8);
+    }
     return ENG_OK;
   }
 
@@ -1569,8 +1580,7 @@ class CudaEngine : public Engine {
     prof_end(pi, KF_RESIDUAL, st, 2.0 * nnz_ * nrhs,
              12.0 * nnz_ + 4.0 * (n_ + 1) + 24.0 * n_ * nrhs);
     std::vector<double> rn, xn;
-    if ((rc = colmax(d_R_, n_, nrhs, st, rn))) return rc;
-    if ((rc = colmax(X, ldx, nrhs, st, xn))) return rc;
+    if ((rc = colmax(d_R_, n_, nrhs, st, rn, X, ldx, &xn))) return rc;
     *out = backward_error(rn, xn, bnorm_);
     return ENG_OK;
   }
@@ -1624,8 +1634,7 @@ class CudaEngine : public Engine {
                                                    d_vals_, dB, ldb, X, ldb,
                                                    nrhs, R, n_);
       CKL();
-      if ((q = colmax(R, n_, nrhs, st, rn))) return q;
-      if ((q = colmax(X, ldb, nrhs, st, xn))) return q;
+      if ((q = colmax(R, n_, nrhs, st, rn, X, ldb, &xn))) return q;
       r.backward_error = backward_error(rn, xn, bn);
       return ENG_OK;
     };
