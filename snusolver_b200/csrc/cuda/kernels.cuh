@@ -110,16 +110,40 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
   for (int i = 0; i < TM; i++)
 #pragma unroll
     for (int j = 0; j < TN; j++) acc[i][j] = (T)0;
-  for (int k0 = 0; k0 < P.k; k0 += BK) {
-    for (int e = tid; e < BM * BK; e += NT) {
-      int i = e % BM, l = e / BM, gi = m0 + i, gl = k0 + l;
-      As[l][i] = (gi < P.m && gl < P.k) ? A[gi + (int64_t)gl * P.lda] : (T)0;
+  // register double buffering: the next k-tile's loads are in flight while
+  // the current tile is multiplied
+  constexpr int LA = (BM * BK + NT - 1) / NT, LB = (BK * BN + NT - 1) / NT;
+  T ra[LA], rb[LB];
+  auto gload = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < LA; q++) {
+      const int e = tid + q * NT;
+      const int i = e % BM, l = e / BM, gi = m0 + i, gl = k0 + l;
+      ra[q] = (e < BM * BK && gi < P.m && gl < P.k)
+                  ? A[gi + (int64_t)gl * P.lda] : (T)0;
     }
-    for (int e = tid; e < BK * BN; e += NT) {
-      int l = e % BK, j = e / BK, gl = k0 + l, gj = n0 + j;
-      Bs[l][j] = (gl < P.k && gj < P.n) ? B[gl + (int64_t)gj * P.ldb] : (T)0;
+#pragma unroll
+    for (int q = 0; q < LB; q++) {
+      const int e = tid + q * NT;
+      const int l = e % BK, j = e / BK, gl = k0 + l, gj = n0 + j;
+      rb[q] = (e < BK * BN && gl < P.k && gj < P.n)
+                  ? B[gl + (int64_t)gj * P.ldb] : (T)0;
+    }
+  };
+  if (P.k > 0) gload(0);
+  for (int k0 = 0; k0 < P.k; k0 += BK) {
+#pragma unroll
+    for (int q = 0; q < LA; q++) {
+      const int e = tid + q * NT;
+      if (e < BM * BK) As[e / BM][e % BM] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < LB; q++) {
+      const int e = tid + q * NT;
+      if (e < BK * BN) Bs[e % BK][e / BK] = rb[q];
     }
     __syncthreads();
+    if (k0 + BK < P.k) gload(k0 + BK);
 #pragma unroll
     for (int l = 0; l < BK; l++) {
       T a[TM], b[TN];
