@@ -102,6 +102,14 @@ SNU_API const char* snu_status_string(snu_status s);
 /* Ordering and symbolic structure only (host); no device work. */
 SNU_API snu_status snu_analyze(snu_handle* h, int n, int nnz,
                                const int* rowptr, const int* colidx);
+/* No reference counterpart: the front plan of an analyzed handle (fronts,
+   levels, the extend-add and assembly maps), built on the host with no
+   device work; fills nfronts, nlevels, factor_entries and factor_flops of
+   snu_stats (capacity planning before any device memory is taken).
+   SNU_ESTATE before snu_analyze.  snu_construct on a handle analyzed for
+   the same pattern (n, nnz, rowptr, colidx) keeps the analysis and, after
+   snu_plan, the plan. */
+SNU_API snu_status snu_plan(snu_handle* h);
 /* snu_analyze + device plan + values (host arrays, reference CSR order). */
 SNU_API snu_status snu_construct(snu_handle* h, int n, int nnz,
                                  const int* rowptr, const int* colidx,

@@ -90,6 +90,7 @@ _EXPORTS = {
     "snu_last_error": (C.c_char_p, [C.c_void_p]),
     "snu_status_string": (C.c_char_p, [C.c_int]),
     "snu_analyze": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _I, _I]),
+    "snu_plan": (C.c_int, [C.c_void_p]),
     "snu_construct": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _I, _I, _D]),
     "snu_construct_batch": (C.c_int, [C.c_void_p, C.c_int, _I, C.c_int,
                                       C.c_int, _I, _I, _D]),
@@ -196,6 +197,13 @@ class Solver:
         self._check(self._lib.snu_analyze(self._h, len(rp) - 1, len(ci),
                                           _iptr(rp), _iptr(ci)))
         self.n, self.nnz = len(rp) - 1, len(ci)
+        return self
+
+    def plan(self):
+        """Front plan of the analyzed pattern, on the host: stats() then
+        holds nfronts, nlevels, factor_entries and factor_flops; a construct
+        of the same pattern reuses the analysis and the plan."""
+        self._check(self._lib.snu_plan(self._h))
         return self
 
     def construct(self, rowptr, colidx, vals):

@@ -169,6 +169,7 @@ SNU_API snu_status snu_analyze(snu_handle* h, int n, int nnz,
   h->batch = 0;
   h->batch_rows.clear();
   h->state = 1;
+  h->plan_ready = false;
   h->eng.reset();
   h->stats.n = n;
   h->stats.nnz = nnz;
@@ -182,9 +183,37 @@ SNU_API snu_status snu_construct(snu_handle* h, int n, int nnz,
                                  const double* vals) {
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
   if (nnz > 0 && !vals) return fail(h, SNU_EINVAL, "null values");
-  snu_status s = snu_analyze(h, n, nnz, rowptr, colidx);
-  if (s != SNU_OK) return s;
-  return snu::finish_construct(h, vals, false);
+  // a handle analyzed (and planned) for this very pattern keeps both
+  const bool same = h->state == 1 && !h->batch && rowptr && colidx &&
+                    n == h->S.n && nnz == h->S.nnz &&
+                    (int)h->rowptr.size() == n + 1 &&
+                    std::equal(rowptr, rowptr + n + 1, h->rowptr.begin()) &&
+                    std::equal(colidx, colidx + nnz, h->colidx.begin());
+  if (!same) {
+    snu_status s = snu_analyze(h, n, nnz, rowptr, colidx);
+    if (s != SNU_OK) return s;
+  }
+  return snu::finish_construct(h, vals, h->plan_ready);
+}
+
+SNU_API snu_status snu_plan(snu_handle* h) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 1) return fail(h, SNU_ESTATE, "plan before analyze");
+  if (h->state == 1 && !h->plan_ready) {
+    NvtxRange r("snu_plan");
+    double t0 = now_s();
+    std::string err;
+    snu::FrontOptions fo;
+    if (snu::build_front_plan(h->S, fo, h->FP, err))
+      return fail(h, SNU_EINVAL, err);
+    h->plan_ready = true;
+    h->stats.analyze_s += now_s() - t0;
+  }
+  h->stats.nfronts = h->FP.nfronts;
+  h->stats.nlevels = h->FP.nlevels;
+  h->stats.factor_entries = h->FP.factor_entries;
+  h->stats.factor_flops = h->FP.flops;
+  return SNU_OK;
 }
 
 SNU_API snu_status snu_construct_batch(snu_handle* h, int nmat,

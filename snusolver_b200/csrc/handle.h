@@ -19,6 +19,7 @@ struct snu_handle {
   std::vector<int> rowptr, colidx;
   std::unique_ptr<snu::Engine> eng;
   int state = 0;  // 0 empty, 1 analyzed, 2 constructed, 3 factorized
+  bool plan_ready = false;  // FP built for the current analysis (snu_plan)
   snu_stats stats;
   double* dB = nullptr;  // staging for host solves
   size_t dcap = 0;

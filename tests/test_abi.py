@@ -178,3 +178,18 @@ def test_read_mtx_binary_cache(tmp_path):
     C1 = snu.read_matrix(str(mtx), expand_symmetric=False, cache=cache)
     assert C1.nnz == 1 and C1.data[0] == 9.0
     assert snu.read_matrix(str(mtx), cache=cache).nnz == 1
+
+
+def test_plan_on_the_host():
+    # the front plan needs no device: deterministic, and refused before
+    # analyze
+    from snusolver_b200 import generators
+    rp, ci, _ = generators.convdiff3d(20)
+    keys = ("nfronts", "nlevels", "factor_entries", "factor_flops")
+    a = snu.Solver(nleaves=8).analyze(rp, ci).plan().stats()
+    b = snu.Solver(nleaves=8).analyze(rp, ci).plan().plan().stats()
+    assert all(a[k] == b[k] for k in keys) and a["nfronts"] > 8
+    assert a["factor_entries"] > 0 and a["factor_flops"] > 0
+    with pytest.raises(snu.SnuError) as e:
+        snu.Solver().plan()
+    assert e.value.status == 6  # SNU_ESTATE

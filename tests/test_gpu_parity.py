@@ -254,3 +254,17 @@ def test_alternative_paths_match(gpu, monkeypatch, env):
     assert st["fp64_fallback"] == 0 and st["ir_iters"] <= 3, st
     for r in range(2):
         assert rel_resid(rp, ci, v, X[:, r], B[:, r]) <= 1e-10
+
+
+def test_construct_reuses_analysis_and_plan(gpu):
+    # analyze + plan, then construct of the same pattern: the plan is kept
+    # (same fronts) and the solve matches a fresh handle's
+    rp, ci, v = generators.laplace2d_perturbed(48, 40, seed=3)
+    b = generators.rhs(len(rp) - 1, 1, seed=4)[:, 0]
+    s = snu.Solver(nleaves=4).analyze(rp, ci).plan()
+    planned = s.stats()["nfronts"]
+    x = s.construct(rp, ci, v).factorize().solve(b)
+    assert s.stats()["nfronts"] == planned
+    ref = snu.Solver(nleaves=4).construct(rp, ci, v).factorize().solve(b)
+    _close(x, ref, 1e-11, "reused plan vs fresh")  # atomics: rounding order
+    assert rel_resid(rp, ci, v, x, b) <= 1e-12
