@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -384,21 +386,46 @@ class CudaEngine : public Engine {
     CK(cudaSetDevice(opt_.device));
     CK(cudaMemcpyAsync(d_vals_, vals, sizeof(double) * nnz_,
                        cudaMemcpyHostToDevice, stream_));
-    // ||A||_inf for the backward error (per matrix of a batch)
+    // ||A||_inf for the backward error (per matrix of a batch), on host
+    // threads while the copy runs: row chunks of one matrix, or whole
+    // matrices of a batch (each row summed in order: the same norm as a
+    // serial loop)
     anorm_ = 0;
     if ((int)anorm_seg_.size() != nseg_) anorm_seg_.assign(nseg_, 0.0);
-    for (int b = 0; b < nseg_; b++) {
-      const int i0 = nseg_ > 1 ? seg_start_[b] : 0;
-      const int i1 = nseg_ > 1 ? seg_start_[b + 1] : n_;
+    auto rows_max = [&](int i0, int i1) {
       double a = 0;
       for (int i = i0; i < i1; i++) {
         double s = 0;
         for (int k = rowptr_h_[i]; k < rowptr_h_[i + 1]; k++) s += std::fabs(vals[k]);
         a = std::max(a, s);
       }
-      anorm_seg_[b] = a;
-      anorm_ = std::max(anorm_, a);
+      return a;
+    };
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = nnz_ > (1 << 17) ? std::min(hw, 16) : 1;
+    if (nseg_ > 1) {
+      std::atomic<int> next{0};
+      auto work = [&] {
+        for (int b; (b = next.fetch_add(1)) < nseg_;)
+          anorm_seg_[b] = rows_max(seg_start_[b], seg_start_[b + 1]);
+      };
+      std::vector<std::thread> th;
+      for (int t = 1; t < nt; t++) th.emplace_back(work);
+      work();
+      for (auto& x : th) x.join();
+    } else {
+      std::vector<double> part(nt, 0.0);
+      std::vector<std::thread> th;
+      for (int t = 1; t < nt; t++)
+        th.emplace_back([&, t] {
+          part[t] = rows_max((int)((int64_t)n_ * t / nt),
+                             (int)((int64_t)n_ * (t + 1) / nt));
+        });
+      part[0] = rows_max(0, (int)((int64_t)n_ / nt));
+      for (auto& x : th) x.join();
+      anorm_seg_[0] = *std::max_element(part.begin(), part.end());
     }
+    for (int b = 0; b < nseg_; b++) anorm_ = std::max(anorm_, anorm_seg_[b]);
     have64_ = have32_ = false;
     CK(cudaStreamSynchronize(stream_));
     return ENG_OK;
