@@ -142,21 +142,29 @@ SNU_API snu_status snu_solve_device(snu_handle* h, const double* dB,
                                     void* stream);
 SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st);
 
-/* No counterpart in the reference.  snu_solve_device for callers that must
-   not allocate device memory: code running while a stream is being captured
-   into a CUDA graph, or a process whose memory manager owns the whole device
-   and forbids cudaMalloc (cudaMalloc may also synchronize the device, which
-   a latency-bound caller cannot accept).  Same arguments and results as
+/* No counterpart in the reference.  snu_solve_device for callers that may
+   not allocate device memory themselves or through a library: a process
+   whose memory manager (a framework's caching allocator, a fixed pool set
+   up at start) owns the device memory and forbids cudaMalloc, or a
+   latency-bound caller that cannot accept cudaMalloc / cudaFree, which may
+   synchronize the whole device.  Same arguments and results as
    snu_solve_device, on a handle that has already been factorized; dX must
-   not alias dB.  The work vectors live in one static device array of 32 MiB
-   that every GPU loading this library holds until exit; a matrix / nrhs whose
-   work vectors do not fit is refused with SNU_EINVAL (snu_last_error gives
-   the size needed).  All calls share that array, so calls whose GPU work
-   overlaps (other streams, other threads, other handles) race.  The first
-   call on a device looks up the array's device address; make that first
-   call before capturing a stream.  The call returns after the solve has
-   finished on the stream.  With SNU_FP32_IR, refinement that would need the
-   FP64 fallback (which allocates) returns SNU_ENOTCONV instead. */
+   not alias dB.  Nothing is allocated: the work vectors live in one static
+   device array of 32 MiB that every GPU loading this library holds until
+   the process exits.  The call needs (wsum*g + psum*g)*es + 8*n*nrhs
+   (FP64) or + 16*n*nrhs (FP32 + refinement) bytes of it, g = min(nrhs, 16),
+   es = 8 (FP64) or 4 (FP32), wsum / psum = the sums of front sizes / pivots
+   (each piece rounded up to 256 bytes); a matrix / nrhs that does not fit
+   is refused with SNU_EINVAL and snu_last_error gives the size needed.
+   All calls share the array and it keeps whatever the last call left
+   (every call rewrites what it reads), so calls whose GPU work overlaps
+   (other streams, threads or handles on the same device) race.  The first
+   call on a device looks up the array's device address
+   (cudaGetSymbolAddress); make that first call before any stream capture.
+   The call returns after the solve has finished on the stream.  With
+   SNU_FP32_IR, refinement that would need the FP64 fallback (which
+   allocates) stops with SNU_ENOTCONV instead; X then holds the refined
+   FP32 solution and snu_get_stats its backward error. */
 SNU_API snu_status snu_solve_device_noalloc(snu_handle* h, const double* dB,
                                             double* dX, int nrhs, int ldb,
                                             void* stream);
@@ -219,7 +227,9 @@ SNU_API snu_status snu_get_coo(const snu_handle* h, int* perm_map, int* coo_r,
 SNU_API snu_status snu_get_leaf_info(snu_handle* h, int rank, int* info);
 /* LU_rowptr[core_n+1], LU_colidx[LU_nnz], LU_diag[core_n],
    LU_bias[leaf_size], core_map[core_nnz] (kernel_sparse.cu:368-596).
-   Any pointer may be NULL. */
+   Any pointer may be NULL.  The first request (here or in
+   snu_get_leaf_factor) computes the patterns of every leaf, one leaf per
+   host thread. */
 SNU_API snu_status snu_get_leaf_pattern(snu_handle* h, int rank,
                                         int* LU_rowptr, int* LU_colidx,
                                         int* LU_diag, int* LU_bias,

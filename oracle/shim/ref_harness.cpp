@@ -7,7 +7,13 @@
 // every rank writes its structure and numeric arrays as raw binary files so
 // the new implementation can be checked against them.
 //
+// With --summary DIR only small files are written: rank 0 its ordering,
+// block layout and (after a solve) x and b, every rank its meta.  --no-solve stops after SnuMat's constructor (ordering,
+// structure, leaf symbolic LU); --order-only runs only the reference's
+// ordering call (call_parmetis, parmetis_driver.cpp:74).
+//
 // usage: snu_ref MATRIX.mtx [--rhs FILE] [--seed S] [--dump DIR]
+//                [--summary DIR] [--no-solve] [--order-only]
 //   ranks: environment SNU_MPI_NP (forked by the mini MPI)
 #include <stdio.h>
 #include <stdlib.h>
@@ -15,6 +21,7 @@
 
 #include <random>
 #include <string>
+#include <vector>
 
 #include "mpi.h"
 #include "read_matrix.h"
@@ -35,6 +42,10 @@ static void dump(const std::string& dir, int rank, const char* name,
 }
 #define DUMPI(name, p, n) dump(dir, iam, name, p, (size_t)(n), 4, "i32")
 #define DUMPD(name, p, n) dump(dir, iam, name, p, (size_t)(n), 8, "f64")
+#define SUMI(name, p, n) dump(sdir, iam, name, p, (size_t)(n), 4, "i32")
+#define SUMD(name, p, n) dump(sdir, iam, name, p, (size_t)(n), 8, "f64")
+
+void call_parmetis(csr_matrix A, int* sizes, int* order);
 
 int main(int argc, char** argv) {
   MPI_Init(&argc, &argv);
@@ -46,12 +57,17 @@ int main(int argc, char** argv) {
     MPI_Finalize();
     return 2;
   }
-  std::string dir, rhs;
+  std::string dir, sdir, rhs;
   unsigned seed = 1;
-  for (int i = 2; i + 1 < argc; i += 2) {
-    if (!strcmp(argv[i], "--dump")) dir = argv[i + 1];
-    else if (!strcmp(argv[i], "--rhs")) rhs = argv[i + 1];
-    else if (!strcmp(argv[i], "--seed")) seed = (unsigned)atoi(argv[i + 1]);
+  bool no_solve = false, order_only = false;
+  for (int i = 2; i < argc; i++) {
+    if (!strcmp(argv[i], "--no-solve")) no_solve = true;
+    else if (!strcmp(argv[i], "--order-only")) order_only = true;
+    else if (i + 1 >= argc) break;
+    else if (!strcmp(argv[i], "--dump")) dir = argv[++i];
+    else if (!strcmp(argv[i], "--summary")) sdir = argv[++i];
+    else if (!strcmp(argv[i], "--rhs")) rhs = argv[++i];
+    else if (!strcmp(argv[i], "--seed")) seed = (unsigned)atoi(argv[++i]);
   }
 
   initialize();
@@ -78,12 +94,33 @@ int main(int argc, char** argv) {
     }
   }
 
+  if (order_only) {
+    // the reference's ordering step alone, as SnuMat.cu:74-96 calls it
+    int n = A.n, nnz = A.nnz;
+    MPI_Bcast(&n, sizeof(int), MPI_BYTE, 0, MPI_COMM_WORLD);
+    MPI_Bcast(&nnz, sizeof(int), MPI_BYTE, 0, MPI_COMM_WORLD);
+    A.n = n, A.nnz = nnz;
+    std::vector<int> sizes(2 * np - 1), order(n);
+    double t0 = MPI_Wtime();
+    call_parmetis(A, sizes.data(), order.data());
+    double t1 = MPI_Wtime();
+    if (!iam) {
+      SUMI("order", order.data(), n);
+      SUMI("sizes", sizes.data(), 2 * np - 1);
+      printf("SNU_REF_RESULT {\"n\": %d, \"nnz\": %d, \"np\": %d, "
+             "\"order_s\": %.6f}\n", n, nnz, np, t1 - t0);
+      fflush(stdout);
+    }
+    MPI_Finalize();
+    return 0;
+  }
+
   MPI_Barrier(MPI_COMM_WORLD);
   double t0 = MPI_Wtime();
   SnuMat* Ab = new SnuMat(A, b, nullptr, nullptr);
   MPI_Barrier(MPI_COMM_WORLD);
   double t1 = MPI_Wtime();
-  Ab->solve(x);
+  if (!no_solve) Ab->solve(x);
   MPI_Barrier(MPI_COMM_WORLD);
   double t2 = MPI_Wtime();
 
@@ -131,7 +168,27 @@ int main(int argc, char** argv) {
     }
   }
 
-  if (!iam) {
+  if (!sdir.empty()) {
+    if (!iam) {
+      SUMI("order", S.order, S.n);
+      SUMI("sizes", S.sizes, 2 * np - 1);
+      SUMI("block_start", S.old_block_start, 2 * np);
+      SUMI("block_size", S.block_size, 2 * np);
+      if (!no_solve) {
+        SUMD("x", x, S.n);
+        SUMD("b", b, S.n);
+      }
+    }
+    int meta[8] = {S.leaf, S.leaf_size, S.dense_row, S.core_n,
+                   S.core_nnz, S.LU_nnz, S.local_b_rows, S.max_level};
+    SUMI("meta", meta, 8);
+  }
+
+  if (!iam && no_solve) {
+    printf("SNU_REF_RESULT {\"n\": %d, \"nnz\": %d, \"np\": %d, "
+           "\"construct_s\": %.6f}\n", A.n, A.nnz, np, t1 - t0);
+    fflush(stdout);
+  } else if (!iam) {
     // driver.cpp:12-28 check: max |Ax - b|
     double M = 0;
     for (int i = 0; i < A.n; i++) {

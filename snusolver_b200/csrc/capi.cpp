@@ -368,7 +368,13 @@ SNU_API snu_status snu_solve_device_noalloc(snu_handle* h, const double* dB,
   if (rc && rc != snu::ENG_ENOTCONV) return from_engine(h, rc);
   h->stats.solve_s = rep.seconds;
   h->stats.ir_iters = rep.ir_iters;
+  h->stats.fp64_fallback = 0;  // this path has no FP64 fallback
   h->stats.backward_error = rep.backward_error;
+  {
+    int64_t fl = 0, sl = 0;
+    h->eng->launch_counts(&fl, &sl);
+    h->stats.solve_launches = (int)sl;
+  }
   if (rc == snu::ENG_ENOTCONV) return from_engine(h, rc);
   return SNU_OK;
 }
@@ -547,6 +553,37 @@ SNU_API snu_status snu_get_leaf_info(snu_handle* h, int rank, int* info) {
   return SNU_OK;
 }
 
+// The leaf LU patterns (the reference's core_symbfact, one per rank) are
+// only needed by the parity read-backs.  The first request computes every
+// missing leaf at once, the leaves on host threads (they are independent:
+// the reference computes them on separate ranks).
+static int leaf_patterns(snu::Structure& S, std::string& err) {
+  std::vector<int> todo;
+  for (int r = 0; r < S.np; r++)
+    if (S.leaves[r].LU_rowptr.empty()) todo.push_back(r);
+  if (todo.empty()) return 0;
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nt = std::min<int>((int)todo.size(), hw);
+  std::vector<std::string> errs(todo.size());
+  std::vector<int> rcs(todo.size(), 0);
+  std::atomic<int> next{0};
+  auto work = [&] {
+    for (int k; (k = next.fetch_add(1)) < (int)todo.size();)
+      rcs[k] = snu::leaf_symbfact(S.leaves[todo[k]], errs[k]);
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; t++) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
+  for (size_t k = 0; k < todo.size(); k++)
+    if (rcs[k]) {
+      err = "leaf " + std::to_string(todo[k]) + ": " + errs[k];
+      for (int r : todo) S.leaves[r].LU_rowptr.clear();
+      return rcs[k];
+    }
+  return 0;
+}
+
 SNU_API snu_status snu_get_leaf_pattern(snu_handle* h, int rank,
                                         int* LU_rowptr, int* LU_colidx,
                                         int* LU_diag, int* LU_bias,
@@ -557,7 +594,7 @@ SNU_API snu_status snu_get_leaf_pattern(snu_handle* h, int rank,
   snu::LeafStructure& L = h->S.leaves[rank];
   if (L.LU_rowptr.empty()) {
     std::string err;
-    if (snu::leaf_symbfact(L, err)) return fail(h, SNU_EINVAL, err);
+    if (leaf_patterns(h->S, err)) return fail(h, SNU_EINVAL, err);
   }
   if (LU_rowptr) std::memcpy(LU_rowptr, L.LU_rowptr.data(), sizeof(int) * (L.core_n + 1));
   if (LU_colidx) std::memcpy(LU_colidx, L.LU_colidx.data(), sizeof(int) * L.LU_nnz);
@@ -575,7 +612,7 @@ SNU_API snu_status snu_get_leaf_factor(snu_handle* h, int rank,
   snu::LeafStructure& L = h->S.leaves[rank];
   if (L.LU_rowptr.empty()) {
     std::string err;
-    if (snu::leaf_symbfact(L, err)) return fail(h, SNU_EINVAL, err);
+    if (leaf_patterns(h->S, err)) return fail(h, SNU_EINVAL, err);
   }
   return from_engine(h, h->eng->leaf_factor(h->S, rank, LU_data));
 }

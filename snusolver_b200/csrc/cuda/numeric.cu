@@ -587,10 +587,15 @@ class CudaEngine : public Engine {
       err_ = "leaf pattern not computed";
       return ENG_ESTATE;
     }
-    std::vector<double> F;
-    int rc;
-    if ((rc = arena_to_host(F))) return rc;
     const FrontPlan& fp = *fp_;
+    // only the fronts of this leaf come back (the arena can be many GB)
+    std::map<int, std::vector<double>> Fh;
+    int rc;
+    for (int j = 0; j < L.leaf_size; j++) {
+      const int f = fp.pivot_front[rank][j];
+      if (Fh.count(f)) continue;
+      if ((rc = front_to_host(f, Fh[f]))) return rc;
+    }
     for (int r = 0; r < L.core_n; r++) {
       for (int k = L.LU_rowptr[r]; k < L.LU_rowptr[r + 1]; k++) {
         int c = L.LU_colidx[k];
@@ -605,8 +610,7 @@ class CudaEngine : public Engine {
           out[k] = 0;  // structurally zero in the symmetric front pattern
           continue;
         }
-        const FrontInfo& fi = fp.fronts[f];
-        out[k] = F[fi.offset + pr + (int64_t)pc * fi.ld];
+        out[k] = Fh[f][pr + (int64_t)pc * fp.fronts[f].ld];
       }
     }
     return ENG_OK;
@@ -643,12 +647,10 @@ class CudaEngine : public Engine {
     int m = s.block_size[i], nn = s.block_size[j];
     std::vector<double> F;
     int rc;
-    if ((rc = arena_to_host(F, fi.offset, (int64_t)fi.ld * (fi.p + fi.q))))
-      return rc;
+    if ((rc = front_to_host(f, F))) return rc;
     for (int c = 0; c < nn; c++)
       for (int r = 0; r < m; r++)
-        out[r + (int64_t)c * m] =
-            F[fi.offset + (ro + r) + (int64_t)(co + c) * fi.ld];
+        out[r + (int64_t)c * m] = F[(ro + r) + (int64_t)(co + c) * fi.ld];
     return ENG_OK;
   }
 
@@ -940,11 +942,14 @@ class CudaEngine : public Engine {
     stream_ = own_stream_ = nullptr;
   }
 
-  int arena_to_host(std::vector<double>& F, int64_t off = 0, int64_t cnt = -1) {
-    if (cnt < 0) cnt = arena_;
-    F.assign((size_t)cnt + (size_t)off, 0.0);
-    CK(cudaMemcpy(F.data() + off, d_F64_ + off, sizeof(double) * cnt,
-                  cudaMemcpyDeviceToHost));
+  // FP64 front f (ld x (p + q), column-major) to the host.
+  int front_to_host(int f, std::vector<double>& F) {
+    const FrontInfo& fi = fp_->fronts[f];
+    const int64_t cnt = (int64_t)fi.ld * (fi.p + fi.q);
+    F.assign((size_t)std::max<int64_t>(cnt, 1), 0.0);
+    if (cnt > 0)
+      CK(cudaMemcpy(F.data(), d_F64_ + fi.offset, sizeof(double) * cnt,
+                    cudaMemcpyDeviceToHost));
     return ENG_OK;
   }
 
@@ -1541,35 +1546,40 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
-  // Max norms of up to 64 columns of M into host out[], per matrix of a
-  // batch (out[b * nc + r]; one matrix: out[r]).  M2 (optional, same
-  // shape): its norms into out2 with the same single read-back.
+  // Max norms of the nrhs columns of M into host out[], per matrix of a
+  // batch (out[b * nrhs + r]; one matrix: out[r]), in groups of up to 64
+  // columns (the device norm buffers hold 64 per matrix and set).  M2
+  // (optional, same shape): its norms into out2 with the same read-backs.
   int colmax(const double* M, int ld, int nrhs, cudaStream_t st,
              std::vector<double>& out, const double* M2 = nullptr,
              int ld2 = 0, std::vector<double>* out2 = nullptr) {
-    const int nc = std::min(nrhs, 64);
-    const size_t cnt = (size_t)nseg_ * nc;
     const int sets = M2 ? 2 : 1;
     unsigned long long* d = nseg_ > 1 ? d_segnorms_ : d_norms_;
-    CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * cnt * sets, st));
-    for (int q = 0; q < sets; q++) {
-      const double* A = q ? M2 : M;
-      const int la = q ? ld2 : ld;
-      if (nseg_ > 1)
-        k_colmax_seg<<<4 * 148, 256, 0, st>>>(n_, nc, A, la, d_seg_, d + q * cnt);
-      else
-        k_colmax<<<148, 256, 0, st>>>(n_, nc, A, la, d + q * cnt);
-      CKL();
-    }
-    std::vector<unsigned long long> h(cnt * sets);
-    CK(cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long) * cnt * sets,
-                       cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    out.assign(cnt, 0.0);
-    for (size_t k = 0; k < cnt; k++) memcpy(&out[k], &h[k], 8);
-    if (M2) {
-      out2->assign(cnt, 0.0);
-      for (size_t k = 0; k < cnt; k++) memcpy(&(*out2)[k], &h[cnt + k], 8);
+    out.assign((size_t)nseg_ * nrhs, 0.0);
+    if (M2) out2->assign((size_t)nseg_ * nrhs, 0.0);
+    for (int c0 = 0; c0 < nrhs; c0 += 64) {
+      const int nc = std::min(nrhs - c0, 64);
+      const size_t cnt = (size_t)nseg_ * nc;
+      CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * cnt * sets, st));
+      for (int q = 0; q < sets; q++) {
+        const int la = q ? ld2 : ld;
+        const double* A = (q ? M2 : M) + (size_t)c0 * la;
+        if (nseg_ > 1)
+          k_colmax_seg<<<4 * 148, 256, 0, st>>>(n_, nc, A, la, d_seg_, d + q * cnt);
+        else
+          k_colmax<<<148, 256, 0, st>>>(n_, nc, A, la, d + q * cnt);
+        CKL();
+      }
+      std::vector<unsigned long long> h(cnt * sets);
+      CK(cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long) * cnt * sets,
+                         cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      for (int b = 0; b < nseg_; b++)
+        for (int r = 0; r < nc; r++) {
+          memcpy(&out[(size_t)b * nrhs + c0 + r], &h[(size_t)b * nc + r], 8);
+          if (M2)
+            memcpy(&(*out2)[(size_t)b * nrhs + c0 + r], &h[cnt + (size_t)b * nc + r], 8);
+        }
     }
     return ENG_OK;
   }
@@ -1592,7 +1602,7 @@ class CudaEngine : public Engine {
   }
 
   // Backward error max_r ||B - A X||inf / (||A||inf ||X||inf + ||B||inf)
-  // (the first 64 columns); leaves R = B - A X in d_R_.
+  // over every column; leaves R = B - A X in d_R_.
   int residual_norms(const double* B, int ldb, const double* X, int ldx,
                      int nrhs, cudaStream_t st, double* out) {
     int rc;
@@ -1630,7 +1640,10 @@ class CudaEngine : public Engine {
     }
     const size_t es = precision == 0 ? sizeof(double) : sizeof(float);
     auto up = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t bw = up((size_t)wtot_ * nrhs * es), by = up((size_t)ytot_ * nrhs * es);
+    // W and Y serve one column group (at most RG columns) at a time; the
+    // residual R and correction D hold every column
+    const size_t gc = (size_t)std::min(nrhs, RG);
+    const size_t bw = up((size_t)wtot_ * gc * es), by = up((size_t)ytot_ * gc * es);
     const size_t br = up((size_t)n_ * nrhs * sizeof(double));
     const size_t need = bw + by + (precision == 0 ? br : 2 * br);
     if (need > NOALLOC_SCRATCH_BYTES) {
@@ -1665,7 +1678,9 @@ class CudaEngine : public Engine {
       r.backward_error = backward_error(rn, xn, bn);
       return ENG_OK;
     };
+    const int64_t l0 = launches_;
     CK(cudaMemsetAsync(d_flags_ + 4, 0, sizeof(int), st));
+    CK(cudaEventRecord(sev0_, st));  // events made at init: no allocation
     do {
       if ((rc = colmax(dB, ldb, nrhs, st, bn))) break;
       if (precision == 0) {
@@ -1706,8 +1721,13 @@ class CudaEngine : public Engine {
     } while (0);
     prof_mask_ = saved_mask;
     if (rc && rc != ENG_ENOTCONV) return rc;
+    CK(cudaEventRecord(sev1_, st));
+    last_solve_launches_ = launches_ - l0;
     int wrc = sweep_status(st);
     if (wrc) return wrc;
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, sev0_, sev1_));
+    r.seconds = ms * 1e-3;
     if (rep) *rep = r;
     return rc;
   }

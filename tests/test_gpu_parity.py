@@ -268,3 +268,59 @@ def test_construct_reuses_analysis_and_plan(gpu):
     ref = snu.Solver(nleaves=4).construct(rp, ci, v).factorize().solve(b)
     _close(x, ref, 1e-11, "reused plan vs fresh")  # atomics: rounding order
     assert rel_resid(rp, ci, v, x, b) <= 1e-12
+
+
+def _sampled(got, g, key, tol, what):
+    """got (flat, the reference's layout) against a golden sample of the
+    reference's array: max |got[k] - ref[k]| <= tol * max |ref|."""
+    idx, val = g[key + "_idx"], g[key + "_val"]
+    scale = max(float(g[key + "_absmax"][0]), 1e-300)
+    err = np.abs(got[idx] - val).max() / scale if len(idx) else 0.0
+    assert err <= tol, f"{what}: relative error {err:.3e} > {tol}"
+    return err
+
+
+def test_c2_against_reference(gpu):
+    # the 64^3 convection-diffusion workload against the reference's own
+    # FP64 run (built from its sources, 8 ranks, the first right-hand side):
+    # sampled leaf and separator factors and the solution within 1e-10, and
+    # the FP32+IR solution's forward error against that same reference x
+    g = golden("c2_convdiff64_np8.npz")
+    rp, ci, v, B = generators.config("c2_convdiff64")
+    s = snu.Solver(nleaves=8).construct(rp, ci, v).factorize()
+    x = s.solve(B[:, 0])
+    _sampled(x, g, "x", X_TOL, "x vs reference")
+    assert rel_resid(rp, ci, v, x, B[:, 0]) <= 1e-12
+    for r in range(8):
+        _sampled(s.leaf_factor(r), g, f"r{r}_LU_data", FACTOR_TOL, f"leaf {r}")
+    for key in g:
+        if key.startswith("dense_") and key.endswith("_idx"):
+            i, j = map(int, key.split("_")[1:3])
+            _sampled(s.dense_block(i, j).ravel(order="F"), g, f"dense_{i}_{j}",
+                     FACTOR_TOL, f"LU[{i},{j}]")
+    s.close()
+    s32 = snu.Solver(nleaves=8, precision=snu.FP32_IR).construct(rp, ci, v)
+    x32 = s32.factorize().solve(B[:, 0])
+    st = s32.stats()
+    assert st["backward_error"] <= 1e-10 and st["fp64_fallback"] == 0, st
+    fwd = _sampled(x32, g, "x", 1e-8, "FP32+IR x vs reference")
+    assert fwd <= 1e-8
+
+
+def test_fp64_fallback_when_refinement_stops(gpu):
+    # no refinement step allowed: the FP32+IR solve must factor in FP64 on
+    # demand, solve the correction with it and reach FP64 accuracy
+    g = golden("c1_2d128_np8.npz")
+    rp, ci, v, B = generators.config("c1_2d128")
+    s = snu.Solver(nleaves=8, precision=snu.FP32_IR,
+                   ir_max_iter=0).construct(rp, ci, v)
+    x = s.factorize().solve(B[:, 0])
+    st = s.stats()
+    assert st["fp64_fallback"] == 1 and st["ir_iters"] == 0, st
+    assert st["backward_error"] <= 1e-12, st
+    _close(x, g["x"], X_TOL, "x vs reference")
+    assert rel_resid(rp, ci, v, x, B[:, 0]) <= 1e-12
+    # a second solve reuses the FP64 factors
+    x2 = s.solve(B[:, 0])
+    assert s.stats()["fp64_fallback"] == 1
+    _close(x2, x, 1e-13, "second solve")

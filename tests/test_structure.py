@@ -76,6 +76,27 @@ def test_c1_structure_bitexact():
     _compare(g, _structure(h, 8), 8, hashed=True)
 
 
+def test_c2_structure_bitexact():
+    # the 64^3 convection-diffusion workload: ordering, block layout, COO
+    # split and every leaf's LU pattern against the reference's own run
+    g = golden("c2_convdiff64_np8.npz")
+    rp, ci, v, _ = generators.config("c2_convdiff64")
+    h = snu.Solver(nleaves=8).analyze(rp, ci)
+    _compare(g, _structure(h, 8), 8, hashed=True)
+
+
+def test_c4_ordering_bitexact():
+    # the 96^3 27-point workload: the reference's ordering call (METIS
+    # nested dissection through its ParMETIS driver) gives the same order and
+    # separator sizes as this library's analysis
+    g = golden("c4_27pt96_np8_order.npz")
+    rp, ci, v, _ = generators.config("c4_27pt96")
+    h = snu.Solver(nleaves=8).analyze(rp, ci)
+    order, sizes = h.ordering()
+    np.testing.assert_array_equal(sizes, g["sizes"])
+    np.testing.assert_array_equal(_digest(order), g["order"])
+
+
 def test_read_mtx_matches_reference_csr(tmp_path):
     g = golden("matrix20_np4.npz")
     p = tmp_path / "m.mtx"
