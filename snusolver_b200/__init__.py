@@ -78,7 +78,8 @@ class _LaunchRec(C.Structure):
 
 KERNEL_FAMILIES = ("assemble", "extend_add", "diag_lu", "panel_trsm",
                    "gemm_trail", "gemm_schur", "solve_diag", "solve_gemm",
-                   "solve_misc", "residual", "panel_block")
+                   "solve_misc", "residual", "panel_block", "block_inv",
+                   "gemm_panel")
 
 _lib = None
 _I = C.POINTER(C.c_int)

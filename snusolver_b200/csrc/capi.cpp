@@ -386,8 +386,9 @@ SNU_API snu_status snu_solve(snu_handle* h, const double* B, double* X,
   if (!B || !X || nrhs <= 0 || ldb < h->S.n)
     return fail(h, SNU_EINVAL, "bad right-hand side arguments");
   const int n = h->S.n;
-  // staged in chunks of up to 16 columns, so device staging stays bounded
-  const int chunk = std::min(nrhs, 16);
+  // staged in chunks of up to 64 columns (one refinement loop per chunk),
+  // so device staging stays bounded
+  const int chunk = std::min(nrhs, 64);
   size_t need = (size_t)n * chunk * 2;
   if (need > h->dcap) {
     if (h->dB) cudaFree(h->dB);

@@ -10,7 +10,8 @@
 // plain TF32 GEMM: TMA loads 128 x 32 (A') and BN x 32 (B') fp32 tiles with
 // 128-byte swizzle into a STAGES-deep shared-memory ring, one thread issues
 // tcgen05.mma (M=128, N=BN, K=8) into a TMEM accumulator, and the four warps
-// read the accumulator back with tcgen05.ld and subtract it from C.
+// read the accumulator back with tcgen05.ld and subtract it from C (or,
+// for the panel products, store it: C = A B).
 //
 // Every wait on an mbarrier is bounded; on timeout the kernel records the
 // failure in err[0], lets its in-flight work drain (bounded), frees its TMEM
@@ -30,7 +31,8 @@ struct TcProb {
   int lda, ldb, ldc;
   int64_t apack, bpack;  // element offsets of A', B' in the pack workspace
   int64_t pc, rel;       // Schur scatter into the parent (see GemmProb)
-  int pld, pad;
+  int pld;
+  int mode;              // 0: C -= A B, 1: C = A B (pc < 0 only)
 };
 
 struct TcTile {
@@ -278,8 +280,9 @@ __global__ void __launch_bounds__(128, 1)
     const int t = threadIdx.x - 64;
     const int r0 = tl.tm * TC_BM, c0 = tl.tn * TC_BN;
     const int nr = min(TC_BM, pr.m - r0), ncl = min(TC_BN, pr.n - c0);
-    for (int c = t; c < ncl; c += 64)
-      prefetch_l2_span(F + pr.c + r0 + (int64_t)(c0 + c) * pr.ldc, nr);
+    if (!pr.mode)  // (an overwritten C is not read)
+      for (int c = t; c < ncl; c += 64)
+        prefetch_l2_span(F + pr.c + r0 + (int64_t)(c0 + c) * pr.ldc, nr);
     if (pr.pc >= 0) {
       const int* rel = rel_base + pr.rel;
       for (int i = t; i < TC_BM; i += 64) rel_r[i] = i < nr ? rel[r0 + i] : 0;
@@ -321,8 +324,12 @@ __global__ void __launch_bounds__(128, 1)
         float cv[32];
 #pragma unroll
         for (int j = 0; j < 32; j++)
-          cv[j] = j < ncol ? cp[(int64_t)j * pr.ldc] : 0.f;
-        if (pr.pc >= 0) {
+          cv[j] = (j < ncol && !pr.mode) ? cp[(int64_t)j * pr.ldc] : 0.f;
+        if (pr.mode) {
+#pragma unroll
+          for (int j = 0; j < 32; j++)
+            if (j < ncol) cp[(int64_t)j * pr.ldc] = __uint_as_float(v[j]);
+        } else if (pr.pc >= 0) {
           // extend-add fused: the child's update goes straight to the parent
           float* prow = F + pr.pc + rel_r[warp * 32 + lane];
 #pragma unroll
@@ -485,7 +492,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
         // this warp's rows of C into L2 while the tile's MMAs run
         const int r0 = tl.tm * TC_BM + qtr * 32, ct = tl.tn * TC_BN;
         const int nr = min(32, pr.m - r0), ncl = min(TC_BN, pr.n - ct);
-        if (nr > 0)
+        if (nr > 0 && !pr.mode)
           for (int c = lane; c < ncl; c += 32)
             prefetch_l2_span(F + pr.c + r0 + (int64_t)(ct + c) * pr.ldc, nr);
       }
@@ -521,8 +528,12 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
           float cv[32];
 #pragma unroll
           for (int j = 0; j < 32; j++)
-            cv[j] = j < ncol ? cp[(int64_t)j * pr.ldc] : 0.f;
-          if (pr.pc >= 0) {
+            cv[j] = (j < ncol && !pr.mode) ? cp[(int64_t)j * pr.ldc] : 0.f;
+          if (pr.mode) {
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+              if (j < ncol) cp[(int64_t)j * pr.ldc] = __uint_as_float(v[j]);
+          } else if (pr.pc >= 0) {
             const int* rel = rel_base + pr.rel;
             float* prow = F + pr.pc + rel[row];
 #pragma unroll

@@ -21,6 +21,7 @@
 #include "panel.cuh"
 #include "sweep.cuh"
 #include "gemm_tc.cuh"
+#include "block_inv.cuh"
 
 namespace snu {
 
@@ -132,6 +133,17 @@ struct OuterBlock {
   int ntasks = 0;
   GemmBatch outer;
   double flops = 0, elems = 0;
+  // FP32 tensor-core panel variant: fronts whose panel products are large
+  // enough take only their diagonal block's row tasks in the fused kernel,
+  // then the block inverses (binv) and L21 / U12 as tensor-core GEMMs
+  // (panel); the other fronts keep their full task lists
+  bool tc = false;
+  BlockTask* tasks_tc = nullptr;
+  int ntasks_tc = 0;
+  BinvTask* binv = nullptr;
+  int nbinv = 0;
+  GemmBatch panel;
+  double flops_tc = 0, elems_tc = 0, binv_flops = 0, binv_elems = 0;
 };
 
 struct LevelSched {
@@ -204,6 +216,8 @@ class CudaEngine : public Engine {
                             (int)tc_smem_bytes()));
     CK(cudaFuncSetAttribute(k_gemm_tcp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)tc_smem_bytes()));
+    CK(cudaFuncSetAttribute(k_block_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)binv_smem()));
     {
       int sms = 0, nb = 0;
       CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
@@ -222,6 +236,10 @@ class CudaEngine : public Engine {
       verbose_ = vb && vb[0] == '1';
       const char* pbk = getenv("SNU_PANEL_BLOCK");
       use_block_ = !(pbk && pbk[0] == '0');
+      // SNU_TC_PANEL=N: FP32 panel products on the tensor cores for levels
+      // with at least N fronts (0: never)
+      const char* tcp = getenv("SNU_TC_PANEL");
+      if (tcp) tcpanel_min_ = atoi(tcp);
     }
     {
       int rc2;
@@ -438,7 +456,8 @@ class CudaEngine : public Engine {
       if (!d_F64_ && (rc = alloc(d_F64_, (size_t)arena_))) return rc;
       if (!d_I64_ && (rc = alloc(d_I64_, (size_t)invtot_))) return rc;
     } else {
-      if (!d_F32_ && (rc = alloc(d_F32_, (size_t)arena_))) return rc;
+      // (FP32: the outer blocks' triangle inverses after the fronts)
+      if (!d_F32_ && (rc = alloc(d_F32_, (size_t)(invb_base_ + invb_need_)))) return rc;
       if (!d_I32_ && (rc = alloc(d_I32_, (size_t)invtot_))) return rc;
     }
     if (precision == 1 && autotune_ && !tuned_ && force_tcp_ < 0) {
@@ -521,23 +540,9 @@ class CudaEngine : public Engine {
       err_ = "solve before factorize";
       return ENG_ESTATE;
     }
-    if (nrhs > SOLVE_CHUNK) {
-      // columns in chunks: work vectors stay bounded by SOLVE_CHUNK columns
-      SolveReport agg;
-      for (int c0 = 0; c0 < nrhs; c0 += SOLVE_CHUNK) {
-        SolveReport r;
-        int rc = solve(dB + (size_t)c0 * ldb, dX + (size_t)c0 * ldb,
-                       std::min(SOLVE_CHUNK, nrhs - c0), ldb, stream,
-                       precision, &r);
-        if (rc) return rc;
-        agg.backward_error = std::max(agg.backward_error, r.backward_error);
-        agg.ir_iters = std::max(agg.ir_iters, r.ir_iters);
-        agg.fp64_fallback |= r.fp64_fallback;
-        agg.seconds += r.seconds;
-      }
-      if (rep) *rep = agg;
-      return ENG_OK;
-    }
+    // all columns in one pass: the sweeps run in groups of up to RG columns
+    // through work vectors sized for one group, the residual, norms and
+    // refinement cover every column at once
     cudaStream_t st = stream ? (cudaStream_t)stream : stream_;
     int rc;
     if ((rc = ensure_solve(nrhs, precision == 0))) return rc;
@@ -547,7 +552,8 @@ class CudaEngine : public Engine {
     CK(cudaEventRecord(sev0_, st));
     SolveReport r;
     if (precision == 0) {
-      if ((rc = tree_solve<double>(d_F64_, d_I64_, d_W64_, d_Y64_, dB, ldb, dX, ldb, nrhs, st)))
+      if ((rc = tree_solve_cols<double>(d_F64_, d_I64_, d_W64_, d_Y64_, dB,
+                                        ldb, dX, ldb, nrhs, st)))
         return rc;
       if ((rc = residual_norms(dB, ldb, dX, ldb, nrhs, st, &r.backward_error)))
         return rc;
@@ -743,10 +749,11 @@ class CudaEngine : public Engine {
   }
   // One cooperative launch of the fused panel kernel for an outer block.
   template <typename T>
-  int block_launch(const OuterBlock& O, T* F, T* I, cudaStream_t st) {
+  int block_launch(const OuterBlock& O, const BlockTask* tasks, int ntasks,
+                   T* F, T* I, cudaStream_t st) {
     auto k = k_panel_block<T>;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(std::min(O.ntasks, coop_cap_[(const void*)k]));
+    cfg.gridDim = dim3(std::min(ntasks, coop_cap_[(const void*)k]));
     cfg.blockDim = dim3(256);
     cfg.dynamicSmemBytes = block_smem<T>();
     cfg.stream = st;
@@ -756,7 +763,7 @@ class CudaEngine : public Engine {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     ++launches_;
-    CK(cudaLaunchKernelEx(&cfg, k, (const BlockTask*)O.tasks, O.ntasks,
+    CK(cudaLaunchKernelEx(&cfg, k, tasks, ntasks,
                           (const FrontDev*)d_fr_, F, I, O.K0, opt_.pivot_eps,
                           d_flags_, d_fflags_, (const int64_t*)d_flag_off_,
                           d_fflags_ + 2 * ntileflags_ + O.ctr, d_flags_ + 5));
@@ -995,7 +1002,7 @@ class CudaEngine : public Engine {
       t.m = g.m, t.n = g.n, t.k = g.k, t.kpad = (g.k + TC_BK - 1) / TC_BK * TC_BK;
       t.a = g.a, t.b = g.b, t.c = g.c;
       t.lda = g.lda, t.ldb = g.ldb, t.ldc = g.ldc;
-      t.pc = g.pc, t.rel = g.rel, t.pld = g.pld, t.pad = 0;
+      t.pc = g.pc, t.rel = g.rel, t.pld = g.pld, t.mode = g.pad;
       t.apack = apos;
       apos += (int64_t)g.m * 3 * t.kpad;
       apos = (apos + 63) / 64 * 64;
@@ -1078,8 +1085,96 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
+  // The FP32 tensor-core panel variant of outer block O (see OuterBlock).
+  // A front takes it when both panel products are large enough for the
+  // tensor cores: KB >= 64 pivot columns in the block, >= 64 rows below its
+  // diagonal block's row tasks and >= 64 columns right of the block (so
+  // neither product has a SIMT remainder, whose tiles would race with the
+  // in-place overwrite; the tensor-core path packs its operands first).
+  int tc_panel_schedule(const LevelSched& L, OuterBlock& O, int maxrows) {
+    const FrontPlan& fp = *fp_;
+    std::vector<char> tcf(L.f1 - L.f0, 0);
+    std::vector<BinvTask> bi;
+    std::vector<GemmProb> pg;
+    int64_t slot = 0;
+    for (int f = L.f0; f < L.f1; f++) {
+      const FrontInfo& fi = fp.fronts[f];
+      if (fi.p <= O.K0) continue;
+      const int K0 = O.K0, K1 = std::min(K0 + OB, fi.p), KB = K1 - K0;
+      const int nt = (KB + NB - 1) / NB, Rs = K0 + nt * NB, dim = fi.p + fi.q;
+      if (KB < 64 || dim - Rs < 64 || dim - K1 < 64) continue;
+      // (a batch holds at most 65535 tensor-core problems, two per front;
+      // the rest of a very wide level keeps the fused path)
+      if (pg.size() + 2 > 65535) continue;
+      tcf[f - L.f0] = 1;
+      const int64_t out = invb_base_ + slot * 2 * OB * OB;
+      slot++;
+      for (int j = 0; j < nt; j++) {
+        bi.push_back({f, 0, j, 0, out});
+        bi.push_back({f, 1, j, 0, out});
+        // block substitution: strip j of L has nt - 1 - j off-diagonal
+        // tiles, tile i summing i - j products plus one with the inverse
+        const int offd = nt - 1 - j;
+        O.binv_flops += 2.0 * offd * (offd + 3) / 2.0 * 2.0 * NB * NB * NB;
+        O.binv_elems += 2.0 * (offd + 1) * NB * NB;
+      }
+      const int64_t o = fi.offset, ld = fi.ld;
+      GemmProb gl{dim - Rs, KB, KB, fi.ld, OB, fi.ld, o + Rs + K0 * ld,
+                  out + (int64_t)OB * OB, o + Rs + K0 * ld};
+      gl.pad = 1;  // C = A Uinv_B (in place: operands are packed first)
+      GemmProb gu{KB, dim - K1, KB, OB, fi.ld, fi.ld, out, o + K0 + K1 * ld,
+                  o + K0 + K1 * ld};
+      gu.pad = 1;  // C = Linv_B A
+      if (!tc_eligible(gl) || !tc_eligible(gu)) {
+        err_ = "tensor-core panel problem below the tensor-core size";
+        return ENG_EINVAL;
+      }
+      pg.push_back(gl);
+      pg.push_back(gu);
+      // the fused kernel's share: the diagonal block's rows only
+      const double rows = nt * NB;
+      O.flops_tc += KB * (2.0 / 3.0 * NB * NB + 2.0 * rows * NB) +
+                    2.0 * rows * KB * KB / 2;
+      O.elems_tc += 2.0 * rows * KB;
+    }
+    if (bi.empty()) return ENG_OK;
+    O.tc = true;
+    invb_need_ = std::max(invb_need_, slot * 2 * OB * OB);
+    std::vector<BlockTask> bt;
+    for (int r = 0; r < maxrows; r++)
+      for (int f = L.f0; f < L.f1; f++) {
+        const FrontInfo& fi = fp.fronts[f];
+        if (fi.p <= O.K0 || O.K0 + r * NB >= fi.p + fi.q) continue;
+        if (tcf[f - L.f0]) {
+          const int KB = std::min(O.K0 + OB, fi.p) - O.K0;
+          if (r >= (KB + NB - 1) / NB) continue;  // rows of the GEMM
+        }
+        bt.push_back({f, 0, r});
+      }
+    for (int f = L.f0; f < L.f1; f++) {
+      const FrontInfo& fi = fp.fronts[f];
+      if (fi.p <= O.K0 || tcf[f - L.f0]) continue;
+      const int K1 = std::min(O.K0 + OB, fi.p), dim = fi.p + fi.q;
+      for (int c = 0; K1 + c * NB < dim; c++) bt.push_back({f, 1, c});
+      const int kk = K1 - O.K0;
+      const double rows = dim - O.K0, cols = dim - K1;
+      O.flops_tc += kk * (2.0 / 3.0 * NB * NB + 2.0 * rows * NB) +
+                    2.0 * rows * kk * kk / 2 + 2.0 * cols * kk * kk;
+      O.elems_tc += 2.0 * rows * kk + 2.0 * cols * kk;
+    }
+    O.ntasks_tc = (int)bt.size();
+    int rc;
+    if (!bt.empty() && (rc = upload(O.tasks_tc, bt))) return rc;
+    O.nbinv = (int)bi.size();
+    if ((rc = upload(O.binv, bi))) return rc;
+    return gemm_batch(pg, O.panel);
+  }
+
   int build_schedule() {
     const FrontPlan& fp = *fp_;
+    // the outer blocks' triangle inverses follow the fronts (FP32)
+    invb_base_ = (arena_ + 63) / 64 * 64;
+    invb_need_ = 0;
     lv_.assign(nlevels_, LevelSched());
     int mc = fp.max_children;
     int rc;
@@ -1243,6 +1338,9 @@ class CudaEngine : public Engine {
         O.ntasks = (int)bt.size();
         if (!bt.empty() && (rc = upload(O.tasks, bt))) return rc;
         if ((rc = gemm_batch(og, O.outer))) return rc;
+        if (use_tc_ && tcpanel_min_ > 0 && L.f1 - L.f0 >= tcpanel_min_ &&
+            (rc = tc_panel_schedule(L, O, maxrows)))
+          return rc;
       }
       if (verbose_) {
         int nf = 0, pmax = 0, qmax = 0;
@@ -1296,8 +1394,9 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
-  // Work vectors for nrhs (<= SOLVE_CHUNK) columns: FP64 (fp64) or FP32
-  // sweeps, FP64 residual and correction.  Buffers only grow; a grown
+  // Work vectors of a solve of nrhs columns: W and Y (FP64 for fp64, else
+  // FP32) for one group of up to RG columns, the FP64 residual and
+  // correction for all columns.  Buffers only grow; a grown
   // buffer replaces (and frees) the smaller one.
   template <typename T>
   int grow(T*& p, size_t& cap, size_t need) {
@@ -1313,7 +1412,8 @@ class CudaEngine : public Engine {
   }
   int ensure_solve(int nrhs, bool fp64) {
     int rc;
-    const size_t w = (size_t)wtot_ * nrhs, y = (size_t)ytot_ * nrhs;
+    const size_t g = (size_t)std::min(nrhs, RG);  // one column group
+    const size_t w = (size_t)wtot_ * g, y = (size_t)ytot_ * g;
     const size_t r = (size_t)n_ * nrhs;
     if (fp64) {
       if ((rc = grow(d_W64_, wcap64_, w)) || (rc = grow(d_Y64_, ycap64_, y)))
@@ -1423,9 +1523,27 @@ class CudaEngine : public Engine {
       int pi;
       if (use_block_) {
         for (const OuterBlock& O : L.ob) {
-          if (O.ntasks) {
+          if (sizeof(T) == 4 && O.tc) {
+            // FP32: diagonal blocks in the fused kernel, their triangles'
+            // inverses, then L21 / U12 on the tensor cores
+            if (O.ntasks_tc) {
+              pi = prof_begin(KF_PANEL_BLOCK, st);
+              if ((rc = block_launch<T>(O, O.tasks_tc, O.ntasks_tc, F, I, st)))
+                return rc;
+              prof_end(pi, KF_PANEL_BLOCK, st, O.flops_tc, O.elems_tc * es);
+            }
+            if (O.nbinv) {
+              pi = prof_begin(KF_BLOCK_INV, st);
+              k_block_inv<<<O.nbinv, 256, binv_smem(), st>>>(
+                  O.binv, d_fr_, (const float*)F, (const float*)I, (float*)F,
+                  O.K0);
+              CKL();
+              prof_end(pi, KF_BLOCK_INV, st, O.binv_flops, O.binv_elems * es);
+            }
+            if ((rc = factor_gemm(O.panel, F, st, KF_GEMM_PANEL))) return rc;
+          } else if (O.ntasks) {
             pi = prof_begin(KF_PANEL_BLOCK, st);
-            if ((rc = block_launch<T>(O, F, I, st))) return rc;
+            if ((rc = block_launch<T>(O, O.tasks, O.ntasks, F, I, st))) return rc;
             prof_end(pi, KF_PANEL_BLOCK, st, O.flops, O.elems * es);
           }
           if ((rc = factor_gemm(O.outer, F, st, KF_GEMM_TRAIL))) return rc;
@@ -1740,7 +1858,8 @@ class CudaEngine : public Engine {
     int total = n_ * nrhs;
     int blocks = (total + 255) / 256;
     // x0 = solve32(b)
-    if ((rc = tree_solve<float>(d_F32_, d_I32_, d_W32_, d_Y32_, B, ldb, X, ldx, nrhs, st)))
+    if ((rc = tree_solve_cols<float>(d_F32_, d_I32_, d_W32_, d_Y32_, B, ldb, X, ldx,
+                                      nrhs, st)))
       return rc;
     double be = 0, prev = INFINITY;
     int it = 0, stagnant = 0;
@@ -1756,8 +1875,8 @@ class CudaEngine : public Engine {
           if (frc) return frc;
         }
         if ((rc = ensure_solve(nrhs, true))) return rc;
-        if ((rc = tree_solve<double>(d_F64_, d_I64_, d_W64_, d_Y64_, d_R_, n_, d_D_, n_,
-                                     nrhs, st)))
+        if ((rc = tree_solve_cols<double>(d_F64_, d_I64_, d_W64_, d_Y64_, d_R_, n_,
+                                          d_D_, n_, nrhs, st)))
           return rc;
         int pi = prof_begin(KF_RESIDUAL, st);
         k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
@@ -1771,7 +1890,8 @@ class CudaEngine : public Engine {
       else stagnant = 0;
       prev = be;
       // d = solve32(r); x += d
-      if ((rc = tree_solve<float>(d_F32_, d_I32_, d_W32_, d_Y32_, d_R_, n_, d_D_, n_, nrhs, st)))
+      if ((rc = tree_solve_cols<float>(d_F32_, d_I32_, d_W32_, d_Y32_, d_R_, n_, d_D_,
+                                      n_, nrhs, st)))
         return rc;
       int pi = prof_begin(KF_RESIDUAL, st);
       k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
@@ -1823,6 +1943,12 @@ class CudaEngine : public Engine {
   bool use_tc_ = true;
   bool use_graphs_ = true;
   bool use_block_ = true;
+  // FP32 tensor-core panel products for levels with at least this many
+  // fronts; off unless SNU_TC_PANEL sets it (on the 64^3 workload the
+  // inverse-based tensor-core products measured 0.5 ms slower per
+  // factorization than the fused kernel's SIMT products at leaf levels)
+  int tcpanel_min_ = 0;
+  int64_t invb_base_ = 0, invb_need_ = 0;  // triangle-inverse scratch (FP32)
   bool verbose_ = false;  // SNU_VERBOSE=1: set-up phase timings on stderr
   static double wall_s() {
     return std::chrono::duration<double>(
@@ -1917,7 +2043,7 @@ const char* kernel_family_name(int f) {
   static const char* names[KF_COUNT] = {
       "assemble", "extend_add", "diag_lu", "panel_trsm", "gemm_trail",
       "gemm_schur", "solve_diag", "solve_gemm", "solve_misc", "residual",
-      "panel_block"};
+      "panel_block", "block_inv", "gemm_panel"};
   return (f >= 0 && f < KF_COUNT) ? names[f] : "?";
 }
 

@@ -21,7 +21,6 @@
 namespace snu {
 
 constexpr int RG = 16;          // right-hand sides per register group
-constexpr int SOLVE_CHUNK = 16; // right-hand sides per solve pass
 constexpr int DIAG_ROWS = 128;  // rows of a pivot-block chunk (= threads)
 constexpr long WAVE_SPIN_LIMIT = 1L << 22;
 

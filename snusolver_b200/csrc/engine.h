@@ -49,6 +49,8 @@ enum KernelFamily {
   KF_SOLVE_MISC,     // gathers, scatters and extend-adds of the sweeps
   KF_RESIDUAL,       // FP64 residual, norms and solution updates
   KF_PANEL_BLOCK,    // fused outer-block panels (tiles, L/U blocks, updates)
+  KF_BLOCK_INV,      // inverses of an outer block's triangles (FP32)
+  KF_GEMM_PANEL,     // L21 = A21 Uinv, U12 = Linv A12 on the tensor cores
   KF_COUNT
 };
 const char* kernel_family_name(int f);

@@ -224,12 +224,14 @@ def test_autotuned_factorization_matches(gpu, tmp_path):
 
 @pytest.mark.parametrize("env", [("SNU_PANEL_BLOCK", "0"), ("SNU_TC_GEMM", "0"),
                                  ("SNU_TC_PERSIST", "1"), ("SNU_TC_PERSIST", "0"),
-                                 ("SNU_GRAPHS", "0")])
+                                 ("SNU_GRAPHS", "0"), ("SNU_TC_PANEL", "0"),
+                                 ("SNU_TC_PANEL", "1")])
 def test_alternative_paths_match(gpu, monkeypatch, env):
     # the paths behind the engine switches (read when an engine is made):
     # per-step panels instead of the fused outer-block kernel, SIMT instead
     # of tensor-core FP32 GEMMs, the persistent GEMM forced on or off, no
-    # CUDA graph -- each must reproduce the oracle like the default path
+    # CUDA graph, the FP32 panel products on the tensor cores for no level
+    # or for every level -- each must reproduce the oracle like the default
     monkeypatch.setenv(*env)
     rng = np.random.default_rng(41)
     rp, ci, v = _random_unsym(rng, 33, 30, 80)
@@ -323,4 +325,4 @@ def test_fp64_fallback_when_refinement_stops(gpu):
     # a second solve reuses the FP64 factors
     x2 = s.solve(B[:, 0])
     assert s.stats()["fp64_fallback"] == 1
-    _close(x2, x, 1e-13, "second solve")
+    _close(x2, x, 1e-11, "second solve")
