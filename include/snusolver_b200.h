@@ -110,6 +110,18 @@ SNU_API snu_status snu_analyze(snu_handle* h, int n, int nnz,
    the same pattern (n, nnz, rowptr, colidx) keeps the analysis and, after
    snu_plan, the plan. */
 SNU_API snu_status snu_plan(snu_handle* h);
+/* No reference counterpart: read-back of the front plan (after snu_plan or
+   snu_construct) for checks and host restatements of the numerics.
+   sizes[6] = {nfronts, gidx entries, rel entries, assembly entries, arena
+   elements, levels}.  fronts[8 per front] = {p, q, ld, parent, level,
+   heap block, static-pivot guard, leaf rank}; offsets[3 per front] = {arena
+   offset, gidx offset, rel offset}; gidx: original row of each front index
+   (P then Q); rel: position of each Q row in the parent; assembly:
+   F[asm_pos[k]] = vals[asm_val[k]].  Any output pointer may be NULL. */
+SNU_API snu_status snu_front_plan_sizes(const snu_handle* h, int64_t* sizes);
+SNU_API snu_status snu_get_front_plan(const snu_handle* h, int* fronts,
+                                      int64_t* offsets, int* gidx, int* rel,
+                                      int64_t* asm_pos, int* asm_val);
 /* snu_analyze + device plan + values (host arrays, reference CSR order). */
 SNU_API snu_status snu_construct(snu_handle* h, int n, int nnz,
                                  const int* rowptr, const int* colidx,
@@ -168,6 +180,46 @@ SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st);
 SNU_API snu_status snu_solve_device_noalloc(snu_handle* h, const double* dB,
                                             double* dX, int nrhs, int ldb,
                                             void* stream);
+
+/* ---- separator-tree distribution over ranks (one GPU each) ----
+   Replaces the reference's MPI data plane: each rank factors the subtree of
+   heap node world + rank (the reference's owner map, SnuMat.cu:24-30); the
+   updates its subtree sends to the shared top separators are summed over
+   the ranks by the caller's collective (the reference's pairwise
+   core_reduction / reduction_gpu, kernel_sparse.cu:54-90,
+   SnuMat_factorize.cu:29-124), after which every rank factors the shared
+   fronts; the solve exchanges the shared fronts' work vectors (scatter_b and
+   the vectorAdd reduction, SnuMat_factorize.cu:22-27, 126-187) and the
+   rows of X.  The collectives are the caller's (snusolver_b200.dist drives
+   them with torch.distributed); these calls are the device steps between.
+   snu_dist_init: before snu_construct; world a power of two <= nleaves. */
+SNU_API snu_status snu_dist_init(snu_handle* h, int rank, int world);
+/* phase 1: this rank's subtree (its updates to the shared fronts stay in
+   place); phase 2: the shared fronts, after their sum over the ranks. */
+SNU_API snu_status snu_dist_factorize(snu_handle* h, int phase);
+/* Size of the exchange buffer: kind 0 the shared fronts, kind 1 their
+   solve work vectors for nrhs columns; element size 8 (FP64) or 4. */
+SNU_API snu_status snu_dist_buffer(const snu_handle* h, int kind, int nrhs,
+                                   int64_t* elems, int* elem_bytes);
+/* dir 0: shared regions -> device buffer dbuf; dir 1: dbuf -> shared
+   regions (synchronizes the handle's stream). */
+SNU_API snu_status snu_dist_copy(snu_handle* h, int kind, int dir, int nrhs,
+                                 void* dbuf);
+/* Solve of 1..16 columns (device arrays, FP64, leading dimension ldb) in two
+   phases around the sum of the shared work vectors (kind 1): phase 1 the
+   subtree's forward sweep, phase 2 the shared fronts' forward and back
+   sweeps, the subtree's back sweep; X then holds this rank's rows (the
+   others zero) for the caller's sum over the ranks.  No refinement: the
+   caller refines with snu_residual_device. */
+SNU_API snu_status snu_dist_solve(snu_handle* h, int phase, const double* dB,
+                                  double* dX, int nrhs, int ldb);
+/* R = B - A X on the original matrix (FP64, device arrays with leading
+   dimension ldb) and the backward error max_r ||R||inf / (||A||inf ||X||inf
+   + ||B||inf) (no reference counterpart; driver.cpp:12-28 prints the
+   maximum residual). */
+SNU_API snu_status snu_residual_device(snu_handle* h, const double* dB,
+                                       const double* dX, double* dR, int nrhs,
+                                       int ldb, double* berr);
 
 /* ---- execution control and measurement (no reference counterpart) ---- */
 /* All device work of the handle goes to this cudaStream_t (NULL: the

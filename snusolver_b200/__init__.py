@@ -79,7 +79,7 @@ class _LaunchRec(C.Structure):
 KERNEL_FAMILIES = ("assemble", "extend_add", "diag_lu", "panel_trsm",
                    "gemm_trail", "gemm_schur", "solve_diag", "solve_gemm",
                    "solve_misc", "residual", "panel_block", "block_inv",
-                   "gemm_panel")
+                   "gemm_panel", "sweep")
 
 _lib = None
 _I = C.POINTER(C.c_int)
@@ -119,6 +119,9 @@ _EXPORTS = {
     "snu_get_profile": (C.c_int, [C.c_void_p, C.POINTER(_KStat), C.c_int,
                                   C.POINTER(C.c_int)]),
     "snu_reset_profile": (C.c_int, [C.c_void_p]),
+    "snu_front_plan_sizes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "snu_get_front_plan": (C.c_int, [C.c_void_p, _I, C.POINTER(C.c_int64), _I,
+                                     _I, C.POINTER(C.c_int64), _I]),
 }
 
 
@@ -344,6 +347,32 @@ class Solver:
         pm, r, c = (np.empty(self.nnz, np.int32) for _ in range(3))
         self._check(self._lib.snu_get_coo(self._h, _iptr(pm), _iptr(r), _iptr(c)))
         return pm, r, c
+
+    def front_plan(self):
+        """The front plan (after :meth:`plan` or :meth:`construct`): dict of
+        per-front arrays p, q, ld, parent, level, block, guard, leaf_rank,
+        offset, idx_offset, rel_offset, plus gidx, rel, asm_pos, asm_val,
+        arena and nlevels (see ``snu_get_front_plan``)."""
+        sz = (C.c_int64 * 6)()
+        self._check(self._lib.snu_front_plan_sizes(self._h, sz))
+        nf, ng, nr, na, arena, nl = (int(x) for x in sz)
+        fr = np.empty((max(nf, 1), 8), np.int32)
+        off = np.empty((max(nf, 1), 3), np.int64)
+        gidx = np.empty(max(ng, 1), np.int32)
+        rel = np.empty(max(nr, 1), np.int32)
+        apos = np.empty(max(na, 1), np.int64)
+        aval = np.empty(max(na, 1), np.int32)
+        i64 = C.POINTER(C.c_int64)
+        self._check(self._lib.snu_get_front_plan(
+            self._h, _iptr(fr), off.ctypes.data_as(i64), _iptr(gidx),
+            _iptr(rel), apos.ctypes.data_as(i64), _iptr(aval)))
+        keys = ("p", "q", "ld", "parent", "level", "block", "guard", "leaf_rank")
+        out = {k: fr[:nf, i].copy() for i, k in enumerate(keys)}
+        for i, k in enumerate(("offset", "idx_offset", "rel_offset")):
+            out[k] = off[:nf, i].copy()
+        out.update(gidx=gidx[:ng], rel=rel[:nr], asm_pos=apos[:na],
+                   asm_val=aval[:na], arena=arena, nlevels=nl)
+        return out
 
     def leaf_info(self, rank):
         info = np.empty(8, np.int32)

@@ -89,6 +89,72 @@ bool valid_csr(int n, int nnz, const int* rowptr, const int* colidx,
 
 }  // namespace
 
+namespace snu {
+snu_status solve_pieces(snu_handle* h, const std::vector<SolvePiece>& pieces) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 3) return fail(h, SNU_ESTATE, "solve before factorize");
+  const int n = h->S.n;
+  // the columns of all blocks in order: (B column, X column)
+  std::vector<std::pair<const double*, double*>> cols;
+  for (const SolvePiece& p : pieces) {
+    if (!p.B || !p.X || p.nrhs <= 0 || p.ldb < n)
+      return fail(h, SNU_EINVAL, "bad right-hand side arguments");
+    for (int r = 0; r < p.nrhs; r++)
+      cols.push_back({p.B + (size_t)r * p.ldb, p.X + (size_t)r * p.ldb});
+  }
+  const int nrhs = (int)cols.size();
+  if (nrhs == 0) return fail(h, SNU_EINVAL, "no right-hand sides");
+  // staged in chunks of up to 64 columns (one refinement loop per chunk),
+  // so device staging stays bounded
+  const int chunk = std::min(nrhs, 64);
+  size_t need = (size_t)n * chunk * 2;
+  if (need > h->dcap) {
+    if (h->dB) cudaFree(h->dB);
+    h->dB = nullptr;
+    h->dcap = 0;
+    if (cudaMalloc((void**)&h->dB, need * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(h, SNU_ENOMEM, "cannot allocate right-hand side staging");
+    }
+    h->dcap = need;
+  }
+  // copies on the engine's stream, so they are ordered with its kernels
+  cudaStream_t st = (cudaStream_t)h->eng->stream();
+  double be = 0, secs = 0;
+  int iters = 0, fb = 0;
+  snu_status result = SNU_OK;
+  for (int c0 = 0; c0 < nrhs; c0 += chunk) {
+    const int nc = std::min(chunk, nrhs - c0);
+    double* dB = h->dB;
+    double* dX = h->dB + (size_t)n * nc;
+    for (int r = 0; r < nc; r++)
+      if (cudaMemcpyAsync(dB + (size_t)r * n, cols[c0 + r].first,
+                          sizeof(double) * n, cudaMemcpyHostToDevice,
+                          st) != cudaSuccess)
+        return fail(h, SNU_ECUDA, "host to device copy failed");
+    snu_status s = snu_solve_device(h, dB, dX, nc, n, st);
+    if (s != SNU_OK && s != SNU_ENOTCONV) return s;
+    if (s != SNU_OK) result = s;
+    be = std::max(be, h->stats.backward_error);
+    iters = std::max(iters, h->stats.ir_iters);
+    fb |= h->stats.fp64_fallback;
+    secs += h->stats.solve_s;
+    for (int r = 0; r < nc; r++)
+      if (cudaMemcpyAsync(cols[c0 + r].second, dX + (size_t)r * n,
+                          sizeof(double) * n, cudaMemcpyDeviceToHost,
+                          st) != cudaSuccess)
+        return fail(h, SNU_ECUDA, "device to host copy failed");
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return fail(h, SNU_ECUDA, "stream synchronize failed");
+  }
+  h->stats.backward_error = be;
+  h->stats.ir_iters = iters;
+  h->stats.fp64_fallback = fb;
+  h->stats.solve_s = secs;
+  return result;
+}
+}  // namespace snu
+
 extern "C" {
 
 SNU_API const char* snu_status_string(snu_status s) {
@@ -213,6 +279,46 @@ SNU_API snu_status snu_plan(snu_handle* h) {
   h->stats.nlevels = h->FP.nlevels;
   h->stats.factor_entries = h->FP.factor_entries;
   h->stats.factor_flops = h->FP.flops;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_front_plan_sizes(const snu_handle* h, int64_t* sizes) {
+  if (!h || !sizes) return fail(const_cast<snu_handle*>(h), SNU_EINVAL, "null argument");
+  if (!(h->plan_ready || h->state >= 2))
+    return fail(const_cast<snu_handle*>(h), SNU_ESTATE, "no front plan (snu_plan)");
+  const snu::FrontPlan& fp = h->FP;
+  sizes[0] = fp.nfronts;
+  sizes[1] = (int64_t)fp.gidx.size();
+  sizes[2] = (int64_t)fp.rel.size();
+  sizes[3] = (int64_t)fp.asm_pos.size();
+  sizes[4] = fp.arena;
+  sizes[5] = fp.nlevels;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_get_front_plan(const snu_handle* h, int* fronts,
+                                      int64_t* offsets, int* gidx, int* rel,
+                                      int64_t* asm_pos, int* asm_val) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (!(h->plan_ready || h->state >= 2))
+    return fail(const_cast<snu_handle*>(h), SNU_ESTATE, "no front plan (snu_plan)");
+  const snu::FrontPlan& fp = h->FP;
+  for (int f = 0; f < fp.nfronts; f++) {
+    const snu::FrontInfo& fi = fp.fronts[f];
+    if (fronts) {
+      int* o = fronts + (size_t)f * 8;
+      o[0] = fi.p, o[1] = fi.q, o[2] = fi.ld, o[3] = fi.parent;
+      o[4] = fi.level, o[5] = fi.block, o[6] = fi.guard, o[7] = fi.leaf_rank;
+    }
+    if (offsets) {
+      int64_t* o = offsets + (size_t)f * 3;
+      o[0] = fi.offset, o[1] = fi.idx_offset, o[2] = fi.rel_offset;
+    }
+  }
+  if (gidx) std::memcpy(gidx, fp.gidx.data(), sizeof(int) * fp.gidx.size());
+  if (rel) std::memcpy(rel, fp.rel.data(), sizeof(int) * fp.rel.size());
+  if (asm_pos) std::memcpy(asm_pos, fp.asm_pos.data(), sizeof(int64_t) * fp.asm_pos.size());
+  if (asm_val) std::memcpy(asm_val, fp.asm_val.data(), sizeof(int) * fp.asm_val.size());
   return SNU_OK;
 }
 
@@ -379,61 +485,90 @@ SNU_API snu_status snu_solve_device_noalloc(snu_handle* h, const double* dB,
   return SNU_OK;
 }
 
+
 SNU_API snu_status snu_solve(snu_handle* h, const double* B, double* X,
                              int nrhs, int ldb) {
+  return snu::solve_pieces(h, {{B, X, nrhs, ldb}});
+}
+
+// ---- separator-tree distribution ----------------------------------------
+
+SNU_API snu_status snu_dist_init(snu_handle* h, int rank, int world) {
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
-  if (h->state < 3) return fail(h, SNU_ESTATE, "solve before factorize");
-  if (!B || !X || nrhs <= 0 || ldb < h->S.n)
-    return fail(h, SNU_EINVAL, "bad right-hand side arguments");
-  const int n = h->S.n;
-  // staged in chunks of up to 64 columns (one refinement loop per chunk),
-  // so device staging stays bounded
-  const int chunk = std::min(nrhs, 64);
-  size_t need = (size_t)n * chunk * 2;
-  if (need > h->dcap) {
-    if (h->dB) cudaFree(h->dB);
-    h->dB = nullptr;
-    h->dcap = 0;
-    if (cudaMalloc((void**)&h->dB, need * sizeof(double)) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(h, SNU_ENOMEM, "cannot allocate right-hand side staging");
-    }
-    h->dcap = need;
+  if (h->state >= 2) return fail(h, SNU_ESTATE, "distribute before construct");
+  if (h->batch) return fail(h, SNU_EINVAL, "not available on a batch handle");
+  if (world < 1 || (world & (world - 1)) || world > h->opts.nleaves ||
+      rank < 0 || rank >= world)
+    return fail(h, SNU_EINVAL,
+                "world must be a power of two up to nleaves, 0 <= rank < world");
+  h->dist_rank = rank;
+  h->dist_world = world;
+  return SNU_OK;
+}
+
+static bool dist_ready(snu_handle* h, int state) {
+  if (!h) return false;
+  if (h->dist_world <= 1) {
+    fail(h, SNU_ESTATE, "not a distributed handle (snu_dist_init)");
+    return false;
   }
-  // copies on the engine's stream, so they are ordered with its kernels
-  cudaStream_t st = (cudaStream_t)h->eng->stream();
-  double be = 0, secs = 0;
-  int iters = 0, fb = 0;
-  snu_status result = SNU_OK;
-  for (int c0 = 0; c0 < nrhs; c0 += chunk) {
-    const int nc = std::min(chunk, nrhs - c0);
-    double* dB = h->dB;
-    double* dX = h->dB + (size_t)n * nc;
-    for (int r = 0; r < nc; r++)
-      if (cudaMemcpyAsync(dB + (size_t)r * n, B + (size_t)(c0 + r) * ldb,
-                          sizeof(double) * n, cudaMemcpyHostToDevice,
-                          st) != cudaSuccess)
-        return fail(h, SNU_ECUDA, "host to device copy failed");
-    snu_status s = snu_solve_device(h, dB, dX, nc, n, st);
-    if (s != SNU_OK && s != SNU_ENOTCONV) return s;
-    if (s != SNU_OK) result = s;
-    be = std::max(be, h->stats.backward_error);
-    iters = std::max(iters, h->stats.ir_iters);
-    fb |= h->stats.fp64_fallback;
-    secs += h->stats.solve_s;
-    for (int r = 0; r < nc; r++)
-      if (cudaMemcpyAsync(X + (size_t)(c0 + r) * ldb, dX + (size_t)r * n,
-                          sizeof(double) * n, cudaMemcpyDeviceToHost,
-                          st) != cudaSuccess)
-        return fail(h, SNU_ECUDA, "device to host copy failed");
-    if (cudaStreamSynchronize(st) != cudaSuccess)
-      return fail(h, SNU_ECUDA, "stream synchronize failed");
+  if (h->state < state) {
+    fail(h, SNU_ESTATE, state >= 3 ? "solve before factorize"
+                                   : "factorize before construct");
+    return false;
   }
-  h->stats.backward_error = be;
-  h->stats.ir_iters = iters;
-  h->stats.fp64_fallback = fb;
-  h->stats.solve_s = secs;
-  return result;
+  return true;
+}
+
+SNU_API snu_status snu_dist_factorize(snu_handle* h, int phase) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (!dist_ready(h, 2)) return SNU_ESTATE;
+  NvtxRange nv(phase == 1 ? "snu_dist_factorize 1" : "snu_dist_factorize 2");
+  const int prec = h->opts.precision == SNU_FP64 ? 0 : 1;
+  snu_status s = from_engine(h, h->eng->dist_factor(prec, phase));
+  if (s == SNU_OK && phase == 2) {
+    h->state = 3;
+    h->stats.tiny_pivots = h->eng->tiny_pivots();
+    h->stats.device_bytes = h->eng->device_bytes();
+  }
+  return s;
+}
+
+SNU_API snu_status snu_dist_buffer(const snu_handle* h, int kind, int nrhs,
+                                   int64_t* elems, int* elem_bytes) {
+  if (!h || !elems || !elem_bytes || (kind != 0 && kind != 1) || nrhs < 0)
+    return fail(const_cast<snu_handle*>(h), SNU_EINVAL, "bad arguments");
+  if (!dist_ready(const_cast<snu_handle*>(h), 2)) return SNU_ESTATE;
+  *elems = h->eng->dist_elems(kind, nrhs);
+  *elem_bytes = h->opts.precision == SNU_FP64 ? 8 : 4;
+  return SNU_OK;
+}
+
+SNU_API snu_status snu_dist_copy(snu_handle* h, int kind, int dir, int nrhs,
+                                 void* dbuf) {
+  if (!h || !dbuf || (kind != 0 && kind != 1) || (dir != 0 && dir != 1))
+    return fail(h, SNU_EINVAL, "bad arguments");
+  if (!dist_ready(h, 2)) return SNU_ESTATE;
+  const int prec = h->opts.precision == SNU_FP64 ? 0 : 1;
+  return from_engine(h, h->eng->dist_copy(kind, dir, prec, nrhs, dbuf));
+}
+
+SNU_API snu_status snu_dist_solve(snu_handle* h, int phase, const double* dB,
+                                  double* dX, int nrhs, int ldb) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (!dist_ready(h, 3)) return SNU_ESTATE;
+  if (!dB || !dX || dB == dX) return fail(h, SNU_EINVAL, "bad device arrays");
+  const int prec = h->opts.precision == SNU_FP64 ? 0 : 1;
+  return from_engine(h, h->eng->dist_solve(phase, dB, dX, nrhs, ldb, prec));
+}
+
+SNU_API snu_status snu_residual_device(snu_handle* h, const double* dB,
+                                       const double* dX, double* dR, int nrhs,
+                                       int ldb, double* berr) {
+  if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
+  if (h->state < 2) return fail(h, SNU_ESTATE, "residual before construct");
+  if (!dB || !dX || !dR || !berr) return fail(h, SNU_EINVAL, "null argument");
+  return from_engine(h, h->eng->residual(dB, dX, dR, nrhs, ldb, berr));
 }
 
 SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st) {
@@ -690,6 +825,8 @@ snu_status finish_construct(snu_handle* h, const double* vals, bool have_plan) {
   eo.ir_tol = h->opts.ir_tol;
   eo.ir_max_iter = h->opts.ir_max_iter;
   eo.mem_budget = h->opts.mem_budget;
+  eo.dist_rank = h->dist_rank;
+  eo.dist_world = h->dist_world;
   h->eng = snu::make_engine(eo, err);
   if (!h->eng) return fail(h, SNU_ECUDA, "CUDA engine unavailable: " + err);
   int rc = h->eng->set_stream(h->stream);

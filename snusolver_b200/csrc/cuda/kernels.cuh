@@ -306,6 +306,16 @@ __global__ void k_axpy_cols(int n, int nrhs, const double* __restrict__ D,
   X[i + (int64_t)r * ldx] += D[i + (int64_t)r * ldd];
 }
 
+// X[i, r] = 0 for the rows not kept (keep[i] == 0): a distributed solve's
+// rows that another rank owns, before the sum of X over the ranks.
+__global__ void k_zero_rows(int n, int nrhs, double* __restrict__ X, int ldx,
+                            const unsigned char* __restrict__ keep) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n * nrhs) return;
+  int i = (int)(e % n), r = (int)(e / n);
+  if (!keep[i]) X[i + (int64_t)r * ldx] = 0.0;
+}
+
 // Column copy with leading dimensions (Y = X).
 __global__ void k_copy_cols(int n, int nrhs, const double* __restrict__ X,
                             int ldx, double* __restrict__ Y, int ldy) {

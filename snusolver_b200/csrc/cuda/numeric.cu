@@ -22,6 +22,7 @@
 #include "sweep.cuh"
 #include "gemm_tc.cuh"
 #include "block_inv.cuh"
+#include "sweep_fused.cuh"
 
 namespace snu {
 
@@ -155,9 +156,9 @@ struct LevelSched {
   std::vector<int> nea;
   EaTask* ea_kids = nullptr;  // (child, first of 256 Q rows) of the level's
   int nea_kids = 0;           // fronts' children (solve extend-add)
-  int* list = nullptr;  // fronts of the level
-  int* listq = nullptr; // fronts of the level with q > 0
-  int nlistq = 0;
+  int* list = nullptr;  // fronts of the level (of the schedule's set)
+  int* listq = nullptr; // those with q > 0
+  int nlist = 0, nlistq = 0;
   std::vector<Step> steps;
   GemmBatch f22;
   std::vector<double> ea_elems;  // per child rank: update entries added
@@ -235,7 +236,8 @@ class CudaEngine : public Engine {
       const char* vb = getenv("SNU_VERBOSE");
       verbose_ = vb && vb[0] == '1';
       const char* pbk = getenv("SNU_PANEL_BLOCK");
-      use_block_ = !(pbk && pbk[0] == '0');
+      // (the distributed schedules have the fused panel path only)
+      use_block_ = !(pbk && pbk[0] == '0') || opt_.dist_world > 1;
       // SNU_TC_PANEL=N: FP32 panel products on the tensor cores for levels
       // with at least N fronts (0: never)
       const char* tcp = getenv("SNU_TC_PANEL");
@@ -249,6 +251,18 @@ class CudaEngine : public Engine {
           (rc2 = sweep_attr<float, 2>()) || (rc2 = sweep_attr<float, 4>()) ||
           (rc2 = sweep_attr<float, 8>()) || (rc2 = sweep_attr<float, 16>()))
         return rc2;
+      if ((rc2 = fused_attr<double, 1>()) || (rc2 = fused_attr<double, 2>()) ||
+          (rc2 = fused_attr<double, 4>()) || (rc2 = fused_attr<double, 8>()) ||
+          (rc2 = fused_attr<double, 16>()) || (rc2 = fused_attr<float, 1>()) ||
+          (rc2 = fused_attr<float, 2>()) || (rc2 = fused_attr<float, 4>()) ||
+          (rc2 = fused_attr<float, 8>()) || (rc2 = fused_attr<float, 16>()))
+        return rc2;
+      // SNU_SOLVE_FUSED=1: whole-tree sweeps (one launch per direction)
+      // instead of the level-by-level sweeps.  Off by default: on the
+      // 64^3 workload they measured 0.5 ms slower per factor+solve (the
+      // chain through the tree levels, not launches, bounds both)
+      const char* sf = getenv("SNU_SOLVE_FUSED");
+      fused_solve_ = sf && sf[0] == '1';
     }
     {
       int sms = 0;
@@ -345,11 +359,13 @@ class CudaEngine : public Engine {
       if ((rc = upload(d_flag_off_, fo))) return rc;
       // solve sweeps: one flag per tile and direction, then one task
       // counter per level and direction
-      if ((rc = alloc(d_tflags_, (size_t)(2 * ntileflags_ + 2 * nlevels_ + 2))))
-        return rc;
+      // (two sets of counters: a distributed run sweeps two schedules)
+      tflags_size_ = 2 * ntileflags_ + 4 * (int64_t)nlevels_ + 2;
+      if ((rc = alloc(d_tflags_, (size_t)tflags_size_))) return rc;
       // fused panel path: two flags per tile, then one task counter per
       // outer-block launch (a level has no more outer blocks than tiles)
-      if ((rc = alloc(d_fflags_, (size_t)(3 * ntileflags_)))) return rc;
+      // (counters for the outer blocks of up to two schedules' launches)
+      if ((rc = alloc(d_fflags_, (size_t)(4 * ntileflags_)))) return rc;
     }
     if ((rc = upload(d_fr_, frh_))) return rc;
     if ((rc = upload(d_gidx_, fp.gidx))) return rc;
@@ -365,6 +381,7 @@ class CudaEngine : public Engine {
     if ((rc = alloc(d_norms_, 3 * 64))) return rc;
     const double t1 = wall_s();
     if ((rc = build_schedule())) return rc;
+    if ((rc = build_fused_sweeps())) return rc;
     const double t2 = wall_s();
     if ((rc = finalize_tc())) return rc;
     const double t3 = wall_s();
@@ -450,6 +467,25 @@ class CudaEngine : public Engine {
   }
 
   int factorize(int precision, double* seconds) override {
+    if (opt_.dist_world > 1) {
+      err_ = "a distributed handle factors through its two phases";
+      return ENG_ESTATE;
+    }
+    return factor_run(precision, 0, seconds);
+  }
+
+  int dist_factor(int precision, int phase) override {
+    if (opt_.dist_world <= 1 || (phase != 1 && phase != 2)) {
+      err_ = "distributed factorization: not a distributed handle, or a "
+             "phase other than 1 and 2";
+      return ENG_EINVAL;
+    }
+    return factor_run(precision, phase, nullptr);
+  }
+
+  // The factorization (phase 0), or one phase of a distributed one: the
+  // fixed schedule replayed from a CUDA graph captured at its first run.
+  int factor_run(int precision, int phase, double* seconds) {
     CK(cudaSetDevice(opt_.device));
     int rc;
     if (precision == 0) {
@@ -460,22 +496,25 @@ class CudaEngine : public Engine {
       if (!d_F32_ && (rc = alloc(d_F32_, (size_t)(invb_base_ + invb_need_)))) return rc;
       if (!d_I32_ && (rc = alloc(d_I32_, (size_t)invtot_))) return rc;
     }
-    if (precision == 1 && autotune_ && !tuned_ && force_tcp_ < 0) {
+    if (phase == 0 && precision == 1 && autotune_ && !tuned_ && force_tcp_ < 0) {
       if ((rc = autotune())) return rc;
     }
-    CK(cudaMemsetAsync(d_flags_, 0, 4 * sizeof(int), stream_));
-    CK(cudaMemsetAsync(d_flags_ + 5, 0, sizeof(int), stream_));
+    if (phase != 2) {  // (phase 2 adds to phase 1's counts)
+      CK(cudaMemsetAsync(d_flags_, 0, 4 * sizeof(int), stream_));
+      CK(cudaMemsetAsync(d_flags_ + 5, 0, sizeof(int), stream_));
+    }
     CK(cudaEventRecord(ev0_, stream_));
     const int64_t l0 = launches_;
     if (use_graphs_ && !prof_mask_ && stream_) {
       // the schedule is fixed after set-up: captured once per precision and
       // replayed (one launch instead of ~1000)
-      cudaGraphExec_t& ex = factor_graph_[precision ? 1 : 0];
+      cudaGraphExec_t& ex = phase ? dist_graph_[phase - 1][precision ? 1 : 0]
+                                  : factor_graph_[precision ? 1 : 0];
       if (!ex) {
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-        rc = precision == 0 ? run_factor<double>(d_F64_, d_I64_)
-                            : run_factor<float>(d_F32_, d_I32_);
+        rc = precision == 0 ? run_factor<double>(d_F64_, d_I64_, phase)
+                            : run_factor<float>(d_F32_, d_I32_, phase);
         cudaError_t ce = cudaStreamEndCapture(stream_, &g);
         if (rc) {
           if (g) cudaGraphDestroy(g);
@@ -491,12 +530,12 @@ class CudaEngine : public Engine {
           return ENG_ECUDA;
         }
       }
-      if (launches_ > l0) graph_launches_[precision ? 1 : 0] = launches_ - l0;
+      if (launches_ > l0 && !phase) graph_launches_[precision ? 1 : 0] = launches_ - l0;
       CK(cudaGraphLaunch(ex, stream_));
-      last_factor_launches_ = graph_launches_[precision ? 1 : 0];
+      last_factor_launches_ = phase ? launches_ - l0 : graph_launches_[precision ? 1 : 0];
     } else {
-      rc = precision == 0 ? run_factor<double>(d_F64_, d_I64_)
-                          : run_factor<float>(d_F32_, d_I32_);
+      rc = precision == 0 ? run_factor<double>(d_F64_, d_I64_, phase)
+                          : run_factor<float>(d_F32_, d_I32_, phase);
       if (rc) return rc;
       last_factor_launches_ = launches_ - l0;
     }
@@ -510,10 +549,12 @@ class CudaEngine : public Engine {
     CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
     if (seconds) *seconds = ms * 1e-3;
     tiny_ = flags[0];
-    if (precision == 0)
-      have64_ = true;
-    else
-      have32_ = true;
+    if (phase != 1) {  // (a distributed factorization is done after phase 2)
+      if (precision == 0)
+        have64_ = true;
+      else
+        have32_ = true;
+    }
     if (flags[2]) {
       err_ = "tensor-core GEMM pipeline wait timed out";
       return ENG_ETIMEOUT;
@@ -532,6 +573,10 @@ class CudaEngine : public Engine {
   int solve(const double* dB, double* dX, int nrhs, int ldb, void* stream,
             int precision, SolveReport* rep) override {
     CK(cudaSetDevice(opt_.device));
+    if (opt_.dist_world > 1) {
+      err_ = "a distributed handle solves through its two phases";
+      return ENG_ESTATE;
+    }
     if (nrhs <= 0 || ldb < n_) {
       err_ = "bad nrhs or ldb";
       return ENG_EINVAL;
@@ -568,6 +613,130 @@ class CudaEngine : public Engine {
     CK(cudaEventElapsedTime(&ms, sev0_, sev1_));
     r.seconds = ms * 1e-3;
     if (rep) *rep = r;
+    return ENG_OK;
+  }
+
+  int64_t dist_elems(int kind, int nrhs) const override {
+    return kind == 0 ? shared_front_elems_ : shared_w_per_rhs_ * nrhs;
+  }
+
+  int dist_copy(int kind, int dir, int precision, int nrhs, void* buf) override {
+    CK(cudaSetDevice(opt_.device));
+    if (opt_.dist_world <= 1) {
+      err_ = "not a distributed handle";
+      return ENG_EINVAL;
+    }
+    const size_t es = precision == 0 ? sizeof(double) : sizeof(float);
+    unsigned char* base =
+        kind == 0 ? (unsigned char*)(precision == 0 ? (void*)d_F64_ : (void*)d_F32_)
+                  : (unsigned char*)(precision == 0 ? (void*)d_W64_ : (void*)d_W32_);
+    if (!base || (kind == 1 && nrhs != dist_nrhs_)) {
+      err_ = kind == 0 ? "no factors of this precision"
+                       : "no distributed solve of these columns in progress";
+      return ENG_ESTATE;
+    }
+    unsigned char* b = (unsigned char*)buf;
+    int64_t at = 0;
+    for (int f : shared_) {
+      const FrontInfo& fi = fp_->fronts[f];
+      const int64_t off = kind == 0 ? fi.offset : frh_[f].w_off * nrhs;
+      const int64_t len = kind == 0 ? (int64_t)fi.ld * (fi.p + fi.q)
+                                    : (int64_t)(fi.p + fi.q) * nrhs;
+      if (len == 0) continue;
+      unsigned char* dev = base + off * es;
+      if (dir == 0)
+        CK(cudaMemcpyAsync(b + at * es, dev, len * es, cudaMemcpyDeviceToDevice,
+                           stream_));
+      else
+        CK(cudaMemcpyAsync(dev, b + at * es, len * es, cudaMemcpyDeviceToDevice,
+                           stream_));
+      at += len;
+    }
+    CK(cudaStreamSynchronize(stream_));
+    return ENG_OK;
+  }
+
+  int dist_solve(int phase, const double* dB, double* dX, int nrhs, int ldb,
+                 int precision) override {
+    CK(cudaSetDevice(opt_.device));
+    if (opt_.dist_world <= 1 || (phase != 1 && phase != 2) || nrhs < 1 ||
+        nrhs > RG || ldb < n_) {
+      err_ = "distributed solve: not a distributed handle, a phase other "
+             "than 1 and 2, or nrhs outside 1..16";
+      return ENG_EINVAL;
+    }
+    if ((precision == 0 && !have64_) || (precision == 1 && !have32_)) {
+      err_ = "solve before factorize";
+      return ENG_ESTATE;
+    }
+    if (phase == 2 && nrhs != dist_nrhs_) {
+      err_ = "distributed solve phase 2 without its phase 1";
+      return ENG_ESTATE;
+    }
+    int rc;
+    if ((rc = ensure_solve(nrhs, precision == 0))) return rc;
+    return precision == 0
+               ? dist_solve_t<double>(phase, d_F64_, d_I64_, d_W64_, d_Y64_, dB,
+                                      dX, nrhs, ldb)
+               : dist_solve_t<float>(phase, d_F32_, d_I32_, d_W32_, d_Y32_, dB,
+                                     dX, nrhs, ldb);
+  }
+
+  template <typename T>
+  int dist_solve_t(int phase, const T* F, const T* I, T* W, T* Y,
+                   const double* dB, double* dX, int nrhs, int ldb) {
+    cudaStream_t st = stream_;
+    int rc;
+    if (phase == 1) {
+      CK(cudaMemsetAsync(d_tflags_, 0, sizeof(int) * tflags_size_, st));
+      CK(cudaMemsetAsync(d_flags_ + 4, 0, sizeof(int), st));
+      // every work vector zero; the shared fronts' pivot rows start from B
+      // on rank 0 only, so the sum over the ranks holds B once
+      CK(cudaMemsetAsync(W, 0, sizeof(T) * wtot_ * nrhs, st));
+      if (opt_.dist_rank == 0 && nslist_) {
+        k_solve_init<T><<<SOLVE_SPLIT * nslist_, 256, 0, st>>>(
+            d_slist_, d_fr_, d_gidx_, dB, ldb, nrhs, W);
+        CKL();
+      }
+      if ((rc = sweep_levels<T>(lv1_, 0, true, true, F, I, W, Y, dB, ldb, dX,
+                                ldb, nrhs, st)))
+        return rc;
+      dist_nrhs_ = nrhs;
+    } else {
+      const int c2 = 2 * nlevels_;  // the shared schedule's task counters
+      if ((rc = sweep_levels<T>(lv2_, c2, true, false, F, I, W, Y, dB, ldb,
+                                dX, ldb, nrhs, st)) ||
+          (rc = sweep_levels<T>(lv2_, c2, false, false, F, I, W, Y, dB, ldb,
+                                dX, ldb, nrhs, st)) ||
+          (rc = sweep_levels<T>(lv1_, 0, false, false, F, I, W, Y, dB, ldb, dX,
+                                ldb, nrhs, st)))
+        return rc;
+      const int64_t tot = (int64_t)n_ * nrhs;
+      k_zero_rows<<<(int)((tot + 255) / 256), 256, 0, st>>>(n_, nrhs, dX, ldb,
+                                                             d_xkeep_);
+      CKL();
+      dist_nrhs_ = 0;
+    }
+    return sweep_status(st);
+  }
+
+  int residual(const double* dB, const double* dX, double* dR, int nrhs,
+               int ldb, double* berr) override {
+    CK(cudaSetDevice(opt_.device));
+    if (nrhs < 1 || ldb < n_) {
+      err_ = "bad nrhs or ldb";
+      return ENG_EINVAL;
+    }
+    cudaStream_t st = stream_;
+    int rc;
+    std::vector<double> bn, rn, xn;
+    if ((rc = colmax(dB, ldb, nrhs, st, bn))) return rc;
+    k_residual<<<(n_ + 255) / 256, 256, 0, st>>>(n_, d_rowptr_, d_colidx_,
+                                                 d_vals_, dB, ldb, dX, ldb,
+                                                 nrhs, dR, ldb);
+    CKL();
+    if ((rc = colmax(dR, ldb, nrhs, st, rn, dX, ldb, &xn))) return rc;
+    *berr = backward_error(rn, xn, bn);
     return ENG_OK;
   }
 
@@ -806,14 +975,70 @@ class CudaEngine : public Engine {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int* fl = d_tflags_ + (fwd ? 0 : ntileflags_);
-    int* ctr = d_tflags_ + 2 * ntileflags_ + 2 * std::max(cur_level_, 0) +
-               (fwd ? 0 : 1);
+    int* ctr = d_tflags_ + 2 * ntileflags_ + ctr_off_ +
+               2 * std::max(cur_level_, 0) + (fwd ? 0 : 1);
     ++launches_;
     CK(cudaLaunchKernelEx(&cfg, k, tasks, ntasks, (const FrontDev*)d_fr_, F, I,
                           (const int64_t*)d_flag_off_, nrhs, W, Y, fl, ctr,
                           d_flags_ + 4));
     return ENG_OK;
   }
+  template <typename T, int R>
+  int fused_attr() {
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
+    for (auto k : {k_sweep_fused<T, R, true>, k_sweep_fused<T, R, false>}) {
+      CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)fused_smem<T>()));
+      int nb = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, DIAG_ROWS,
+                                                       fused_smem<T>()));
+      if (nb < 1) {
+        err_ = "fused sweep kernel does not fit on an SM";
+        return ENG_ECUDA;
+      }
+      coop_cap_[(const void*)k] = nb * sms;
+    }
+    return ENG_OK;
+  }
+  // One cooperative launch of a whole-tree sweep (see sweep_fused.cuh).
+  template <typename T, int R>
+  int fused_launch_r(bool fwd, const T* F, const T* I, int nrhs, T* Z, T* Y,
+                     double* X, int ldx, cudaStream_t st) {
+    auto k = fwd ? k_sweep_fused<T, R, true> : k_sweep_fused<T, R, false>;
+    const int ntasks = fwd ? nfwd_ : nbwd_;
+    if (ntasks == 0) return ENG_OK;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(std::min(ntasks, coop_cap_[(const void*)k]));
+    cfg.blockDim = dim3(DIAG_ROWS);
+    cfg.dynamicSmemBytes = fused_smem<T>();
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int* flags = d_sctl_ + (fwd ? 0 : ntileflags_);
+    int* ctr = d_sctl_ + 2 * ntileflags_;
+    int* next = ctr + 3 * (int64_t)nfronts_ + (fwd ? 0 : 1);
+    ++launches_;
+    CK(cudaLaunchKernelEx(&cfg, k, (const SolveTask*)(fwd ? d_fwd_tasks_ : d_bwd_tasks_),
+                          ntasks, (const FrontDev*)d_fr_, (const SweepDep*)d_dep_,
+                          (const int*)d_gidx_, F, I, (const int64_t*)d_flag_off_,
+                          nfronts_, nrhs, n_, Z, Y, X, ldx, flags, ctr, next,
+                          d_flags_ + 4));
+    return ENG_OK;
+  }
+  template <typename T>
+  int fused_launch(bool fwd, const T* F, const T* I, int nrhs, T* Z, T* Y,
+                   double* X, int ldx, cudaStream_t st) {
+    if (nrhs <= 1) return fused_launch_r<T, 1>(fwd, F, I, nrhs, Z, Y, X, ldx, st);
+    if (nrhs <= 2) return fused_launch_r<T, 2>(fwd, F, I, nrhs, Z, Y, X, ldx, st);
+    if (nrhs <= 4) return fused_launch_r<T, 4>(fwd, F, I, nrhs, Z, Y, X, ldx, st);
+    if (nrhs <= 8) return fused_launch_r<T, 8>(fwd, F, I, nrhs, Z, Y, X, ldx, st);
+    return fused_launch_r<T, 16>(fwd, F, I, nrhs, Z, Y, X, ldx, st);
+  }
+
   template <typename T>
   int diag_sweep(bool fwd, const SweepTask* tasks, int ntasks, const T* F,
                  const T* I, int nrhs, T* W, T* Y, cudaStream_t st) {
@@ -929,6 +1154,12 @@ class CudaEngine : public Engine {
         cudaGraphExecDestroy(ex);
         ex = nullptr;
       }
+    for (auto& row : dist_graph_)
+      for (auto& ex : row)
+        if (ex) {
+          cudaGraphExecDestroy(ex);
+          ex = nullptr;
+        }
     for (void* p : ptrs_) cudaFree(p);
     ptrs_.clear();
     sizes_.clear();
@@ -1170,17 +1401,104 @@ class CudaEngine : public Engine {
     return gemm_batch(pg, O.panel);
   }
 
-  int build_schedule() {
+  // Rank whose subtree holds heap block b, -1 for the shared top blocks
+  // (b < dist_world): rank d owns the subtree of heap node 2W - 1 - d, so
+  // with one rank per leaf it owns the leaf of the reference's rank d
+  // (SnuMat.cu:24-30, leaf 2np - 1 - rank).
+  int dist_owner(int b) const {
+    const int W = opt_.dist_world;
+    if (b < W) return -1;
+    while (b >= 2 * W) b /= 2;
+    return 2 * W - 1 - b;
+  }
+
+  // Distributed set-up: this rank's assembly entries (its fronts, and on
+  // rank 0 the shared fronts, so the sum over ranks assembles each value
+  // once), the shared fronts' exchange segments, the shared fronts with
+  // pivots (their work vectors start from B on rank 0), and which rows of
+  // X this rank keeps.
+  int dist_setup(const std::vector<char>& own, const std::vector<char>& shared) {
     const FrontPlan& fp = *fp_;
+    int rc;
+    // front of every assembly entry: fronts are laid out in arena order
+    std::vector<int64_t> starts(nfronts_);
+    for (int f = 0; f < nfronts_; f++) starts[f] = fp.fronts[f].offset;
+    std::vector<int> byoff(nfronts_);
+    for (int f = 0; f < nfronts_; f++) byoff[f] = f;
+    std::sort(byoff.begin(), byoff.end(),
+              [&](int a, int b) { return starts[a] < starts[b]; });
+    std::vector<int64_t> sorted(nfronts_);
+    for (int k = 0; k < nfronts_; k++) sorted[k] = starts[byoff[k]];
+    std::vector<int64_t> pos;
+    std::vector<int> val;
+    const bool root = opt_.dist_rank == 0;
+    for (size_t k = 0; k < fp.asm_pos.size(); k++) {
+      const int64_t a = fp.asm_pos[k];
+      const int idx = (int)(std::upper_bound(sorted.begin(), sorted.end(), a) -
+                            sorted.begin()) - 1;
+      const int f = byoff[std::max(idx, 0)];
+      if (own[f] || (shared[f] && root)) {
+        pos.push_back(a);
+        val.push_back(fp.asm_val[k]);
+      }
+    }
+    na1_ = (int64_t)pos.size();
+    if ((rc = upload(d_asm1_pos_, pos)) || (rc = upload(d_asm1_val_, val)))
+      return rc;
+    shared_.clear();
+    std::vector<int> slist;
+    std::vector<unsigned char> keep(n_, 0);
+    shared_front_elems_ = shared_w_per_rhs_ = 0;
+    for (int f = 0; f < nfronts_; f++) {
+      const FrontInfo& fi = fp.fronts[f];
+      if (shared[f]) {
+        shared_.push_back(f);
+        shared_front_elems_ += (int64_t)fi.ld * (fi.p + fi.q);
+        shared_w_per_rhs_ += fi.p + fi.q;
+        if (fi.p > 0) slist.push_back(f);
+      }
+      // rows this rank's solution is final for: its fronts' pivots, and
+      // on rank 0 the shared pivots
+      if (own[f] || (shared[f] && root))
+        for (int t = 0; t < fi.p; t++) keep[fp.gidx[fi.idx_offset + t]] = 1;
+    }
+    nslist_ = (int)slist.size();
+    if ((rc = upload(d_slist_, slist))) return rc;
+    return upload(d_xkeep_, keep);
+  }
+
+  int build_schedule() {
     // the outer blocks' triangle inverses follow the fronts (FP32)
     invb_base_ = (arena_ + 63) / 64 * 64;
     invb_need_ = 0;
-    lv_.assign(nlevels_, LevelSched());
+    obc_ = 0;
+    if (opt_.dist_world <= 1) return build_levels(lv_, nullptr);
+    // separator-tree distribution: this rank's subtree fronts (phase 1)
+    // and the shared top fronts (phase 2, every rank)
+    std::vector<char> own(nfronts_, 0), shared(nfronts_, 0);
+    for (int f = 0; f < nfronts_; f++) {
+      const int r = dist_owner(fp_->fronts[f].block);
+      if (r < 0) shared[f] = 1;
+      else own[f] = r == opt_.dist_rank;
+    }
+    int rc;
+    if ((rc = build_levels(lv1_, &own)) || (rc = build_levels(lv2_, &shared)))
+      return rc;
+    return dist_setup(own, shared);
+  }
+
+  // The level schedules of the fronts selected by `in` (all when null).
+  // Extend-add work is child-driven: a selected child's update goes to its
+  // parent whether or not the parent is selected.
+  int build_levels(std::vector<LevelSched>& lvs, const std::vector<char>* in) {
+    const FrontPlan& fp = *fp_;
+    auto inset = [&](int f) { return in == nullptr || (*in)[f] != 0; };
+    lvs.assign(nlevels_, LevelSched());
     int mc = fp.max_children;
     int rc;
-    int obc = 0;  // outer-block launches so far (task counters)
+    int& obc = obc_;  // outer-block launches so far (task counters)
     for (int l = 0; l < nlevels_; l++) {
-      LevelSched& L = lv_[l];
+      LevelSched& L = lvs[l];
       L.f0 = fp.level_start[l];
       L.f1 = fp.level_start[l + 1];
       if (L.f1 > L.f0) {
@@ -1193,9 +1511,11 @@ class CudaEngine : public Engine {
       L.asm1 = fp.asm_level[l + 1];
       std::vector<int> list, listq;
       for (int f = L.f0; f < L.f1; f++) {
+        if (!inset(f)) continue;
         list.push_back(f);
         if (fp.fronts[f].q > 0) listq.push_back(f);
       }
+      L.nlist = (int)list.size();
       if ((rc = upload(L.list, list))) return rc;
       L.nlistq = (int)listq.size();
       if ((rc = upload(L.listq, listq))) return rc;
@@ -1203,13 +1523,14 @@ class CudaEngine : public Engine {
       L.nea.assign(mc, 0);
       L.ea_elems.assign(mc, 0.0);
       for (int f = L.f0; f < L.f1; f++)
-        L.solve_elems += fp.fronts[f].p + fp.fronts[f].q;
+        if (inset(f)) L.solve_elems += fp.fronts[f].p + fp.fronts[f].q;
       std::vector<EaTask> kids;
       for (int r = 0; r < mc; r++) {
         int b0 = fp.ea_ptr[(size_t)l * mc + r], b1 = fp.ea_ptr[(size_t)l * mc + r + 1];
         std::vector<EaTask> tasks;
         for (int k = b0; k < b1; k++) {
           int c = fp.ea_child[k];
+          if (!inset(c)) continue;
           for (int i0 = 0; i0 < fp.fronts[c].q; i0 += 256) kids.push_back({c, i0});
           for (int j = 0; j < fp.fronts[c].q; j++) tasks.push_back({c, j});
           L.ea_elems[r] += (double)fp.fronts[c].q * fp.fronts[c].q;
@@ -1220,8 +1541,10 @@ class CudaEngine : public Engine {
       L.nea_kids = (int)kids.size();
       if (!kids.empty() && (rc = upload(L.ea_kids, kids))) return rc;
       int maxp = 0;
-      for (int f = L.f0; f < L.f1; f++) maxp = std::max(maxp, fp.fronts[f].p);
-      int nsteps = (maxp + NB - 1) / NB;
+      for (int f = L.f0; f < L.f1; f++)
+        if (inset(f)) maxp = std::max(maxp, fp.fronts[f].p);
+      // (the per-step panel path serves one-GPU runs only)
+      int nsteps = in ? 0 : (maxp + NB - 1) / NB;
       L.steps.assign(nsteps, Step());
       for (int s = 0; s < nsteps; s++) {
         Step& S = L.steps[s];
@@ -1283,7 +1606,7 @@ class CudaEngine : public Engine {
       for (int f = L.f0; f < L.f1; f++) {
         const FrontInfo& fi = fp.fronts[f];
         // (a front without pivots passes its update matrix on: k = 0)
-        if (fi.q == 0) continue;
+        if (fi.q == 0 || !inset(f)) continue;
         int64_t o = fi.offset, ld = fi.ld;
         GemmProb g{fi.q, fi.q, fi.p, fi.ld, fi.ld, fi.ld, o + fi.p,
                    o + fi.p * ld, o + fi.p + fi.p * ld};
@@ -1307,17 +1630,18 @@ class CudaEngine : public Engine {
         int maxrows = 0;
         for (int f = L.f0; f < L.f1; f++) {
           const FrontInfo& fi = fp.fronts[f];
-          if (fi.p > O.K0)
+          if (fi.p > O.K0 && inset(f))
             maxrows = std::max(maxrows, (fi.p + fi.q - O.K0 + NB - 1) / NB);
         }
         for (int r = 0; r < maxrows; r++)
           for (int f = L.f0; f < L.f1; f++) {
             const FrontInfo& fi = fp.fronts[f];
-            if (fi.p > O.K0 && O.K0 + r * NB < fi.p + fi.q) bt.push_back({f, 0, r});
+            if (inset(f) && fi.p > O.K0 && O.K0 + r * NB < fi.p + fi.q)
+              bt.push_back({f, 0, r});
           }
         for (int f = L.f0; f < L.f1; f++) {
           const FrontInfo& fi = fp.fronts[f];
-          if (fi.p <= O.K0) continue;
+          if (fi.p <= O.K0 || !inset(f)) continue;
           const int K0 = O.K0, K1 = std::min(K0 + OB, fi.p), dim = fi.p + fi.q;
           for (int c = 0; K1 + c * NB < dim; c++) bt.push_back({f, 1, c});
           const int64_t o = fi.offset, ld = fi.ld;
@@ -1338,7 +1662,7 @@ class CudaEngine : public Engine {
         O.ntasks = (int)bt.size();
         if (!bt.empty() && (rc = upload(O.tasks, bt))) return rc;
         if ((rc = gemm_batch(og, O.outer))) return rc;
-        if (use_tc_ && tcpanel_min_ > 0 && L.f1 - L.f0 >= tcpanel_min_ &&
+        if (!in && use_tc_ && tcpanel_min_ > 0 && L.f1 - L.f0 >= tcpanel_min_ &&
             (rc = tc_panel_schedule(L, O, maxrows)))
           return rc;
       }
@@ -1362,7 +1686,7 @@ class CudaEngine : public Engine {
       // solve sweeps; fronts with the longest tile chains first
       std::vector<int> byp;
       for (int f = L.f0; f < L.f1; f++)
-        if (fp.fronts[f].p > 0) byp.push_back(f);
+        if (fp.fronts[f].p > 0 && inset(f)) byp.push_back(f);
       std::stable_sort(byp.begin(), byp.end(), [&](int x, int y) {
         return fp.fronts[x].p > fp.fronts[y].p;
       });
@@ -1498,27 +1822,31 @@ class CudaEngine : public Engine {
   }
 
   template <typename T>
-  int run_factor(T* F, T* I) {
+  // phase 0: the whole factorization (one GPU); 1 / 2: a distributed
+  // run's subtree / shared phase (see Engine::dist_factor)
+  int run_factor(T* F, T* I, int phase = 0) {
     cudaStream_t st = stream_;
     const double es = sizeof(T);
     int rc;
     // every front zeroed and assembled first: children's Schur updates add
     // into their parents directly (extend-add fused into the Schur GEMM)
-    {
-      const int64_t na = fp_->asm_level[nlevels_];
+    if (phase != 2) {
+      const int64_t na = phase == 1 ? na1_ : fp_->asm_level[nlevels_];
+      const int64_t* apos = phase == 1 ? d_asm1_pos_ : d_asm_pos_;
+      const int* aval = phase == 1 ? d_asm1_val_ : d_asm_val_;
       int pi = prof_begin(KF_ASSEMBLE, st);
       CK(cudaMemsetAsync(F, 0, sizeof(T) * arena_, st));
-      CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 3 * ntileflags_, st));
+      CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 4 * ntileflags_, st));
       if (na > 0) {
         int blocks = (int)std::min<int64_t>((na + 255) / 256, 148 * 16);
-        k_assemble<T><<<blocks, 256, 0, st>>>(d_asm_pos_, d_asm_val_, d_vals_,
-                                              F, na);
+        k_assemble<T><<<blocks, 256, 0, st>>>(apos, aval, d_vals_, F, na);
         CKL();
       }
       prof_end(pi, KF_ASSEMBLE, st, 0, es * arena_ + (20.0 + es) * na);
     }
+    std::vector<LevelSched>& lvs = phase == 1 ? lv1_ : phase == 2 ? lv2_ : lv_;
     for (int l = 0; l < nlevels_; l++) {
-      LevelSched& L = lv_[l];
+      LevelSched& L = lvs[l];
       cur_level_ = l;
       int pi;
       if (use_block_) {
@@ -1579,88 +1907,205 @@ class CudaEngine : public Engine {
   int tree_solve_cols(const T* F, const T* I, T* W, T* Y, const double* B,
                       int ldb, double* X, int ldx, int nrhs, cudaStream_t st) {
     for (int c0 = 0; c0 < nrhs; c0 += RG) {
-      int rc = tree_solve<T>(F, I, W, Y, B + (size_t)c0 * ldb, ldb,
-                             X + (size_t)c0 * ldx, ldx,
-                             std::min(RG, nrhs - c0), st);
+      const int nc = std::min(RG, nrhs - c0);
+      int rc = fused_solve_
+                   ? tree_solve_fused<T>(F, I, W, Y, B + (size_t)c0 * ldb, ldb,
+                                         X + (size_t)c0 * ldx, ldx, nc, st)
+                   : tree_solve<T>(F, I, W, Y, B + (size_t)c0 * ldb, ldb,
+                                   X + (size_t)c0 * ldx, ldx, nc, st);
       if (rc) return rc;
     }
     return ENG_OK;
   }
 
+  // The solve of up to RG columns as two whole-tree sweeps (forward,
+  // backward; see sweep_fused.cuh).  W serves as Z (n x nrhs: the work
+  // vectors hold at least n entries per column).
+  template <typename T>
+  int tree_solve_fused(const T* F, const T* I, T* W, T* Y, const double* B,
+                       int ldb, double* X, int ldx, int nrhs, cudaStream_t st) {
+    const double es = sizeof(T);
+    if (nrhs < 1 || nrhs > RG) {
+      err_ = "tree solve of more than 16 columns at once";
+      return ENG_EINVAL;
+    }
+    cur_level_ = -1;
+    int pi = prof_begin(KF_SWEEP, st);
+    CK(cudaMemsetAsync(d_sctl_, 0, sizeof(int) * sctl_size_, st));
+    const int64_t tot = (int64_t)n_ * nrhs;
+    k_sweep_init<T><<<(int)((tot + 255) / 256), 256, 0, st>>>(n_, nrhs, B, ldb, W);
+    CKL();
+    int rc;
+    if ((rc = fused_launch<T>(true, F, I, nrhs, W, Y, nullptr, ldx, st))) return rc;
+    prof_end(pi, KF_SWEEP, st, 2.0 * sweep_elems_ * nrhs,
+             sweep_elems_ * es + (es + 8.0) * tot);
+    pi = prof_begin(KF_SWEEP, st);
+    if ((rc = fused_launch<T>(false, F, I, nrhs, W, Y, X, ldx, st))) return rc;
+    prof_end(pi, KF_SWEEP, st, 2.0 * sweep_elems_ * nrhs,
+             sweep_elems_ * es + 8.0 * tot);
+    return ENG_OK;
+  }
+
+  // Task lists and dependency data of the whole-tree sweeps (the levels'
+  // fronts in the order of the level sweeps: longest pivot chains first).
+  int build_fused_sweeps() {
+    const FrontPlan& fp = *fp_;
+    const int nf = nfronts_;
+    std::vector<SweepDep> dep(nf);
+    std::vector<int> ngl(nf, 0);
+    sweep_elems_ = 0;
+    for (int f = 0; f < nf; f++) {
+      const FrontInfo& fi = fp.fronts[f];
+      int a = fi.parent;
+      while (a >= 0 && fp.fronts[a].p == 0) a = fp.fronts[a].parent;
+      dep[f].effpar = a;
+      dep[f].need = 0;
+      dep[f].nch = (fi.p + DIAG_ROWS - 1) / DIAG_ROWS;
+      const bool off = fi.p > 0 && fi.q > 0;
+      ngl[f] = off ? ((fi.q + GEMV_ROWS - 1) / GEMV_ROWS) * ((fi.p + GEMV_K - 1) / GEMV_K) : 0;
+      dep[f].ngq = off ? ((fi.p + GEMV_ROWS - 1) / GEMV_ROWS) * ((fi.q + GEMV_K - 1) / GEMV_K) : 0;
+      sweep_elems_ += 0.5 * fi.p * (fi.p + 1.0) + (double)fi.p * fi.q;
+    }
+    for (int f = 0; f < nf; f++)
+      if (fp.fronts[f].p > 0 && dep[f].effpar >= 0) dep[dep[f].effpar].need += ngl[f];
+    std::vector<SolveTask> fw, bw;
+    std::vector<std::vector<int>> byp(nlevels_);
+    for (int l = 0; l < nlevels_; l++) {
+      for (int f = fp.level_start[l]; f < fp.level_start[l + 1]; f++)
+        if (fp.fronts[f].p > 0) byp[l].push_back(f);
+      std::stable_sort(byp[l].begin(), byp[l].end(), [&](int x, int y) {
+        return fp.fronts[x].p > fp.fronts[y].p;
+      });
+    }
+    for (int l = 0; l < nlevels_; l++) {
+      for (int f : byp[l])
+        for (int c = 0; c < dep[f].nch; c++) fw.push_back({0, f, c, 0});
+      for (int f : byp[l]) {
+        const FrontInfo& fi = fp.fronts[f];
+        if (!ngl[f]) continue;
+        for (int a = 0; a < (fi.q + GEMV_ROWS - 1) / GEMV_ROWS; a++)
+          for (int b = 0; b < (fi.p + GEMV_K - 1) / GEMV_K; b++)
+            fw.push_back({1, f, a, b});
+      }
+    }
+    for (int l = nlevels_ - 1; l >= 0; l--) {
+      for (int f : byp[l]) {
+        const FrontInfo& fi = fp.fronts[f];
+        if (!dep[f].ngq) continue;
+        for (int a = 0; a < (fi.p + GEMV_ROWS - 1) / GEMV_ROWS; a++)
+          for (int b = 0; b < (fi.q + GEMV_K - 1) / GEMV_K; b++)
+            bw.push_back({1, f, a, b});
+      }
+      for (int f : byp[l])
+        for (int c = dep[f].nch - 1; c >= 0; c--) bw.push_back({0, f, c, 0});
+    }
+    nfwd_ = (int)fw.size();
+    nbwd_ = (int)bw.size();
+    int rc;
+    if ((rc = upload(d_dep_, dep))) return rc;
+    if ((rc = upload(d_fwd_tasks_, fw))) return rc;
+    if ((rc = upload(d_bwd_tasks_, bw))) return rc;
+    sctl_size_ = 2 * ntileflags_ + 3 * (int64_t)nf + 2;
+    return alloc(d_sctl_, (size_t)sctl_size_);
+  }
+
   template <typename T>
   int tree_solve(const T* F, const T* I, T* W, T* Y, const double* B, int ldb,
                  double* X, int ldx, int nrhs, cudaStream_t st) {
-    const double es = sizeof(T);
-    int pi, rc;
     if (nrhs < 1 || nrhs > RG) {  // the kernels hold at most RG columns
       err_ = "tree solve of more than 16 columns at once";
       return ENG_EINVAL;
     }
-    CK(cudaMemsetAsync(d_tflags_, 0,
-                       sizeof(int) * (2 * ntileflags_ + 2 * nlevels_ + 2), st));
-    for (int l = 0; l < nlevels_; l++) {
-      LevelSched& L = lv_[l];
-      cur_level_ = l;
-      int nf = L.f1 - L.f0;
-      if (!nf) continue;
-      pi = prof_begin(KF_SOLVE_MISC, st);
-      k_solve_init<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_, B,
-                                                   ldb, nrhs, W);
-      CKL();
-      if (L.nea_kids) {
-        k_solve_ea<T><<<L.nea_kids, 256, 0, st>>>(L.ea_kids, d_fr_, d_rel_,
-                                                  nrhs, W);
+    CK(cudaMemsetAsync(d_tflags_, 0, sizeof(int) * tflags_size_, st));
+    int rc;
+    if ((rc = sweep_levels<T>(lv_, 0, true, true, F, I, W, Y, B, ldb, X, ldx,
+                              nrhs, st)))
+      return rc;
+    return sweep_levels<T>(lv_, 0, false, false, F, I, W, Y, B, ldb, X, ldx,
+                           nrhs, st);
+  }
+
+  // One direction of the level-by-level sweeps over the fronts of a
+  // schedule (forward from the leaves, backward from the root).  ctr_off
+  // selects the schedule's task counters; init: the forward sweep first
+  // loads B into each level's fronts (off for fronts whose work vectors
+  // were set up and summed across ranks beforehand).
+  template <typename T>
+  int sweep_levels(const std::vector<LevelSched>& lvs, int ctr_off, bool fwd,
+                   bool init, const T* F, const T* I, T* W, T* Y,
+                   const double* B, int ldb, double* X, int ldx, int nrhs,
+                   cudaStream_t st) {
+    const double es = sizeof(T);
+    int pi, rc;
+    ctr_off_ = ctr_off;
+    if (fwd) {
+      for (int l = 0; l < nlevels_; l++) {
+        const LevelSched& L = lvs[l];
+        cur_level_ = l;
+        const int nf = L.nlist;
+        pi = prof_begin(KF_SOLVE_MISC, st);
+        if (init && nf) {
+          k_solve_init<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_,
+                                                       B, ldb, nrhs, W);
+          CKL();
+        }
+        if (L.nea_kids) {
+          k_solve_ea<T><<<L.nea_kids, 256, 0, st>>>(L.ea_kids, d_fr_, d_rel_,
+                                                    nrhs, W);
+          CKL();
+        }
+        prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
+        if (L.nwf) {
+          pi = prof_begin(KF_SOLVE_DIAG, st);
+          if ((rc = diag_sweep<T>(true, L.wf, L.nwf, F, I, nrhs, W, Y, st)))
+            return rc;
+          prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.diag_elems * nrhs,
+                   L.diag_elems * es);
+        }
+        if (L.ngl) {
+          pi = prof_begin(KF_SOLVE_GEMM, st);
+          SNU_RG_DISPATCH(nrhs, k_gemv_l21, T, (L.ngl, 256, 0, st),
+                          (L.gl, d_fr_, F, nrhs, W, Y));
+          CKL();
+          prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
+                   L.gq_elems * es);
+        }
+      }
+    } else {
+      for (int l = nlevels_ - 1; l >= 0; l--) {
+        const LevelSched& L = lvs[l];
+        cur_level_ = l;
+        const int nf = L.nlist;
+        if (!nf) continue;
+        pi = prof_begin(KF_SOLVE_MISC, st);
+        k_bwd_init<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_, X,
+                                                   ldx, nrhs, Y, W);
         CKL();
-      }
-      prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
-      if (L.nwf) {
-        pi = prof_begin(KF_SOLVE_DIAG, st);
-        if ((rc = diag_sweep<T>(true, L.wf, L.nwf, F, I, nrhs, W, Y, st)))
-          return rc;
-        prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.diag_elems * nrhs,
-                 L.diag_elems * es);
-      }
-      if (L.ngl) {
-        pi = prof_begin(KF_SOLVE_GEMM, st);
-        SNU_RG_DISPATCH(nrhs, k_gemv_l21, T, (L.ngl, 256, 0, st),
-                        (L.gl, d_fr_, F, nrhs, W, Y));
+        prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
+        if (L.ngq) {
+          pi = prof_begin(KF_SOLVE_GEMM, st);
+          SNU_RG_DISPATCH(nrhs, k_gemv_u12, T, (L.ngq, 256, 0, st),
+                          (L.gq, d_fr_, F, nrhs, W, Y));
+          CKL();
+          prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
+                   L.gq_elems * es);
+        }
+        if (L.nwb) {
+          pi = prof_begin(KF_SOLVE_DIAG, st);
+          if ((rc = diag_sweep<T>(false, L.wb, L.nwb, F, I, nrhs, W, Y, st)))
+            return rc;
+          prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.diag_elems * nrhs,
+                   L.diag_elems * es);
+        }
+        pi = prof_begin(KF_SOLVE_MISC, st);
+        k_scatter_y<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_, Y,
+                                                    nrhs, X, ldx);
         CKL();
-        prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
-                 L.gq_elems * es);
+        prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
       }
-    }
-    for (int l = nlevels_ - 1; l >= 0; l--) {
-      LevelSched& L = lv_[l];
-      cur_level_ = l;
-      int nf = L.f1 - L.f0;
-      if (!nf) continue;
-      pi = prof_begin(KF_SOLVE_MISC, st);
-      k_bwd_init<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_, X,
-                                                 ldx, nrhs, Y, W);
-      CKL();
-      prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
-      if (L.ngq) {
-        pi = prof_begin(KF_SOLVE_GEMM, st);
-        SNU_RG_DISPATCH(nrhs, k_gemv_u12, T, (L.ngq, 256, 0, st),
-                        (L.gq, d_fr_, F, nrhs, W, Y));
-        CKL();
-        prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
-                 L.gq_elems * es);
-      }
-      if (L.nwb) {
-        pi = prof_begin(KF_SOLVE_DIAG, st);
-        if ((rc = diag_sweep<T>(false, L.wb, L.nwb, F, I, nrhs, W, Y, st)))
-          return rc;
-        prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.diag_elems * nrhs,
-                 L.diag_elems * es);
-      }
-      pi = prof_begin(KF_SOLVE_MISC, st);
-      k_scatter_y<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_, Y,
-                                                  nrhs, X, ldx);
-      CKL();
-      prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
     }
     cur_level_ = -1;
+    ctr_off_ = 0;
     return ENG_OK;
   }
 
@@ -1748,6 +2193,10 @@ class CudaEngine : public Engine {
   int solve_noalloc(const double* dB, double* dX, int nrhs, int ldb,
                     void* stream, int precision, SolveReport* rep) override {
     CK(cudaSetDevice(opt_.device));
+    if (opt_.dist_world > 1) {
+      err_ = "a distributed handle solves through its two phases";
+      return ENG_ESTATE;
+    }
     if (nrhs <= 0 || ldb < n_) {
       err_ = "bad nrhs or ldb";
       return ENG_EINVAL;
@@ -1932,6 +2381,23 @@ class CudaEngine : public Engine {
   // pivot-block sweep flags (forward, then backward) and per-front offsets
   int64_t* d_flag_off_ = nullptr;
   int* d_tflags_ = nullptr;
+  int64_t tflags_size_ = 0;
+  int ctr_off_ = 0;  // sweep task counters of the schedule being swept
+  // separator-tree distribution: the subtree (lv1_) and shared (lv2_)
+  // schedules, this rank's assembly entries, the shared fronts, their
+  // fronts with pivots, the rows of X this rank keeps
+  std::vector<LevelSched> lv1_, lv2_;
+  int64_t* d_asm1_pos_ = nullptr;
+  int* d_asm1_val_ = nullptr;
+  int64_t na1_ = 0;
+  std::vector<int> shared_;
+  int* d_slist_ = nullptr;
+  int nslist_ = 0;
+  unsigned char* d_xkeep_ = nullptr;
+  int64_t shared_front_elems_ = 0, shared_w_per_rhs_ = 0;
+  cudaGraphExec_t dist_graph_[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int dist_nrhs_ = 0;  // columns of the distributed solve in progress
+  int obc_ = 0;      // outer-block launches of the schedules built
   int* d_fflags_ = nullptr;  // diagonal tiles done (fused panel path)
   int64_t ntileflags_ = 0;
   // co-resident grid size of each pivot-block sweep kernel
@@ -1955,6 +2421,15 @@ class CudaEngine : public Engine {
                std::chrono::steady_clock::now().time_since_epoch())
         .count();
   }
+  // whole-tree sweeps instead of the level-by-level sweeps (SNU_SOLVE_FUSED)
+  bool fused_solve_ = false;
+  SolveTask* d_fwd_tasks_ = nullptr;
+  SolveTask* d_bwd_tasks_ = nullptr;
+  int nfwd_ = 0, nbwd_ = 0;
+  SweepDep* d_dep_ = nullptr;
+  int* d_sctl_ = nullptr;  // tile flags (both directions), counters, task counters
+  int64_t sctl_size_ = 0;
+  double sweep_elems_ = 0;  // factor entries one sweep reads (per column)
   int force_tcp_ = -1;  // tensor-core kernel variant forced (-1: per batch)
   int tcp_cap_ = 148;
   // autotuner of the tensor-core kernel variant per GEMM batch
@@ -2043,7 +2518,7 @@ const char* kernel_family_name(int f) {
   static const char* names[KF_COUNT] = {
       "assemble", "extend_add", "diag_lu", "panel_trsm", "gemm_trail",
       "gemm_schur", "solve_diag", "solve_gemm", "solve_misc", "residual",
-      "panel_block", "block_inv", "gemm_panel"};
+      "panel_block", "block_inv", "gemm_panel", "sweep"};
   return (f >= 0 && f < KF_COUNT) ? names[f] : "?";
 }
 

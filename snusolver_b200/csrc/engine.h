@@ -27,6 +27,11 @@ struct EngineOptions {
   double ir_tol = 1e-10;
   int ir_max_iter = 10;
   int64_t mem_budget = 0;
+  // separator-tree distribution over dist_world ranks (1: off): this
+  // engine factors the fronts of its rank's subtree, then (after the
+  // caller has summed the shared fronts over the ranks) the shared top
+  // fronts; see Engine::dist_*
+  int dist_rank = 0, dist_world = 1;
 };
 
 struct SolveReport {
@@ -51,6 +56,7 @@ enum KernelFamily {
   KF_PANEL_BLOCK,    // fused outer-block panels (tiles, L/U blocks, updates)
   KF_BLOCK_INV,      // inverses of an outer block's triangles (FP32)
   KF_GEMM_PANEL,     // L21 = A21 Uinv, U12 = Linv A12 on the tensor cores
+  KF_SWEEP,          // dependency-driven whole-tree sweeps (one per direction)
   KF_COUNT
 };
 const char* kernel_family_name(int f);
@@ -110,6 +116,31 @@ class Engine {
   // instead of memory the handle allocates (snu_solve_device_noalloc).
   virtual int solve_noalloc(const double* dB, double* dX, int nrhs, int ldb,
                             void* stream, int precision, SolveReport* rep) = 0;
+  // ---- separator-tree distribution (dist_world > 1 at construction) ----
+  // Rank of a heap block's subtree, -1 for the shared top blocks.
+  // Phase 1: zero the fronts, assemble this rank's fronts (and, on rank 0,
+  // the shared fronts) and factor this rank's subtree; its updates to the
+  // shared fronts accumulate there.  Phase 2: factor the shared fronts
+  // (every rank; the caller has summed them over the ranks in between).
+  virtual int dist_factor(int precision, int phase) = 0;
+  // Elements (precision T) of the exchange buffer: kind 0 the shared
+  // fronts, kind 1 their solve work vectors for nrhs columns.
+  virtual int64_t dist_elems(int kind, int nrhs) const = 0;
+  // Copies the shared regions into (dir 0) or back from (dir 1) a device
+  // buffer of dist_elems elements, on the engine's stream.
+  virtual int dist_copy(int kind, int dir, int precision, int nrhs,
+                        void* buf) = 0;
+  // Solve of up to 16 columns in two phases around the caller's sum of the
+  // shared work vectors: phase 1 sets up the work vectors and sweeps this
+  // rank's subtree forward; phase 2 sweeps the shared fronts forward and
+  // back, this rank's subtree back, and zeroes the rows of X this rank does
+  // not own (the caller then sums X over the ranks).
+  virtual int dist_solve(int phase, const double* dB, double* dX, int nrhs,
+                         int ldb, int precision) = 0;
+  // R = B - A X on the original matrix (FP64) and the backward error
+  // max over columns of ||R|| / (||A|| ||X|| + ||B||).
+  virtual int residual(const double* dB, const double* dX, double* dR,
+                       int nrhs, int ldb, double* berr) = 0;
   virtual int64_t device_bytes() const = 0;
   virtual int tiny_pivots() const = 0;
   virtual const std::string& error() const = 0;

@@ -27,6 +27,7 @@ struct snu_handle {
   unsigned prof_mask = 0;    // profiling families (applied at construct)
   int autotune = 0;          // tune the GEMM variants at the next factorize
   std::string tune_path;     // cache file of tuned choices ("" = none)
+  int dist_rank = 0, dist_world = 1;  // separator-tree distribution
   int batch = 0;             // matrices of a batch handle (0: one matrix)
   std::vector<int> batch_rows;  // row_start of every matrix (batch + 1)
 };
@@ -37,4 +38,17 @@ namespace snu {
 // have_plan), engine, setup, values.  Used by snu_construct and by the
 // server when it reuses a cached plan.
 snu_status finish_construct(snu_handle* h, const double* vals, bool have_plan);
+
+// Columns of one right-hand-side block: X = A^-1 B for nrhs columns, host
+// arrays with leading dimension ldb.
+struct SolvePiece {
+  const double* B;
+  double* X;
+  int nrhs, ldb;
+};
+// Solves the columns of several blocks as one system of their concatenated
+// columns (in chunks of up to 64 columns, each one device solve with its
+// own refinement): snu_solve for one block, and for the server's merged
+// solve requests.  stats.backward_error is the worst over all columns.
+snu_status solve_pieces(snu_handle* h, const std::vector<SolvePiece>& pieces);
 }  // namespace snu

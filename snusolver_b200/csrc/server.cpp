@@ -15,6 +15,15 @@
 //   fails with SNU_ENOMEM instead of waiting.
 // * Plan cache: host plans keyed by an FNV-1a hash of (n, rowptr, colidx),
 //   checked entry by entry, least recently used dropped past `plan_cache`.
+// * Device plan reuse: a released matrix's handle (device plan, factors,
+//   captured factorization graph) is parked, up to `plan_cache` of them;
+//   a factor request on the same pattern takes a parked handle and only
+//   uploads its values and refactors.  Parked memory counts against the
+//   budget and is the first to be freed when admission needs room.
+// * Merged solves: a worker that takes a solve request also takes the
+//   solve requests queued behind it on the same matrix (up to 64 columns
+//   in all, none past a refactor or release of that matrix) and solves
+//   their columns together, one refinement loop for all of them.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -112,7 +121,19 @@ struct Matrix {
   bool busy = false;
   bool gone = false;  // released or failed to factor
   int n = 0, nnz = 0;
+  uint64_t key = 0;   // pattern hash (for parking the handle at release)
 };
+
+// A released matrix's handle kept for a later factor request on the same
+// pattern (its plan and device arrays are reused; only values change).
+struct Parked {
+  uint64_t key = 0;
+  std::vector<int> rowptr, colidx;  // the pattern, checked on reuse
+  snu_handle* h = nullptr;
+  int64_t bytes = 0;
+};
+
+constexpr int MERGE_COLUMNS = 64;  // columns of one merged solve
 
 }  // namespace
 
@@ -128,6 +149,8 @@ struct snu_server {
   std::map<int64_t, Matrix> mats;
   std::deque<snu_completion> done;
   std::list<std::shared_ptr<const Plan>> plans;  // most recently used first
+  std::list<Parked> parked;                     // most recently parked first
+  int64_t parked_bytes = 0;
   std::vector<std::thread> workers;
   std::string err;
   int64_t next_id = 1, next_mat = 1;
@@ -175,22 +198,67 @@ struct snu_server {
     cv_done.notify_all();
   }
 
-  // Oldest queued request whose matrix is idle (factor requests always are).
-  std::unique_ptr<Request> take() {
+  // Oldest queued request whose matrix is idle (factor requests always
+  // are), and for a solve the solve requests queued behind it on the same
+  // matrix (up to MERGE_COLUMNS columns, none past another request of that
+  // matrix).
+  std::vector<std::unique_ptr<Request>> take() {
+    std::vector<std::unique_ptr<Request>> out;
     for (auto it = queue.begin(); it != queue.end(); ++it) {
       Matrix& m = mats[(*it)->matrix];
       if (m.busy) continue;
       m.busy = true;
-      auto r = std::move(*it);
-      queue.erase(it);
-      return r;
+      const int64_t mid = (*it)->matrix;
+      const bool solve = (*it)->type == SNU_REQ_SOLVE;
+      int cols = (*it)->nrhs;
+      out.push_back(std::move(*it));
+      it = queue.erase(it);
+      if (!solve) return out;
+      while (it != queue.end()) {
+        if ((*it)->matrix != mid) {
+          ++it;
+          continue;
+        }
+        if ((*it)->type != SNU_REQ_SOLVE || cols + (*it)->nrhs > MERGE_COLUMNS)
+          break;
+        cols += (*it)->nrhs;
+        out.push_back(std::move(*it));
+        it = queue.erase(it);
+      }
+      return out;
     }
+    return out;
+  }
+  // Frees parked handles, oldest first, until `need` more bytes fit beside
+  // the resident and admitted ones (or none is left); call with mu held.
+  void unpark_for(int64_t need, std::unique_lock<std::mutex>& lk) {
+    while (!parked.empty() && resident + admitted + need > budget) {
+      Parked p = std::move(parked.back());
+      parked.pop_back();
+      parked_bytes -= p.bytes;
+      resident -= p.bytes;
+      lk.unlock();
+      snu_destroy(p.h);
+      lk.lock();
+    }
+  }
+  // A parked handle of this pattern, removed from the park (mu held).
+  snu_handle* take_parked(uint64_t key, const Request& r, int64_t* bytes) {
+    for (auto it = parked.begin(); it != parked.end(); ++it)
+      if (it->key == key && it->rowptr == r.rowptr && it->colidx == r.colidx) {
+        snu_handle* h = it->h;
+        *bytes = it->bytes;
+        parked_bytes -= it->bytes;
+        parked.erase(it);
+        return h;
+      }
     return nullptr;
   }
 
   void worker_loop(int slot);
   int run_factor(Request& r, cudaStream_t st, double t_start);
-  int run_other(Request& r, Matrix& m, cudaStream_t st, double* be, int* it);
+  int run_other(std::vector<std::unique_ptr<Request>>& batch, Matrix& m,
+                cudaStream_t st, double* be, int* it);
 };
 
 void snu_server::worker_loop(int slot) {
@@ -200,12 +268,14 @@ void snu_server::worker_loop(int slot) {
   cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   std::unique_lock<std::mutex> lk(mu);
   for (;;) {
-    std::unique_ptr<Request> r;
+    std::vector<std::unique_ptr<Request>> batch;
     cv_work.wait(lk, [&] {
-      if ((r = take())) return true;
+      batch = take();
+      if (!batch.empty()) return true;
       return stop && queue.empty();
     });
-    if (!r) break;
+    if (batch.empty()) break;
+    std::unique_ptr<Request>& r = batch[0];
     running++;
     const double t0 = now_s();
     Matrix& m = mats[r->matrix];  // std::map nodes stay put
@@ -220,19 +290,42 @@ void snu_server::worker_loop(int slot) {
     } else if (m.gone || !m.h) {
       status = SNU_ESTATE;
     } else if (r->type == SNU_REQ_RELEASE) {
-      resident -= m.bytes;
-      m.bytes = 0;
       m.gone = true;
       snu_handle* h = m.h;
       m.h = nullptr;
-      lk.unlock();
-      snu_destroy(h);
-      lk.lock();
+      if (o.plan_cache > 0 && m.key) {
+        // parked for a later factor request on the same pattern (its bytes
+        // stay resident until a reuse or unpark_for frees them)
+        Parked p;
+        p.key = m.key;
+        p.rowptr = h->rowptr;
+        p.colidx = h->colidx;
+        p.h = h;
+        p.bytes = m.bytes;
+        parked_bytes += m.bytes;
+        parked.push_front(std::move(p));
+        m.bytes = 0;
+        while ((int)parked.size() > o.plan_cache) {
+          Parked q = std::move(parked.back());
+          parked.pop_back();
+          parked_bytes -= q.bytes;
+          resident -= q.bytes;
+          lk.unlock();
+          snu_destroy(q.h);
+          lk.lock();
+        }
+      } else {
+        resident -= m.bytes;
+        m.bytes = 0;
+        lk.unlock();
+        snu_destroy(h);
+        lk.lock();
+      }
       status = SNU_OK;
       cv_mem.notify_all();
     } else {
       lk.unlock();
-      status = run_other(*r, m, st, &be, &iters);
+      status = run_other(batch, m, st, &be, &iters);
       lk.lock();
       int64_t now_bytes = m.h ? m.h->stats.device_bytes +
                                     (int64_t)(m.h->dcap * sizeof(double))
@@ -243,7 +336,7 @@ void snu_server::worker_loop(int slot) {
     }
     running--;
     m.busy = false;
-    post(*r, status, t0, be, iters, reused);
+    for (auto& q : batch) post(*q, status, t0, be, iters, reused);
     cv_work.notify_all();
     cv_mem.notify_all();
   }
@@ -261,11 +354,41 @@ int snu_server::run_factor(Request& r, cudaStream_t st, double t_start) {
   ho.ir_tol = o.ir_tol;
   ho.ir_max_iter = o.ir_max_iter;
   ho.device = o.device;
+  const uint64_t key = pattern_hash(r.n, r.nnz, r.rowptr.data(), r.colidx.data());
+  {
+    // a parked handle of this pattern: new values and a refactorization
+    int64_t pb = 0;
+    snu_handle* ph = nullptr;
+    {
+      std::lock_guard<std::mutex> g(mu);
+      ph = take_parked(key, r, &pb);
+    }
+    if (ph) {
+      snu_status s = snu_set_stream(ph, st);
+      if (s == SNU_OK) s = snu_refactor(ph, r.vals.data());
+      snu_set_stream(ph, nullptr);
+      std::lock_guard<std::mutex> g(mu);
+      Matrix& m = mats[r.matrix];
+      if (s == SNU_OK) {
+        m.h = ph;
+        m.n = r.n;
+        m.key = key;
+        m.bytes = ph->stats.device_bytes + (int64_t)(ph->dcap * sizeof(double));
+        resident += m.bytes - pb;
+      } else {
+        m.gone = true;
+        resident -= pb;
+        snu_destroy(ph);
+      }
+      peak = std::max(peak, resident + admitted);
+      cv_mem.notify_all();
+      return (int)s + 100;
+    }
+  }
   snu_handle* h = nullptr;
   snu_status s = snu_create(&h, &ho);
   if (s != SNU_OK) return s;
   h->stream = st;
-  const uint64_t key = pattern_hash(r.n, r.nnz, r.rowptr.data(), r.colidx.data());
   std::shared_ptr<const Plan> plan;
   {
     // one analysis per pattern: a request whose pattern is being analysed
@@ -328,6 +451,7 @@ int snu_server::run_factor(Request& r, cudaStream_t st, double t_start) {
       return SNU_ENOMEM;
     }
     waiting_mem++;
+    unpark_for(est, lk);
     while (resident + admitted + est > budget) {
       // a queued release of an idle matrix can be run right here
       bool ran = false;
@@ -378,6 +502,7 @@ int snu_server::run_factor(Request& r, cudaStream_t st, double t_start) {
   if (s == SNU_OK) {
     m.h = h;
     m.n = r.n;
+    m.key = key;
     m.bytes = h->stats.device_bytes;
     resident += m.bytes;
   } else {
@@ -389,14 +514,18 @@ int snu_server::run_factor(Request& r, cudaStream_t st, double t_start) {
   return (int)s + (reused ? 100 : 0);
 }
 
-int snu_server::run_other(Request& r, Matrix& m, cudaStream_t st, double* be,
-                          int* iters) {
+int snu_server::run_other(std::vector<std::unique_ptr<Request>>& batch,
+                          Matrix& m, cudaStream_t st, double* be, int* iters) {
   snu_status s = snu_set_stream(m.h, st);
   if (s != SNU_OK) return s;
+  Request& r = *batch[0];
   if (r.type == SNU_REQ_REFACTOR) {
     s = snu_refactor(m.h, r.vals.data());
   } else {
-    s = snu_solve(m.h, r.B, r.X, r.nrhs, r.ldb);
+    // the batch's solve requests: their columns solved together
+    std::vector<snu::SolvePiece> pieces;
+    for (auto& q : batch) pieces.push_back({q->B, q->X, q->nrhs, q->ldb});
+    s = snu::solve_pieces(m.h, pieces);
     *be = m.h->stats.backward_error;
     *iters = m.h->stats.ir_iters;
   }
@@ -494,6 +623,7 @@ SNU_API snu_status snu_server_destroy(snu_server* s) {
   for (auto& t : s->workers) t.join();
   for (auto& kv : s->mats)
     if (kv.second.h) snu_destroy(kv.second.h);
+  for (auto& p : s->parked) snu_destroy(p.h);
   delete s;
   return SNU_OK;
 }

@@ -225,13 +225,14 @@ def test_autotuned_factorization_matches(gpu, tmp_path):
 @pytest.mark.parametrize("env", [("SNU_PANEL_BLOCK", "0"), ("SNU_TC_GEMM", "0"),
                                  ("SNU_TC_PERSIST", "1"), ("SNU_TC_PERSIST", "0"),
                                  ("SNU_GRAPHS", "0"), ("SNU_TC_PANEL", "0"),
-                                 ("SNU_TC_PANEL", "1")])
+                                 ("SNU_TC_PANEL", "1"), ("SNU_SOLVE_FUSED", "1")])
 def test_alternative_paths_match(gpu, monkeypatch, env):
     # the paths behind the engine switches (read when an engine is made):
     # per-step panels instead of the fused outer-block kernel, SIMT instead
     # of tensor-core FP32 GEMMs, the persistent GEMM forced on or off, no
     # CUDA graph, the FP32 panel products on the tensor cores for no level
-    # or for every level -- each must reproduce the oracle like the default
+    # or for every level, the whole-tree solve sweeps instead of the
+    # level-by-level ones -- each must reproduce the oracle like the default
     monkeypatch.setenv(*env)
     rng = np.random.default_rng(41)
     rp, ci, v = _random_unsym(rng, 33, 30, 80)
