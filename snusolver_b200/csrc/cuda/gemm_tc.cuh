@@ -179,9 +179,12 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
       : "memory");
 }
 
+// Tile width BN (the MMA's N and the accumulator's TMEM columns): 128, or
+// 64 for batches of narrow problems (the autotuner picks per batch).
+template <int BN = TC_BN>
 constexpr size_t tc_smem_bytes() {
   return 1024 /* alignment slack */ +
-         (size_t)TC_STAGES * (TC_BM + TC_BN) * TC_BK * sizeof(float);
+         (size_t)TC_STAGES * (TC_BM + BN) * TC_BK * sizeof(float);
 }
 
 // ----------------------------------------------------------------- GEMM
@@ -197,6 +200,7 @@ __device__ __forceinline__ void prefetch_l2_span(const float* p, int n) {
                : "memory");
 }
 
+template <int BN>
 __global__ void __launch_bounds__(128, 1)
     k_gemm_tc(const TcTile* __restrict__ tiles, const TcProb* __restrict__ probs,
               const CUtensorMap* __restrict__ amaps,
@@ -206,7 +210,7 @@ __global__ void __launch_bounds__(128, 1)
   __shared__ uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES], acc_bar;
   __shared__ uint32_t tmem_base_s;
   __shared__ int failed_s;
-  __shared__ int rel_r[TC_BM], rel_c[TC_BN];  // scatter map of the tile
+  __shared__ int rel_r[TC_BM], rel_c[BN];  // scatter map of the tile
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   float* As = (float*)smem;                                   // [STAGES][BM*BK]
   float* Bs = As + (size_t)TC_STAGES * TC_BM * TC_BK;         // [STAGES][BN*BK]
@@ -228,7 +232,7 @@ __global__ void __launch_bounds__(128, 1)
     asm volatile(
         "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
             smem_addr(&tmem_base_s)),
-        "r"(TC_BN));
+        "r"(BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -248,16 +252,16 @@ __global__ void __launch_bounds__(128, 1)
         failed_s = 1;
         break;
       }
-      mbar_expect_tx(&full_bar[s], (TC_BM + TC_BN) * TC_BK * sizeof(float));
+      mbar_expect_tx(&full_bar[s], (TC_BM + BN) * TC_BK * sizeof(float));
       tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * TC_BK, tl.tm * TC_BM,
                   &full_bar[s]);
-      tma_load_2d(Bs + (size_t)s * TC_BN * TC_BK, bm, kb * TC_BK, tl.tn * TC_BN,
+      tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, kb * TC_BK, tl.tn * BN,
                   &full_bar[s]);
       issued = kb + 1;
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
-    const uint32_t idesc = tc_idesc(TC_BN);
+    const uint32_t idesc = tc_idesc(BN);
     for (int kb = 0; kb < nk; kb++) {
       const int s = kb % TC_STAGES;
       if (!mbar_wait(&full_bar[s], (kb / TC_STAGES) & 1, err)) {
@@ -266,7 +270,7 @@ __global__ void __launch_bounds__(128, 1)
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t a0 = smem_addr(As + (size_t)s * TC_BM * TC_BK);
-      const uint32_t b0 = smem_addr(Bs + (size_t)s * TC_BN * TC_BK);
+      const uint32_t b0 = smem_addr(Bs + (size_t)s * BN * TC_BK);
 #pragma unroll
       for (int kk = 0; kk < TC_BK / 8; kk++)
         tc_mma(tmem, umma_desc(a0 + kk * 32), umma_desc(b0 + kk * 32), idesc,
@@ -278,15 +282,15 @@ __global__ void __launch_bounds__(128, 1)
     // while the main loop runs: the tile's columns of C into L2 and the
     // scatter map into shared memory, for the epilogue
     const int t = threadIdx.x - 64;
-    const int r0 = tl.tm * TC_BM, c0 = tl.tn * TC_BN;
-    const int nr = min(TC_BM, pr.m - r0), ncl = min(TC_BN, pr.n - c0);
+    const int r0 = tl.tm * TC_BM, c0 = tl.tn * BN;
+    const int nr = min(TC_BM, pr.m - r0), ncl = min(BN, pr.n - c0);
     if (!pr.mode)  // (an overwritten C is not read)
       for (int c = t; c < ncl; c += 64)
         prefetch_l2_span(F + pr.c + r0 + (int64_t)(c0 + c) * pr.ldc, nr);
     if (pr.pc >= 0) {
       const int* rel = rel_base + pr.rel;
       for (int i = t; i < TC_BM; i += 64) rel_r[i] = i < nr ? rel[r0 + i] : 0;
-      for (int j = t; j < TC_BN; j += 64) rel_c[j] = j < ncl ? rel[c0 + j] : 0;
+      for (int j = t; j < BN; j += 64) rel_c[j] = j < ncl ? rel[c0 + j] : 0;
     }
   }
   __syncthreads();  // every role has finished issuing
@@ -298,7 +302,7 @@ __global__ void __launch_bounds__(128, 1)
   if (ok && nk > 0) {
     const int row = tl.tm * TC_BM + warp * 32 + lane;
     float* Cc = F + pr.c;
-    for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+    for (int c0 = 0; c0 < BN; c0 += 32) {
       uint32_t v[32];
       const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
       asm volatile(
@@ -318,7 +322,7 @@ __global__ void __launch_bounds__(128, 1)
       if (row < pr.m) {
         // all 32 loads of the chunk first, then the stores (no load waits
         // behind a store to a possibly aliasing address)
-        const int colbase = tl.tn * TC_BN + c0;
+        const int colbase = tl.tn * BN + c0;
         float* cp = Cc + row + (int64_t)colbase * pr.ldc;
         const int ncol = min(32, pr.n - colbase);
         float cv[32];
@@ -354,7 +358,7 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 2)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
                      tmem),
-                 "r"(TC_BN));
+                 "r"(BN));
 }
 
 // ------------------------------------------------------ persistent GEMM
@@ -375,6 +379,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
                : "memory");
 }
 
+template <int BN>
 __global__ void __launch_bounds__(TCP_THREADS, 1)
     k_gemm_tcp(const TcTile* __restrict__ tiles, int ntiles,
                const TcProb* __restrict__ probs,
@@ -407,7 +412,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
     asm volatile(
         "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
             smem_addr(&tmem_base_s)),
-        "r"(2 * TC_BN));
+        "r"(2 * BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -431,11 +436,11 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
           abort_s = 1;
           break;
         }
-        mbar_expect_tx(&full_bar[s], (TC_BM + TC_BN) * TC_BK * sizeof(float));
+        mbar_expect_tx(&full_bar[s], (TC_BM + BN) * TC_BK * sizeof(float));
         tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * TC_BK,
                     tl.tm * TC_BM, &full_bar[s]);
-        tma_load_2d(Bs + (size_t)s * TC_BN * TC_BK, bm, kb * TC_BK,
-                    tl.tn * TC_BN, &full_bar[s]);
+        tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, kb * TC_BK,
+                    tl.tn * BN, &full_bar[s]);
       }
     }
     // every issued load has landed before the CTA may exit
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
       mbar_wait(&full_bar[q % TC_STAGES], (q / TC_STAGES) & 1, err);
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
-    const uint32_t idesc = tc_idesc(TC_BN);
+    const uint32_t idesc = tc_idesc(BN);
     int g = 0, i = 0;
     for (int t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x, i++) {
       const int a = i & 1;
@@ -454,7 +459,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const TcProb pr = probs[tiles[t].prob];
       const int nk = 3 * pr.kpad / TC_BK;
-      const uint32_t d = tmem + (uint32_t)(a * TC_BN);
+      const uint32_t d = tmem + (uint32_t)(a * BN);
       bool ok = true;
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g % TC_STAGES;
@@ -464,7 +469,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t a0 = smem_addr(As + (size_t)s * TC_BM * TC_BK);
-        const uint32_t b0 = smem_addr(Bs + (size_t)s * TC_BN * TC_BK);
+        const uint32_t b0 = smem_addr(Bs + (size_t)s * BN * TC_BK);
 #pragma unroll
         for (int kk = 0; kk < TC_BK / 8; kk++)
           tc_mma(d, umma_desc(a0 + kk * 32), umma_desc(b0 + kk * 32), idesc,
@@ -490,8 +495,8 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
       const TcProb pr = probs[tl.prob];
       {
         // this warp's rows of C into L2 while the tile's MMAs run
-        const int r0 = tl.tm * TC_BM + qtr * 32, ct = tl.tn * TC_BN;
-        const int nr = min(32, pr.m - r0), ncl = min(TC_BN, pr.n - ct);
+        const int r0 = tl.tm * TC_BM + qtr * 32, ct = tl.tn * BN;
+        const int nr = min(32, pr.m - r0), ncl = min(BN, pr.n - ct);
         if (nr > 0 && !pr.mode)
           for (int c = lane; c < ncl; c += 32)
             prefetch_l2_span(F + pr.c + r0 + (int64_t)(ct + c) * pr.ldc, nr);
@@ -503,10 +508,10 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int row = tl.tm * TC_BM + qtr * 32 + lane;
       float* Cc = F + pr.c;
-      for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+      for (int c0 = 0; c0 < BN; c0 += 32) {
         uint32_t v[32];
         const uint32_t taddr =
-            tmem + (uint32_t)(a * TC_BN + c0) + ((uint32_t)(qtr * 32) << 16);
+            tmem + (uint32_t)(a * BN + c0) + ((uint32_t)(qtr * 32) << 16);
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
             "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -522,7 +527,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (row < pr.m) {
-          const int colbase = tl.tn * TC_BN + c0;
+          const int colbase = tl.tn * BN + c0;
           float* cp = Cc + row + (int64_t)colbase * pr.ldc;
           const int ncol = min(32, pr.n - colbase);
           float cv[32];
@@ -559,7 +564,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
   if (warp == 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
                      tmem),
-                 "r"(2 * TC_BN));
+                 "r"(2 * BN));
 }
 
 }  // namespace snu

@@ -177,6 +177,112 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
   }
 }
 
+// FP64 C -= A B (mode 0) or C = A B (mode 1) on the FP64 tensor cores
+// (mma.sync m8n8k4 .f64): the same 64 x 64 tiles and problems as k_gemm, four
+// warps of 32 x 32 each (4 x 4 MMA tiles of 8 x 8), k in steps of 16 staged
+// through shared memory with the next step's loads in flight in registers.
+// A warp reads one A and one B value per lane for every 4 x 4 block of
+// MMAs (16 fused multiply-adds per load, four times the SIMT kernel's).
+// Fragment layouts (PTX ISA, mma.m8n8k4 .f64): lane l holds A(l / 4, l % 4),
+// B(l % 4, l / 4) and C(l / 4, 2 (l % 4) + {0, 1}).
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, "
+      "{%0, %1};"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(128)
+    k_gemm_dmma(const GemmTile* __restrict__ tiles,
+                const GemmProb* __restrict__ probs,
+                const double* __restrict__ Abase,
+                const double* __restrict__ Bbase, double* __restrict__ Cbase,
+                int mode, const int* __restrict__ rel_base) {
+  constexpr int BM = 64, BN = 64, BK = 16, PAD = 4;
+  __shared__ double As[BK][BM + PAD];  // As[k][m]
+  __shared__ double Bs[BK][BN + PAD];  // Bs[k][n]
+  const GemmTile tl = tiles[blockIdx.x];
+  const GemmProb P = probs[tl.prob];
+  const int m0 = tl.tm * BM, n0 = tl.tn * BN;
+  const double* A = Abase + P.a;
+  const double* B = Bbase + P.b;
+  double* C = Cbase + P.c;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;  // warp tile origin
+  const int gr = lane >> 2, gc = lane & 3;                // fragment coords
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+  // loads: A tile BM x BK (8 per thread, rows contiguous), B tile BK x BN
+  // (8 per thread, k contiguous)
+  constexpr int LA = BM * BK / 128, LB = BK * BN / 128;
+  double ra[LA], rb[LB];
+  auto gload = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < LA; q++) {
+      const int e = tid + q * 128, i = e % BM, l = e / BM;
+      const int gi = m0 + i, gl = k0 + l;
+      ra[q] = (gi < P.m && gl < P.k) ? A[gi + (int64_t)gl * P.lda] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < LB; q++) {
+      const int e = tid + q * 128, l = e % BK, j = e / BK;
+      const int gl = k0 + l, gj = n0 + j;
+      rb[q] = (gl < P.k && gj < P.n) ? B[gl + (int64_t)gj * P.ldb] : 0.0;
+    }
+  };
+  if (P.k > 0) gload(0);
+  for (int k0 = 0; k0 < P.k; k0 += BK) {
+#pragma unroll
+    for (int q = 0; q < LA; q++) {
+      const int e = tid + q * 128;
+      As[e / BM][e % BM] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < LB; q++) {
+      const int e = tid + q * 128;
+      Bs[e % BK][e / BK] = rb[q];
+    }
+    __syncthreads();
+    if (k0 + BK < P.k) gload(k0 + BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = As[kk + gc][wm + 8 * i + gr];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = Bs[kk + gc][wn + 8 * j + gr];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) dmma_8x8x4(acc[i][j], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+  const int* rel = rel_base + P.rel;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int gi = m0 + wm + 8 * i + gr;
+    if (gi >= P.m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int gj = n0 + wn + 8 * j + 2 * gc + h;
+        if (gj >= P.n) continue;
+        double* c = C + gi + (int64_t)gj * P.ldc;
+        if (P.pc >= 0)  // extend-add fused: the update goes to the parent
+          atomicAdd(Cbase + P.pc + rel[gi] + (int64_t)rel[gj] * P.pld,
+                    *c - acc[i][j][h]);
+        else
+          *c = mode ? acc[i][j][h] : *c - acc[i][j][h];
+      }
+  }
+}
+
 // ------------------------------------------------------------------ solves
 
 // Work vectors: front f holds dim x nrhs values at W + w_off * nrhs.

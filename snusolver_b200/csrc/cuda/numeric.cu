@@ -93,16 +93,18 @@ struct GemmBatch {
   // FP32 path: problems large enough for the tensor cores, and the rest
   std::vector<TcProb> tc_host;
   TcProb* tcp = nullptr;
-  TcTile* tct = nullptr;
+  // per tile width (index 0: BN = 128, 1: BN = 64): tiles and B maps
+  TcTile* tct[2] = {nullptr, nullptr};
   CUtensorMap* amaps = nullptr;
-  CUtensorMap* bmaps = nullptr;
-  int ntcp = 0, ntct = 0, tc_maxm = 0, tc_maxn = 0, tc_maxkpad = 0;
+  CUtensorMap* bmaps[2] = {nullptr, nullptr};
+  int ntcp = 0, ntct[2] = {0, 0}, tc_maxm = 0, tc_maxn = 0, tc_maxkpad = 0;
   GemmProb* rprobs = nullptr;  // SIMT remainder of the FP32 path
   GemmTile* rtiles = nullptr;
   int nrtiles = 0;
-  // tensor-core kernel variant: 0 one CTA per tile, 1 persistent and
-  // warp-specialised; a heuristic default (mean K of the tiles) unless the
-  // autotuner timed both
+  // tensor-core kernel variant: bit 0 -- 0 one CTA per tile, 1 persistent
+  // and warp-specialised; bit 1 -- tile width 128 (0) or 64 (1); a
+  // heuristic default (width 128, persistent for a long mean K) unless the
+  // autotuner timed all four
   int variant = 0;
   double ktiles = 0;  // sum of kpad over tiles (for the heuristic)
 };
@@ -213,18 +215,27 @@ class CudaEngine : public Engine {
     CK(cudaFuncSetAttribute(k_diag_lu_inv<float>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)diag_smem<float>()));
-    CK(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)tc_smem_bytes()));
-    CK(cudaFuncSetAttribute(k_gemm_tcp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)tc_smem_bytes()));
+    CK(cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tc_smem_bytes<128>()));
+    CK(cudaFuncSetAttribute(k_gemm_tcp<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tc_smem_bytes<128>()));
+    CK(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tc_smem_bytes<64>()));
+    CK(cudaFuncSetAttribute(k_gemm_tcp<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tc_smem_bytes<64>()));
     CK(cudaFuncSetAttribute(k_block_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)binv_smem()));
     {
       int sms = 0, nb = 0;
       CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gemm_tcp, TCP_THREADS,
-                                                       tc_smem_bytes()));
-      tcp_cap_ = std::max(1, std::min(nb, 2)) * sms;  // TMEM: 2 x 256 columns
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gemm_tcp<128>,
+                                                       TCP_THREADS,
+                                                       tc_smem_bytes<128>()));
+      tcp_cap_[0] = std::max(1, std::min(nb, 2)) * sms;  // TMEM: 2 x 256 columns
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gemm_tcp<64>,
+                                                       TCP_THREADS,
+                                                       tc_smem_bytes<64>()));
+      tcp_cap_[1] = std::max(1, std::min(nb, 4)) * sms;  // TMEM: 4 x 128 columns
     }
     {
       const char* e = getenv("SNU_TC_GEMM");
@@ -233,6 +244,12 @@ class CudaEngine : public Engine {
       use_graphs_ = !(g && g[0] == '0');
       const char* tp = getenv("SNU_TC_PERSIST");
       force_tcp_ = tp ? (tp[0] == '0' ? 0 : 1) : -1;
+      // SNU_TC_WIDTH=64 or 128: every tensor-core batch at that tile width
+      // SNU_DMMA=0: FP64 GEMMs on the SIMT kernel instead of mma.sync f64
+      const char* dm = getenv("SNU_DMMA");
+      use_dmma_ = !(dm && dm[0] == '0');
+      const char* tw = getenv("SNU_TC_WIDTH");
+      force_width_ = tw ? (atoi(tw) == 64 ? 1 : 0) : -1;
       const char* vb = getenv("SNU_VERBOSE");
       verbose_ = vb && vb[0] == '1';
       const char* pbk = getenv("SNU_PANEL_BLOCK");
@@ -496,7 +513,8 @@ class CudaEngine : public Engine {
       if (!d_F32_ && (rc = alloc(d_F32_, (size_t)(invb_base_ + invb_need_)))) return rc;
       if (!d_I32_ && (rc = alloc(d_I32_, (size_t)invtot_))) return rc;
     }
-    if (phase == 0 && precision == 1 && autotune_ && !tuned_ && force_tcp_ < 0) {
+    if (phase == 0 && precision == 1 && autotune_ && !tuned_ && force_tcp_ < 0 &&
+        force_width_ < 0) {
       if ((rc = autotune())) return rc;
     }
     if (phase != 2) {  // (phase 2 adds to phase 1's counts)
@@ -830,11 +848,12 @@ class CudaEngine : public Engine {
   }
 
  private:
-  // Picks the tensor-core kernel variant of every FP32 GEMM batch: from the
-  // cache file when it holds this pattern, else by timing two complete
-  // factorizations (every batch with variant 0, then 1; the factorization
-  // is recomputed from the values each time, so nothing is lost) and
-  // keeping the faster variant per batch.  The choice is baked into the
+  // Picks the tensor-core kernel variant of every FP32 GEMM batch -- one CTA
+  // per tile or persistent, tile width 128 or 64: from the cache file when
+  // it holds this pattern, else by timing four complete factorizations
+  // (every batch with variant 0, 1, 2, then 3; the factorization is
+  // recomputed from the values each time, so nothing is lost) and keeping
+  // the fastest variant per batch.  The choice is baked into the
   // factorization's CUDA graph.
   int autotune() {
     tuned_ = true;
@@ -855,8 +874,9 @@ class CudaEngine : public Engine {
         if (hit) return ENG_OK;
       }
     }
-    std::vector<double> t(2 * nb, 0.0);
-    for (int v = 0; v < 2; v++) {
+    constexpr int NV = 4;  // {one CTA per tile, persistent} x {128, 64}
+    std::vector<double> t(NV * nb, 0.0);
+    for (int v = 0; v < NV; v++) {
       for (GemmBatch* gb : tc_batches_) gb->variant = v;
       tuning_ = true;
       tune_rec_.clear();
@@ -870,15 +890,18 @@ class CudaEngine : public Engine {
         CK(cudaEventElapsedTime(&ms, tune_events_[r.second],
                                 tune_events_[r.second + 1]));
         for (size_t i = 0; i < nb; i++)
-          if (tc_batches_[i] == r.first) t[2 * i + v] += ms;
+          if (tc_batches_[i] == r.first) t[NV * i + v] += ms;
       }
       for (cudaEvent_t e : tune_events_) cudaEventDestroy(e);
       tune_events_.clear();
     }
     std::string choice(nb, '0');
     for (size_t i = 0; i < nb; i++) {
-      tc_batches_[i]->variant = t[2 * i + 1] < t[2 * i] ? 1 : 0;
-      choice[i] = (char)('0' + tc_batches_[i]->variant);
+      int best = 0;
+      for (int v = 1; v < NV; v++)
+        if (t[NV * i + v] < t[NV * i + best]) best = v;
+      tc_batches_[i]->variant = best;
+      choice[i] = (char)('0' + best);
     }
     if (factor_graph_[1]) {
       cudaGraphExecDestroy(factor_graph_[1]);
@@ -1273,14 +1296,16 @@ class CudaEngine : public Engine {
     }
     EncodeTiledFn enc = (EncodeTiledFn)fn;
     for (GemmBatch* gb : tc_batches_) {
-      std::vector<CUtensorMap> am(gb->tc_host.size()), bm(gb->tc_host.size());
-      std::vector<TcTile> tiles;
-      for (size_t k = 0; k < gb->tc_host.size(); k++) {
+      const size_t np = gb->tc_host.size();
+      std::vector<CUtensorMap> am(np), bm[2] = {std::vector<CUtensorMap>(np),
+                                                std::vector<CUtensorMap>(np)};
+      std::vector<TcTile> tiles[2];
+      for (size_t k = 0; k < np; k++) {
         const TcProb& t = gb->tc_host[k];
         const cuuint64_t kk = 3 * (cuuint64_t)t.kpad;
         cuuint64_t dimA[2] = {kk, (cuuint64_t)t.m}, dimB[2] = {kk, (cuuint64_t)t.n};
         cuuint64_t stride[1] = {kk * sizeof(float)};
-        cuuint32_t boxA[2] = {TC_BK, TC_BM}, boxB[2] = {TC_BK, TC_BN};
+        cuuint32_t boxA[2] = {TC_BK, TC_BM};
         cuuint32_t es[2] = {1, 1};
         CUresult r1 = enc(&am[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
                           d_pack_ + t.apack, dimA, stride, boxA, es,
@@ -1288,30 +1313,42 @@ class CudaEngine : public Engine {
                           CU_TENSOR_MAP_SWIZZLE_128B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        CUresult r2 = enc(&bm[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                          d_pack_ + t.bpack, dimB, stride, boxB, es,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          CU_TENSOR_MAP_SWIZZLE_128B,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) {
+        if (r1 != CUDA_SUCCESS) {
           err_ = "tensor map encoding failed";
           return ENG_ECUDA;
         }
-        int tm = (t.m + TC_BM - 1) / TC_BM, tn = (t.n + TC_BN - 1) / TC_BN;
-        gb->ktiles += (double)t.kpad * tm * tn;
-        for (int b = 0; b < tn; b++)
-          for (int a = 0; a < tm; a++) tiles.push_back({(int)k, a, b});
+        const int tm = (t.m + TC_BM - 1) / TC_BM;
+        for (int w = 0; w < 2; w++) {
+          const int bn = w ? 64 : 128;
+          cuuint32_t boxB[2] = {TC_BK, (cuuint32_t)bn};
+          CUresult r2 = enc(&bm[w][k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                            d_pack_ + t.bpack, dimB, stride, boxB, es,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+          if (r2 != CUDA_SUCCESS) {
+            err_ = "tensor map encoding failed";
+            return ENG_ECUDA;
+          }
+          const int tn = (t.n + bn - 1) / bn;
+          if (!w) gb->ktiles += (double)t.kpad * tm * tn;
+          for (int b = 0; b < tn; b++)
+            for (int a = 0; a < tm; a++) tiles[w].push_back({(int)k, a, b});
+        }
       }
-      gb->ntcp = (int)gb->tc_host.size();
-      gb->ntct = (int)tiles.size();
+      gb->ntcp = (int)np;
+      gb->ntct[0] = (int)tiles[0].size();
+      gb->ntct[1] = (int)tiles[1].size();
       // long K per tile: the persistent kernel hides each epilogue behind
       // the next tile's MMAs; short K: one CTA per tile balances better
-      gb->variant = gb->ktiles / std::max(1, gb->ntct) >= 512 ? 1 : 0;
+      gb->variant = gb->ktiles / std::max(1, gb->ntct[0]) >= 512 ? 1 : 0;
       if ((rc = upload(gb->tcp, gb->tc_host))) return rc;
-      if ((rc = upload(gb->tct, tiles))) return rc;
       if ((rc = upload(gb->amaps, am))) return rc;
-      if ((rc = upload(gb->bmaps, bm))) return rc;
+      for (int w = 0; w < 2; w++) {
+        if ((rc = upload(gb->tct[w], tiles[w]))) return rc;
+        if ((rc = upload(gb->bmaps[w], bm[w]))) return rc;
+      }
     }
     return ENG_OK;
   }
@@ -1766,8 +1803,13 @@ class CudaEngine : public Engine {
                   cudaStream_t st, int fam) {
     if (gb.ntiles == 0) return ENG_OK;
     int pi = prof_begin(fam, st);
-    k_gemm<T, GBM, GBN, 16, 4, 4><<<gb.ntiles, 256, 0, st>>>(
-        gb.tiles, gb.probs, A, B, C, mode, d_rel_);
+    if (sizeof(T) == 8 && use_dmma_)  // FP64 on the FP64 tensor cores
+      k_gemm_dmma<<<gb.ntiles, 128, 0, st>>>(gb.tiles, gb.probs,
+                                             (const double*)A, (const double*)B,
+                                             (double*)C, mode, d_rel_);
+    else
+      k_gemm<T, GBM, GBN, 16, 4, 4><<<gb.ntiles, 256, 0, st>>>(
+          gb.tiles, gb.probs, A, B, C, mode, d_rel_);
     CKL();
     prof_end(pi, fam, st, gb.flops, gb.elems * sizeof(T));
     return ENG_OK;
@@ -1788,7 +1830,9 @@ class CudaEngine : public Engine {
     dim3 gbp((gb.tc_maxn + 7) / 8, gb.ntcp);
     k_tc_pack_b<<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
     CKL();
-    const int variant = force_tcp_ >= 0 ? force_tcp_ : gb.variant;
+    const int variant =
+        (force_tcp_ >= 0 ? force_tcp_ : (gb.variant & 1)) |
+        ((force_width_ >= 0 ? force_width_ : (gb.variant >> 1) & 1) << 1);
     int te = -1;
     if (tuning_) {  // autotuner: time this launch
       te = (int)tune_events_.size();
@@ -1799,14 +1843,24 @@ class CudaEngine : public Engine {
       }
       CK(cudaEventRecord(tune_events_[te], st));
     }
-    if (variant == 1)  // persistent, warp-specialised
-      k_gemm_tcp<<<std::min(gb.ntct, tcp_cap_), TCP_THREADS, tc_smem_bytes(),
-                   st>>>(gb.tct, gb.ntct, gb.tcp, gb.amaps, gb.bmaps, F,
-                         d_flags_ + 2, d_rel_);
+    const int w = (variant >> 1) & 1;  // tile width 128 or 64
+    const int nt = gb.ntct[w];
+    if ((variant & 1) && !w)  // persistent, warp-specialised
+      k_gemm_tcp<128><<<std::min(nt, tcp_cap_[0]), TCP_THREADS,
+                        tc_smem_bytes<128>(), st>>>(gb.tct[0], nt, gb.tcp,
+                                                    gb.amaps, gb.bmaps[0], F,
+                                                    d_flags_ + 2, d_rel_);
+    else if (variant & 1)
+      k_gemm_tcp<64><<<std::min(nt, tcp_cap_[1]), TCP_THREADS,
+                       tc_smem_bytes<64>(), st>>>(gb.tct[1], nt, gb.tcp,
+                                                  gb.amaps, gb.bmaps[1], F,
+                                                  d_flags_ + 2, d_rel_);
+    else if (!w)
+      k_gemm_tc<128><<<nt, 128, tc_smem_bytes<128>(), st>>>(
+          gb.tct[0], gb.tcp, gb.amaps, gb.bmaps[0], F, d_flags_ + 2, d_rel_);
     else
-      k_gemm_tc<<<gb.ntct, 128, tc_smem_bytes(), st>>>(gb.tct, gb.tcp, gb.amaps,
-                                                      gb.bmaps, F, d_flags_ + 2,
-                                                      d_rel_);
+      k_gemm_tc<64><<<nt, 128, tc_smem_bytes<64>(), st>>>(
+          gb.tct[1], gb.tcp, gb.amaps, gb.bmaps[1], F, d_flags_ + 2, d_rel_);
     if (te >= 0) {
       CK(cudaEventRecord(tune_events_[te + 1], st));
       tune_rec_.push_back({(const GemmBatch*)&gb, te});
@@ -2431,7 +2485,9 @@ class CudaEngine : public Engine {
   int64_t sctl_size_ = 0;
   double sweep_elems_ = 0;  // factor entries one sweep reads (per column)
   int force_tcp_ = -1;  // tensor-core kernel variant forced (-1: per batch)
-  int tcp_cap_ = 148;
+  int force_width_ = -1;  // tensor-core tile width forced (0: 128, 1: 64)
+  bool use_dmma_ = true;  // FP64 GEMMs on the FP64 tensor cores
+  int tcp_cap_[2] = {148, 148};  // persistent grid per tile width
   // autotuner of the tensor-core kernel variant per GEMM batch
   bool autotune_ = false, tuned_ = false, tuning_ = false;
   std::string tune_path_;

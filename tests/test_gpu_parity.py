@@ -199,8 +199,9 @@ def test_solve_device_pointers(gpu):
 
 
 def test_autotuned_factorization_matches(gpu, tmp_path):
-    # the autotuner times both tensor-core GEMM kernels per batch, keeps the
-    # faster, and records the choice; results stay those of the default
+    # the autotuner times the tensor-core GEMM variants per batch (one CTA
+    # per tile or persistent, tile width 128 or 64), keeps the fastest and
+    # records the choice; results stay those of the default
     rp, ci, v = generators.convdiff3d(20)
     n = len(rp) - 1
     B = generators.rhs(n, 2, seed=3)
@@ -211,7 +212,7 @@ def test_autotuned_factorization_matches(gpu, tmp_path):
     s.set_autotune(True, str(cache))
     X = s.factorize().solve(B)
     lines = cache.read_text().split()
-    assert len(lines) == 2 and set(lines[1]) <= {"0", "1"}
+    assert len(lines) == 2 and set(lines[1]) <= {"0", "1", "2", "3"}
     for r in range(2):
         assert rel_resid(rp, ci, v, X[:, r], B[:, r]) <= 1e-10
     assert np.abs(X - Xr).max() <= 1e-8 * np.abs(Xr).max()
@@ -225,14 +226,16 @@ def test_autotuned_factorization_matches(gpu, tmp_path):
 @pytest.mark.parametrize("env", [("SNU_PANEL_BLOCK", "0"), ("SNU_TC_GEMM", "0"),
                                  ("SNU_TC_PERSIST", "1"), ("SNU_TC_PERSIST", "0"),
                                  ("SNU_GRAPHS", "0"), ("SNU_TC_PANEL", "0"),
-                                 ("SNU_TC_PANEL", "1"), ("SNU_SOLVE_FUSED", "1")])
+                                 ("SNU_TC_PANEL", "1"), ("SNU_SOLVE_FUSED", "1"),
+                                 ("SNU_TC_WIDTH", "64"), ("SNU_DMMA", "0")])
 def test_alternative_paths_match(gpu, monkeypatch, env):
     # the paths behind the engine switches (read when an engine is made):
     # per-step panels instead of the fused outer-block kernel, SIMT instead
     # of tensor-core FP32 GEMMs, the persistent GEMM forced on or off, no
     # CUDA graph, the FP32 panel products on the tensor cores for no level
     # or for every level, the whole-tree solve sweeps instead of the
-    # level-by-level ones -- each must reproduce the oracle like the default
+    # level-by-level ones, 64-wide tensor-core tiles -- each must reproduce
+    # the oracle like the default
     monkeypatch.setenv(*env)
     rng = np.random.default_rng(41)
     rp, ci, v = _random_unsym(rng, 33, 30, 80)
