@@ -18,6 +18,7 @@
 // and returns.
 #pragma once
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <stdint.h>
 
 namespace snu {
@@ -29,7 +30,7 @@ struct TcProb {
   int m, n, k, kpad;
   int64_t a, b, c;  // element offsets of A, B, C in the front arena
   int lda, ldb, ldc;
-  int64_t apack, bpack;  // element offsets of A', B' in the pack workspace
+  int64_t apack, bpack;  // byte offsets of A', B' in the pack workspace
   int64_t pc, rel;       // Schur scatter into the parent (see GemmProb)
   int pld;
   int mode;              // 0: C -= A B, 1: C = A B (pc < 0 only)
@@ -47,11 +48,39 @@ __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float(r);
 }
 
+// The split of one value into hi + lo: TF32 (BF = false, kind::tf32) or
+// BF16 (BF = true, kind::f16 with both operands bf16).  TF32x3 keeps FP32
+// accuracy (lo carries the next 11 bits); BF16x3 about 16 bits (2^-16
+// relative per product), which FP64 refinement then recovers.
+template <bool BF>
+struct Split;
+template <>
+struct Split<false> {
+  typedef float E;
+  static constexpr int KB = 32;  // elements per 128-byte row of a tile
+  __device__ __forceinline__ static void apply(float v, E& hi, E& lo) {
+    hi = tf32_rna(v);
+    lo = tf32_rna(v - hi);
+  }
+};
+template <>
+struct Split<true> {
+  typedef __nv_bfloat16 E;
+  static constexpr int KB = 64;
+  __device__ __forceinline__ static void apply(float v, E& hi, E& lo) {
+    hi = __float2bfloat16_rn(v);
+    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+  }
+};
+
 // A' (m rows x 3*kpad) from A (m x k, column-major): 32 x 32 blocks through
 // shared memory so both the column-major reads and the row-major writes are
 // coalesced.  grid: (kpad/32, ceil(m/32), problems); block 32 x 8.
+template <bool BF>
 __global__ void k_tc_pack_a(const TcProb* __restrict__ probs,
-                            const float* __restrict__ F, float* __restrict__ P) {
+                            const float* __restrict__ F,
+                            unsigned char* __restrict__ P) {
+  typedef typename Split<BF>::E E;
   __shared__ float t[32][33];
   const TcProb pr = probs[blockIdx.z];
   const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
@@ -62,14 +91,14 @@ __global__ void k_tc_pack_a(const TcProb* __restrict__ probs,
     t[cc][threadIdx.x] = (r < pr.m && c < pr.k) ? A[r + (int64_t)c * pr.lda] : 0.f;
   }
   __syncthreads();
-  float* out = P + pr.apack;
+  E* out = reinterpret_cast<E*>(P + pr.apack);
   const int64_t kk = 3 * (int64_t)pr.kpad;
   for (int rr = threadIdx.y; rr < 32; rr += 8) {
     int r = r0 + rr, c = c0 + threadIdx.x;
     if (r >= pr.m) continue;
-    float v = t[threadIdx.x][rr];
-    float hi = tf32_rna(v), lo = tf32_rna(v - hi);
-    float* row = out + r * kk;
+    E hi, lo;
+    Split<BF>::apply(t[threadIdx.x][rr], hi, lo);
+    E* row = out + r * kk;
     row[c] = hi;
     row[pr.kpad + c] = hi;
     row[2 * pr.kpad + c] = lo;
@@ -78,17 +107,20 @@ __global__ void k_tc_pack_a(const TcProb* __restrict__ probs,
 
 // B' (n rows x 3*kpad) from B (k x n, column-major): column c of B is row c
 // of B', already contiguous.  grid: (ceil(n/8), problems); block 256.
+template <bool BF>
 __global__ void k_tc_pack_b(const TcProb* __restrict__ probs,
-                            const float* __restrict__ F, float* __restrict__ P) {
+                            const float* __restrict__ F,
+                            unsigned char* __restrict__ P) {
+  typedef typename Split<BF>::E E;
   const TcProb pr = probs[blockIdx.y];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = blockIdx.x * 8 + warp;
   if (c >= pr.n) return;
   const float* B = F + pr.b + (int64_t)c * pr.ldb;
-  float* row = P + pr.bpack + (int64_t)c * 3 * pr.kpad;
+  E* row = reinterpret_cast<E*>(P + pr.bpack) + (int64_t)c * 3 * pr.kpad;
   for (int kk = lane; kk < pr.kpad; kk += 32) {
-    float v = kk < pr.k ? B[kk] : 0.f;
-    float hi = tf32_rna(v), lo = tf32_rna(v - hi);
+    E hi, lo;
+    Split<BF>::apply(kk < pr.k ? B[kk] : 0.f, hi, lo);
     row[kk] = hi;
     row[pr.kpad + kk] = lo;
     row[2 * pr.kpad + kk] = hi;
@@ -154,22 +186,34 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
   return d;
 }
 
-// Instruction descriptor: D f32, A/B tf32, both K-major, M = 128, N = BN.
+// Instruction descriptor: D f32, A and B both tf32 (BF false) or both bf16
+// (BF true), both K-major, M = 128, N = BN.
+template <bool BF = false>
 __host__ __device__ constexpr uint32_t tc_idesc(int bn) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(bn >> 3) << 17) |
-         ((uint32_t)(TC_BM >> 4) << 24);
+  return (1u << 4) | ((BF ? 1u : 2u) << 7) | ((BF ? 1u : 2u) << 10) |
+         ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
 }
 
+template <bool BF = false>
 __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc,
                                        uint64_t bdesc, uint32_t idesc,
                                        uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(
-          tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
+  if constexpr (BF)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+            tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+            tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
 }
 
 __device__ __forceinline__ void tc_commit(uint64_t* bar) {
@@ -200,7 +244,7 @@ __device__ __forceinline__ void prefetch_l2_span(const float* p, int n) {
                : "memory");
 }
 
-template <int BN>
+template <int BN, bool BF = false>
 __global__ void __launch_bounds__(128, 1)
     k_gemm_tc(const TcTile* __restrict__ tiles, const TcProb* __restrict__ probs,
               const CUtensorMap* __restrict__ amaps,
@@ -217,7 +261,7 @@ __global__ void __launch_bounds__(128, 1)
   const TcTile tl = tiles[blockIdx.x];
   const TcProb pr = probs[tl.prob];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nk = 3 * pr.kpad / TC_BK;
+  const int nk = 3 * pr.kpad / Split<BF>::KB;
 
   if (threadIdx.x == 0) {
     failed_s = 0;
@@ -253,15 +297,15 @@ __global__ void __launch_bounds__(128, 1)
         break;
       }
       mbar_expect_tx(&full_bar[s], (TC_BM + BN) * TC_BK * sizeof(float));
-      tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * TC_BK, tl.tm * TC_BM,
+      tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * Split<BF>::KB, tl.tm * TC_BM,
                   &full_bar[s]);
-      tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, kb * TC_BK, tl.tn * BN,
+      tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, kb * Split<BF>::KB, tl.tn * BN,
                   &full_bar[s]);
       issued = kb + 1;
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
-    const uint32_t idesc = tc_idesc(BN);
+    const uint32_t idesc = tc_idesc<BF>(BN);
     for (int kb = 0; kb < nk; kb++) {
       const int s = kb % TC_STAGES;
       if (!mbar_wait(&full_bar[s], (kb / TC_STAGES) & 1, err)) {
@@ -273,7 +317,7 @@ __global__ void __launch_bounds__(128, 1)
       const uint32_t b0 = smem_addr(Bs + (size_t)s * BN * TC_BK);
 #pragma unroll
       for (int kk = 0; kk < TC_BK / 8; kk++)
-        tc_mma(tmem, umma_desc(a0 + kk * 32), umma_desc(b0 + kk * 32), idesc,
+        tc_mma<BF>(tmem, umma_desc(a0 + kk * 32), umma_desc(b0 + kk * 32), idesc,
                (kb > 0 || kk > 0) ? 1u : 0u);
       tc_commit(&empty_bar[s]);
     }
@@ -379,7 +423,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
                : "memory");
 }
 
-template <int BN>
+template <int BN, bool BF = false>
 __global__ void __launch_bounds__(TCP_THREADS, 1)
     k_gemm_tcp(const TcTile* __restrict__ tiles, int ntiles,
                const TcProb* __restrict__ probs,
@@ -428,7 +472,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
       const TcProb pr = probs[tl.prob];
       const CUtensorMap* am = amaps + tl.prob;
       const CUtensorMap* bm = bmaps + tl.prob;
-      const int nk = 3 * pr.kpad / TC_BK;
+      const int nk = 3 * pr.kpad / Split<BF>::KB;
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g % TC_STAGES;
         if (g >= TC_STAGES &&
@@ -437,9 +481,9 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
           break;
         }
         mbar_expect_tx(&full_bar[s], (TC_BM + BN) * TC_BK * sizeof(float));
-        tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * TC_BK,
+        tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * Split<BF>::KB,
                     tl.tm * TC_BM, &full_bar[s]);
-        tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, kb * TC_BK,
+        tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, kb * Split<BF>::KB,
                     tl.tn * BN, &full_bar[s]);
       }
     }
@@ -448,7 +492,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
       mbar_wait(&full_bar[q % TC_STAGES], (q / TC_STAGES) & 1, err);
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
-    const uint32_t idesc = tc_idesc(BN);
+    const uint32_t idesc = tc_idesc<BF>(BN);
     int g = 0, i = 0;
     for (int t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x, i++) {
       const int a = i & 1;
@@ -458,7 +502,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const TcProb pr = probs[tiles[t].prob];
-      const int nk = 3 * pr.kpad / TC_BK;
+      const int nk = 3 * pr.kpad / Split<BF>::KB;
       const uint32_t d = tmem + (uint32_t)(a * BN);
       bool ok = true;
       for (int kb = 0; kb < nk; kb++, g++) {
@@ -472,7 +516,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
         const uint32_t b0 = smem_addr(Bs + (size_t)s * BN * TC_BK);
 #pragma unroll
         for (int kk = 0; kk < TC_BK / 8; kk++)
-          tc_mma(d, umma_desc(a0 + kk * 32), umma_desc(b0 + kk * 32), idesc,
+          tc_mma<BF>(d, umma_desc(a0 + kk * 32), umma_desc(b0 + kk * 32), idesc,
                  (kb > 0 || kk > 0) ? 1u : 0u);
         tc_commit(&empty_bar[s]);
       }

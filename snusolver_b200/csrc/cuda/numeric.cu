@@ -158,6 +158,10 @@ struct LevelSched {
   std::vector<int> nea;
   EaTask* ea_kids = nullptr;  // (child, first of 256 Q rows) of the level's
   int nea_kids = 0;           // fronts' children (solve extend-add)
+  // deterministic mode: the same, one list per child rank (siblings add
+  // into their parent in a fixed order, one launch per rank)
+  std::vector<EaTask*> ea_kids_r;
+  std::vector<int> nea_kids_r;
   int* list = nullptr;  // fronts of the level (of the schedule's set)
   int* listq = nullptr; // those with q > 0
   int nlist = 0, nlistq = 0;
@@ -215,24 +219,27 @@ class CudaEngine : public Engine {
     CK(cudaFuncSetAttribute(k_diag_lu_inv<float>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)diag_smem<float>()));
-    CK(cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)tc_smem_bytes<128>()));
-    CK(cudaFuncSetAttribute(k_gemm_tcp<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)tc_smem_bytes<128>()));
-    CK(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)tc_smem_bytes<64>()));
-    CK(cudaFuncSetAttribute(k_gemm_tcp<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)tc_smem_bytes<64>()));
+    {
+      const int s128 = (int)tc_smem_bytes<128>(), s64 = (int)tc_smem_bytes<64>();
+      CK(cudaFuncSetAttribute(k_gemm_tc<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128));
+      CK(cudaFuncSetAttribute(k_gemm_tcp<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128));
+      CK(cudaFuncSetAttribute(k_gemm_tc<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
+      CK(cudaFuncSetAttribute(k_gemm_tcp<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
+      CK(cudaFuncSetAttribute(k_gemm_tc<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128));
+      CK(cudaFuncSetAttribute(k_gemm_tcp<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128));
+      CK(cudaFuncSetAttribute(k_gemm_tc<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
+      CK(cudaFuncSetAttribute(k_gemm_tcp<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
+    }
     CK(cudaFuncSetAttribute(k_block_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)binv_smem()));
     {
       int sms = 0, nb = 0;
       CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gemm_tcp<128>,
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gemm_tcp<128, false>,
                                                        TCP_THREADS,
                                                        tc_smem_bytes<128>()));
       tcp_cap_[0] = std::max(1, std::min(nb, 2)) * sms;  // TMEM: 2 x 256 columns
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gemm_tcp<64>,
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gemm_tcp<64, false>,
                                                        TCP_THREADS,
                                                        tc_smem_bytes<64>()));
       tcp_cap_[1] = std::max(1, std::min(nb, 4)) * sms;  // TMEM: 4 x 128 columns
@@ -244,10 +251,19 @@ class CudaEngine : public Engine {
       use_graphs_ = !(g && g[0] == '0');
       const char* tp = getenv("SNU_TC_PERSIST");
       force_tcp_ = tp ? (tp[0] == '0' ? 0 : 1) : -1;
-      // SNU_TC_WIDTH=64 or 128: every tensor-core batch at that tile width
+      // SNU_DETERMINISTIC=1: bit-reproducible results -- sibling updates
+      // added in a fixed order (F22 in place, one extend-add launch per
+      // child rank) and the solve's products without split-K atomics
+      const char* de = getenv("SNU_DETERMINISTIC");
+      deterministic_ = de && de[0] == '1';
+      // SNU_SPLIT=bf16: FP32 GEMMs with the BF16x3 split (kind::f16)
+      // instead of TF32x3 (kind::tf32)
+      const char* sp = getenv("SNU_SPLIT");
+      split_bf16_ = sp && (sp[0] == 'b' || sp[0] == 'B');
       // SNU_DMMA=0: FP64 GEMMs on the SIMT kernel instead of mma.sync f64
       const char* dm = getenv("SNU_DMMA");
       use_dmma_ = !(dm && dm[0] == '0');
+      // SNU_TC_WIDTH=64 or 128: every tensor-core batch at that tile width
       const char* tw = getenv("SNU_TC_WIDTH");
       force_width_ = tw ? (atoi(tw) == 64 ? 1 : 0) : -1;
       const char* vb = getenv("SNU_VERBOSE");
@@ -279,7 +295,7 @@ class CudaEngine : public Engine {
       // 64^3 workload they measured 0.5 ms slower per factor+solve (the
       // chain through the tree levels, not launches, bounds both)
       const char* sf = getenv("SNU_SOLVE_FUSED");
-      fused_solve_ = sf && sf[0] == '1';
+      fused_solve_ = sf && sf[0] == '1' && !deterministic_;
     }
     {
       int sms = 0;
@@ -1253,16 +1269,19 @@ class CudaEngine : public Engine {
         continue;
       }
       TcProb t;
-      t.m = g.m, t.n = g.n, t.k = g.k, t.kpad = (g.k + TC_BK - 1) / TC_BK * TC_BK;
+      // (K rounded up to one 128-byte row of a tile: 32 tf32 / 64 bf16)
+      const int kbe = split_bf16_ ? 64 : 32;
+      const int64_t esz = split_bf16_ ? 2 : 4;
+      t.m = g.m, t.n = g.n, t.k = g.k, t.kpad = (g.k + kbe - 1) / kbe * kbe;
       t.a = g.a, t.b = g.b, t.c = g.c;
       t.lda = g.lda, t.ldb = g.ldb, t.ldc = g.ldc;
       t.pc = g.pc, t.rel = g.rel, t.pld = g.pld, t.mode = g.pad;
-      t.apack = apos;
-      apos += (int64_t)g.m * 3 * t.kpad;
-      apos = (apos + 63) / 64 * 64;
+      t.apack = apos;  // (bytes)
+      apos += (int64_t)g.m * 3 * t.kpad * esz;
+      apos = (apos + 255) / 256 * 256;
       t.bpack = apos;
-      apos += (int64_t)g.n * 3 * t.kpad;
-      apos = (apos + 63) / 64 * 64;
+      apos += (int64_t)g.n * 3 * t.kpad * esz;
+      apos = (apos + 255) / 256 * 256;
       gb.tc_host.push_back(t);
       gb.tc_maxm = std::max(gb.tc_maxm, g.m);
       gb.tc_maxn = std::max(gb.tc_maxn, g.n);
@@ -1303,12 +1322,15 @@ class CudaEngine : public Engine {
       for (size_t k = 0; k < np; k++) {
         const TcProb& t = gb->tc_host[k];
         const cuuint64_t kk = 3 * (cuuint64_t)t.kpad;
+        const CUtensorMapDataType dt = split_bf16_
+                                           ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                           : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        const cuuint32_t kbe = split_bf16_ ? 64 : 32;  // one 128-byte row
         cuuint64_t dimA[2] = {kk, (cuuint64_t)t.m}, dimB[2] = {kk, (cuuint64_t)t.n};
-        cuuint64_t stride[1] = {kk * sizeof(float)};
-        cuuint32_t boxA[2] = {TC_BK, TC_BM};
+        cuuint64_t stride[1] = {kk * (split_bf16_ ? 2 : 4)};
+        cuuint32_t boxA[2] = {kbe, TC_BM};
         cuuint32_t es[2] = {1, 1};
-        CUresult r1 = enc(&am[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                          d_pack_ + t.apack, dimA, stride, boxA, es,
+        CUresult r1 = enc(&am[k], dt, 2, d_pack_ + t.apack, dimA, stride, boxA, es,
                           CU_TENSOR_MAP_INTERLEAVE_NONE,
                           CU_TENSOR_MAP_SWIZZLE_128B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1320,9 +1342,9 @@ class CudaEngine : public Engine {
         const int tm = (t.m + TC_BM - 1) / TC_BM;
         for (int w = 0; w < 2; w++) {
           const int bn = w ? 64 : 128;
-          cuuint32_t boxB[2] = {TC_BK, (cuuint32_t)bn};
-          CUresult r2 = enc(&bm[w][k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                            d_pack_ + t.bpack, dimB, stride, boxB, es,
+          cuuint32_t boxB[2] = {kbe, (cuuint32_t)bn};
+          CUresult r2 = enc(&bm[w][k], dt, 2, d_pack_ + t.bpack, dimB, stride,
+                            boxB, es,
                             CU_TENSOR_MAP_INTERLEAVE_NONE,
                             CU_TENSOR_MAP_SWIZZLE_128B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1562,18 +1584,25 @@ class CudaEngine : public Engine {
       for (int f = L.f0; f < L.f1; f++)
         if (inset(f)) L.solve_elems += fp.fronts[f].p + fp.fronts[f].q;
       std::vector<EaTask> kids;
+      L.ea_kids_r.assign(mc, nullptr);
+      L.nea_kids_r.assign(mc, 0);
       for (int r = 0; r < mc; r++) {
         int b0 = fp.ea_ptr[(size_t)l * mc + r], b1 = fp.ea_ptr[(size_t)l * mc + r + 1];
-        std::vector<EaTask> tasks;
+        std::vector<EaTask> tasks, kr;
         for (int k = b0; k < b1; k++) {
           int c = fp.ea_child[k];
           if (!inset(c)) continue;
-          for (int i0 = 0; i0 < fp.fronts[c].q; i0 += 256) kids.push_back({c, i0});
+          for (int i0 = 0; i0 < fp.fronts[c].q; i0 += 256) {
+            kids.push_back({c, i0});
+            kr.push_back({c, i0});
+          }
           for (int j = 0; j < fp.fronts[c].q; j++) tasks.push_back({c, j});
           L.ea_elems[r] += (double)fp.fronts[c].q * fp.fronts[c].q;
         }
         L.nea[r] = (int)tasks.size();
         if (!tasks.empty() && (rc = upload(L.ea[r], tasks))) return rc;
+        L.nea_kids_r[r] = (int)kr.size();
+        if (!kr.empty() && (rc = upload(L.ea_kids_r[r], kr))) return rc;
       }
       L.nea_kids = (int)kids.size();
       if (!kids.empty() && (rc = upload(L.ea_kids, kids))) return rc;
@@ -1648,9 +1677,11 @@ class CudaEngine : public Engine {
         GemmProb g{fi.q, fi.q, fi.p, fi.ld, fi.ld, fi.ld, o + fi.p,
                    o + fi.p * ld, o + fi.p + fi.p * ld};
         const FrontInfo& par = fp.fronts[fi.parent];
-        g.pc = par.offset;
-        g.pld = par.ld;
-        g.rel = fi.rel_offset;
+        if (!deterministic_) {  // (else F22 in place, then k_extend_add)
+          g.pc = par.offset;
+          g.pld = par.ld;
+          g.rel = fi.rel_offset;
+        }
         f22.push_back(g);
       }
       if ((rc = gemm_batch(f22, L.f22))) return rc;
@@ -1735,12 +1766,16 @@ class CudaEngine : public Engine {
         for (int c = nc - 1; c >= 0; c--) wb.push_back({f, c, 0});
         L.diag_elems += 0.5 * fi.p * (fi.p + 1.0);
         if (fi.q == 0) continue;
+        // (deterministic mode: one task per row chunk over every column
+        // chunk, kchunk -1, so each row has one writer)
+        const int nbl = deterministic_ ? 1 : (fi.p + GEMV_K - 1) / GEMV_K;
+        const int nbq = deterministic_ ? 1 : (fi.q + GEMV_K - 1) / GEMV_K;
         for (int a = 0; a < (fi.q + GEMV_ROWS - 1) / GEMV_ROWS; a++)
-          for (int b = 0; b < (fi.p + GEMV_K - 1) / GEMV_K; b++)
-            gl.push_back({f, a, b});
+          for (int b = 0; b < nbl; b++)
+            gl.push_back({f, a, deterministic_ ? -1 : b});
         for (int a = 0; a < (fi.p + GEMV_ROWS - 1) / GEMV_ROWS; a++)
-          for (int b = 0; b < (fi.q + GEMV_K - 1) / GEMV_K; b++)
-            gq.push_back({f, a, b});
+          for (int b = 0; b < nbq; b++)
+            gq.push_back({f, a, deterministic_ ? -1 : b});
         L.gq_elems += (double)fi.p * fi.q;
       }
       L.nwf = (int)wf.size();
@@ -1820,16 +1855,45 @@ class CudaEngine : public Engine {
   int factor_gemm(const GemmBatch& gb, double* F, cudaStream_t st, int fam) {
     return launch_gemm<double>(gb, F, F, F, 0, st, fam);
   }
+  // One tensor-core GEMM launch of a batch: persistent or one CTA per tile,
+  // tile width 128 (w 0) or 64 (w 1), TF32x3 or BF16x3 operands.
+  template <bool BF>
+  void launch_tc(const GemmBatch& gb, int persistent, int w, float* F,
+                 cudaStream_t st) {
+    const int nt = gb.ntct[w];
+    if (persistent && !w)
+      k_gemm_tcp<128, BF><<<std::min(nt, tcp_cap_[0]), TCP_THREADS,
+                            tc_smem_bytes<128>(), st>>>(
+          gb.tct[0], nt, gb.tcp, gb.amaps, gb.bmaps[0], F, d_flags_ + 2, d_rel_);
+    else if (persistent)
+      k_gemm_tcp<64, BF><<<std::min(nt, tcp_cap_[1]), TCP_THREADS,
+                           tc_smem_bytes<64>(), st>>>(
+          gb.tct[1], nt, gb.tcp, gb.amaps, gb.bmaps[1], F, d_flags_ + 2, d_rel_);
+    else if (!w)
+      k_gemm_tc<128, BF><<<nt, 128, tc_smem_bytes<128>(), st>>>(
+          gb.tct[0], gb.tcp, gb.amaps, gb.bmaps[0], F, d_flags_ + 2, d_rel_);
+    else
+      k_gemm_tc<64, BF><<<nt, 128, tc_smem_bytes<64>(), st>>>(
+          gb.tct[1], gb.tcp, gb.amaps, gb.bmaps[1], F, d_flags_ + 2, d_rel_);
+  }
+
   int factor_gemm(const GemmBatch& gb, float* F, cudaStream_t st, int fam) {
     if (gb.ntiles == 0) return ENG_OK;
     if (!use_tc_ || gb.ntcp == 0) return launch_gemm<float>(gb, F, F, F, 0, st, fam);
     int pi = prof_begin(fam, st);
     dim3 ga(gb.tc_maxkpad / 32, (gb.tc_maxm + 31) / 32, gb.ntcp);
-    k_tc_pack_a<<<ga, dim3(32, 8), 0, st>>>(gb.tcp, F, d_pack_);
-    CKL();
     dim3 gbp((gb.tc_maxn + 7) / 8, gb.ntcp);
-    k_tc_pack_b<<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
-    CKL();
+    if (split_bf16_) {
+      k_tc_pack_a<true><<<ga, dim3(32, 8), 0, st>>>(gb.tcp, F, d_pack_);
+      CKL();
+      k_tc_pack_b<true><<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
+      CKL();
+    } else {
+      k_tc_pack_a<false><<<ga, dim3(32, 8), 0, st>>>(gb.tcp, F, d_pack_);
+      CKL();
+      k_tc_pack_b<false><<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
+      CKL();
+    }
     const int variant =
         (force_tcp_ >= 0 ? force_tcp_ : (gb.variant & 1)) |
         ((force_width_ >= 0 ? force_width_ : (gb.variant >> 1) & 1) << 1);
@@ -1844,23 +1908,10 @@ class CudaEngine : public Engine {
       CK(cudaEventRecord(tune_events_[te], st));
     }
     const int w = (variant >> 1) & 1;  // tile width 128 or 64
-    const int nt = gb.ntct[w];
-    if ((variant & 1) && !w)  // persistent, warp-specialised
-      k_gemm_tcp<128><<<std::min(nt, tcp_cap_[0]), TCP_THREADS,
-                        tc_smem_bytes<128>(), st>>>(gb.tct[0], nt, gb.tcp,
-                                                    gb.amaps, gb.bmaps[0], F,
-                                                    d_flags_ + 2, d_rel_);
-    else if (variant & 1)
-      k_gemm_tcp<64><<<std::min(nt, tcp_cap_[1]), TCP_THREADS,
-                       tc_smem_bytes<64>(), st>>>(gb.tct[1], nt, gb.tcp,
-                                                  gb.amaps, gb.bmaps[1], F,
-                                                  d_flags_ + 2, d_rel_);
-    else if (!w)
-      k_gemm_tc<128><<<nt, 128, tc_smem_bytes<128>(), st>>>(
-          gb.tct[0], gb.tcp, gb.amaps, gb.bmaps[0], F, d_flags_ + 2, d_rel_);
+    if (split_bf16_)
+      launch_tc<true>(gb, variant & 1, w, F, st);
     else
-      k_gemm_tc<64><<<nt, 128, tc_smem_bytes<64>(), st>>>(
-          gb.tct[1], gb.tcp, gb.amaps, gb.bmaps[1], F, d_flags_ + 2, d_rel_);
+      launch_tc<false>(gb, variant & 1, w, F, st);
     if (te >= 0) {
       CK(cudaEventRecord(tune_events_[te + 1], st));
       tune_rec_.push_back({(const GemmBatch*)&gb, te});
@@ -1903,6 +1954,17 @@ class CudaEngine : public Engine {
       LevelSched& L = lvs[l];
       cur_level_ = l;
       int pi;
+      if (deterministic_) {
+        // the children's update matrices (F22 in place) into this level's
+        // fronts, one launch per child rank: a fixed order of additions
+        for (size_t r = 0; r < L.nea.size(); r++)
+          if (L.nea[r]) {
+            pi = prof_begin(KF_EXTEND_ADD, st);
+            k_extend_add<T><<<L.nea[r], 256, 0, st>>>(L.ea[r], d_fr_, d_rel_, F);
+            CKL();
+            prof_end(pi, KF_EXTEND_ADD, st, L.ea_elems[r], L.ea_elems[r] * 3 * es);
+          }
+      }
       if (use_block_) {
         for (const OuterBlock& O : L.ob) {
           if (sizeof(T) == 4 && O.tc) {
@@ -2103,7 +2165,14 @@ class CudaEngine : public Engine {
                                                        B, ldb, nrhs, W);
           CKL();
         }
-        if (L.nea_kids) {
+        if (deterministic_) {
+          for (size_t r = 0; r < L.nea_kids_r.size(); r++)
+            if (L.nea_kids_r[r]) {
+              k_solve_ea<T><<<L.nea_kids_r[r], 256, 0, st>>>(
+                  L.ea_kids_r[r], d_fr_, d_rel_, nrhs, W);
+              CKL();
+            }
+        } else if (L.nea_kids) {
           k_solve_ea<T><<<L.nea_kids, 256, 0, st>>>(L.ea_kids, d_fr_, d_rel_,
                                                     nrhs, W);
           CKL();
@@ -2457,7 +2526,7 @@ class CudaEngine : public Engine {
   // co-resident grid size of each pivot-block sweep kernel
   std::map<const void*, int> coop_cap_;
   // tensor-core GEMM workspace (packed split operands) and its batches
-  float* d_pack_ = nullptr;
+  unsigned char* d_pack_ = nullptr;  // split operands (bytes)
   int64_t pack_need_ = 0;
   std::vector<GemmBatch*> tc_batches_;
   bool use_tc_ = true;
@@ -2487,6 +2556,8 @@ class CudaEngine : public Engine {
   int force_tcp_ = -1;  // tensor-core kernel variant forced (-1: per batch)
   int force_width_ = -1;  // tensor-core tile width forced (0: 128, 1: 64)
   bool use_dmma_ = true;  // FP64 GEMMs on the FP64 tensor cores
+  bool split_bf16_ = false;  // BF16x3 split of the FP32 GEMMs (else TF32x3)
+  bool deterministic_ = false;  // fixed-order reductions (SNU_DETERMINISTIC)
   int tcp_cap_[2] = {148, 148};  // persistent grid per tile width
   // autotuner of the tensor-core kernel variant per GEMM batch
   bool autotune_ = false, tuned_ = false, tuning_ = false;

@@ -356,7 +356,9 @@ __global__ void k_bwd_init(const int* __restrict__ list,
 constexpr int GEMV_ROWS = 64, GEMV_K = 256;
 
 // Off-diagonal products of the sweeps, one (64-row, 256-column) block per
-// CTA; the column blocks of a front add into W with atomics.
+// CTA; the column blocks of a front add into W with atomics.  kchunk -1:
+// the CTA runs over every column block itself, so each row of W has one
+// writer (the bit-reproducible schedule).
 //   FWD:  W[p + i] -= L21[i, :] Y        (i < q, over the p pivot columns)
 //   !FWD: W[i]     -= U12[i, :] W[p:dim] (i < p, over the q update columns)
 template <typename T, int R, bool FWD>
@@ -377,7 +379,9 @@ __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
   const int dim = f.p + f.q;
   const int nrows = FWD ? f.q : f.p, nk = FWD ? f.p : f.q;
   const int i = t.chunk * GEMV_ROWS + (threadIdx.x & 63), g = threadIdx.x >> 6;
-  const int kc0 = t.kchunk * GEMV_K, kc1 = min(nk, kc0 + GEMV_K);
+  const int nkb = (nk + GEMV_K - 1) / GEMV_K;
+  const int kb0 = t.kchunk < 0 ? 0 : t.kchunk,
+            kb1 = t.kchunk < 0 ? nkb : t.kchunk + 1;
   T* Wf = W + f.w_off * nrhs;
   // source vector (ld lds) and the operand block's first element
   const T* src = FWD ? Y + f.y_off * nrhs : Wf + f.p;
@@ -386,32 +390,35 @@ __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
   T* dst = FWD ? Wf + f.p : Wf;
   for (int r0 = 0; r0 < nrhs; r0 += R) {
     const int nr = min(R, nrhs - r0);
-    __syncthreads();  // the previous pass's reduction is read
-    for (int e = threadIdx.x; e < GEMV_K * R; e += blockDim.x) {
-      const int k = e % GEMV_K, r = e / GEMV_K;
-      ys[k][r] = (kc0 + k < kc1 && r < nr)
-                     ? src[kc0 + k + (int64_t)(r0 + r) * lds]
-                     : (T)0;
-    }
-    __syncthreads();
     T acc[R];
 #pragma unroll
     for (int r = 0; r < R; r++) acc[r] = (T)0;
-    if (i < nrows) {
-      constexpr int UB = R <= 4 ? 8 : (R <= 8 ? 4 : 2);  // loads in flight
-      for (int k0 = kc0 + g; k0 < kc1; k0 += 4 * UB) {
-        T av[UB], wv[UB][R];
+    for (int kb = kb0; kb < kb1; kb++) {
+      const int kc0 = kb * GEMV_K, kc1 = min(nk, kc0 + GEMV_K);
+      __syncthreads();  // the previous pass's ys / reduction is read
+      for (int e = threadIdx.x; e < GEMV_K * R; e += blockDim.x) {
+        const int k = e % GEMV_K, r = e / GEMV_K;
+        ys[k][r] = (kc0 + k < kc1 && r < nr)
+                       ? src[kc0 + k + (int64_t)(r0 + r) * lds]
+                       : (T)0;
+      }
+      __syncthreads();
+      if (i < nrows) {
+        constexpr int UB = R <= 4 ? 8 : (R <= 8 ? 4 : 2);  // loads in flight
+        for (int k0 = kc0 + g; k0 < kc1; k0 += 4 * UB) {
+          T av[UB], wv[UB][R];
 #pragma unroll
-        for (int u = 0; u < UB; u++) {
-          const int k = k0 + 4 * u;
-          av[u] = k < kc1 ? a[(int64_t)k * f.ld] : (T)0;
+          for (int u = 0; u < UB; u++) {
+            const int k = k0 + 4 * u;
+            av[u] = k < kc1 ? a[(int64_t)k * f.ld] : (T)0;
 #pragma unroll
-          for (int r = 0; r < R; r++) wv[u][r] = ys[min(k, kc1 - 1) - kc0][r];
+            for (int r = 0; r < R; r++) wv[u][r] = ys[min(k, kc1 - 1) - kc0][r];
+          }
+#pragma unroll
+          for (int u = 0; u < UB; u++)
+#pragma unroll
+            for (int r = 0; r < R; r++) acc[r] += av[u] * wv[u][r];
         }
-#pragma unroll
-        for (int u = 0; u < UB; u++)
-#pragma unroll
-          for (int r = 0; r < R; r++) acc[r] += av[u] * wv[u][r];
       }
     }
     __syncthreads();  // ys is read

@@ -227,15 +227,19 @@ def test_autotuned_factorization_matches(gpu, tmp_path):
                                  ("SNU_TC_PERSIST", "1"), ("SNU_TC_PERSIST", "0"),
                                  ("SNU_GRAPHS", "0"), ("SNU_TC_PANEL", "0"),
                                  ("SNU_TC_PANEL", "1"), ("SNU_SOLVE_FUSED", "1"),
-                                 ("SNU_TC_WIDTH", "64"), ("SNU_DMMA", "0")])
+                                 ("SNU_TC_WIDTH", "64"), ("SNU_DMMA", "0"),
+                                 ("SNU_SPLIT", "bf16"),
+                                 ("SNU_DETERMINISTIC", "1")])
 def test_alternative_paths_match(gpu, monkeypatch, env):
     # the paths behind the engine switches (read when an engine is made):
     # per-step panels instead of the fused outer-block kernel, SIMT instead
     # of tensor-core FP32 GEMMs, the persistent GEMM forced on or off, no
     # CUDA graph, the FP32 panel products on the tensor cores for no level
     # or for every level, the whole-tree solve sweeps instead of the
-    # level-by-level ones, 64-wide tensor-core tiles -- each must reproduce
-    # the oracle like the default
+    # level-by-level ones, 64-wide tensor-core tiles, SIMT FP64 GEMMs
+    # instead of mma.sync f64, the BF16x3 split instead of TF32x3, the
+    # fixed-order (bit-reproducible) reductions -- each must reproduce the
+    # oracle like the default
     monkeypatch.setenv(*env)
     rng = np.random.default_rng(41)
     rp, ci, v = _random_unsym(rng, 33, 30, 80)
@@ -330,3 +334,26 @@ def test_fp64_fallback_when_refinement_stops(gpu):
     x2 = s.solve(B[:, 0])
     assert s.stats()["fp64_fallback"] == 1
     _close(x2, x, 1e-11, "second solve")
+
+
+@pytest.mark.parametrize("precision", [snu.FP64, snu.FP32_IR])
+def test_deterministic_mode_is_bit_reproducible(gpu, monkeypatch, precision):
+    # SNU_DETERMINISTIC=1: sibling updates enter their parent in a fixed
+    # order and the solve's products have one writer per row, so two
+    # handles (and two factorizations of one handle) give identical bits
+    monkeypatch.setenv("SNU_DETERMINISTIC", "1")
+    rng = np.random.default_rng(43)
+    cases = [_random_unsym(rng, 40, 37, 90), generators.convdiff3d(20)]
+    for rp, ci, v in cases:
+        n = len(rp) - 1
+        B = generators.rhs(n, 3, seed=12)
+        runs = []
+        for _ in range(2):
+            s = snu.Solver(nleaves=8, precision=precision).construct(rp, ci, v)
+            X1 = s.factorize().solve(B)
+            X2 = s.factorize().solve(B)
+            assert np.array_equal(X1, X2)
+            runs.append(X1)
+            for r in range(3):
+                assert rel_resid(rp, ci, v, X1[:, r], B[:, r]) <= 1e-10
+        assert np.array_equal(runs[0], runs[1])
