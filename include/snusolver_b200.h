@@ -71,7 +71,14 @@ typedef struct snu_opts {
                            default 10 */
   int device;           /* CUDA device ordinal; default 0 */
   int64_t mem_budget;   /* bytes of device memory the handle may hold; 0 = no limit */
-  int reserved[8];
+  double fp64_growth;   /* FP32_IR, when refinement stagnates: the fronts whose
+                           largest |L| entry (no-pivot growth) exceeds this are
+                           refactored in FP64 together with their ancestors,
+                           the other fronts keep their FP32 factors (promoted),
+                           and refinement goes on with FP64 solves; no front
+                           above it, or 0: the whole matrix in FP64.
+                           default 1e3 */
+  int reserved[6];
 } snu_opts;
 
 typedef struct snu_stats {
@@ -88,7 +95,9 @@ typedef struct snu_stats {
   int tiny_pivots;          /* leaf pivots replaced by +-pivot_eps */
   int factor_launches;      /* kernels of the last factorization */
   int solve_launches;       /* kernels of the last solve (all chunks) */
-  int reserved[5];
+  int fp64_fronts;          /* fronts the last solve refactored in FP64 (all of
+                               them for a whole-matrix fallback; 0: none) */
+  int reserved[4];
 } snu_stats;
 
 typedef struct snu_handle snu_handle;

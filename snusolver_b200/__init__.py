@@ -49,7 +49,8 @@ class _Opts(C.Structure):
     _fields_ = [("nleaves", C.c_int), ("precision", C.c_int),
                 ("pivot_eps", C.c_double), ("ir_tol", C.c_double),
                 ("ir_max_iter", C.c_int), ("device", C.c_int),
-                ("mem_budget", C.c_int64), ("reserved", C.c_int * 8)]
+                ("mem_budget", C.c_int64), ("fp64_growth", C.c_double),
+                ("reserved", C.c_int * 6)]
 
 
 class _Stats(C.Structure):
@@ -61,7 +62,7 @@ class _Stats(C.Structure):
                 ("ir_iters", C.c_int), ("fp64_fallback", C.c_int),
                 ("backward_error", C.c_double), ("tiny_pivots", C.c_int),
                 ("factor_launches", C.c_int), ("solve_launches", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("fp64_fronts", C.c_int), ("reserved", C.c_int * 4)]
 
 
 class _KStat(C.Structure):
@@ -156,13 +157,15 @@ class Solver:
     """One handle of the C-ABI: plan (host) + factors (device)."""
 
     def __init__(self, nleaves=8, precision=FP64, pivot_eps=1e-15,
-                 ir_tol=1e-10, ir_max_iter=10, device=0, mem_budget=0):
+                 ir_tol=1e-10, ir_max_iter=10, device=0, mem_budget=0,
+                 fp64_growth=1e3):
         self._lib = load_library()
         o = _Opts()
         self._lib.snu_default_opts(C.byref(o))
         o.nleaves, o.precision = nleaves, precision
         o.pivot_eps, o.ir_tol, o.ir_max_iter = pivot_eps, ir_tol, ir_max_iter
         o.device, o.mem_budget = device, mem_budget
+        o.fp64_growth = fp64_growth
         h = C.c_void_p()
         st = self._lib.snu_create(C.byref(h), C.byref(o))
         if st:

@@ -121,7 +121,7 @@ snu_status solve_pieces(snu_handle* h, const std::vector<SolvePiece>& pieces) {
   // copies on the engine's stream, so they are ordered with its kernels
   cudaStream_t st = (cudaStream_t)h->eng->stream();
   double be = 0, secs = 0;
-  int iters = 0, fb = 0;
+  int iters = 0, fb = 0, nf64 = 0;
   snu_status result = SNU_OK;
   for (int c0 = 0; c0 < nrhs; c0 += chunk) {
     const int nc = std::min(chunk, nrhs - c0);
@@ -138,6 +138,7 @@ snu_status solve_pieces(snu_handle* h, const std::vector<SolvePiece>& pieces) {
     be = std::max(be, h->stats.backward_error);
     iters = std::max(iters, h->stats.ir_iters);
     fb |= h->stats.fp64_fallback;
+    nf64 = std::max(nf64, h->stats.fp64_fronts);
     secs += h->stats.solve_s;
     for (int r = 0; r < nc; r++)
       if (cudaMemcpyAsync(cols[c0 + r].second, dX + (size_t)r * n,
@@ -150,6 +151,7 @@ snu_status solve_pieces(snu_handle* h, const std::vector<SolvePiece>& pieces) {
   h->stats.backward_error = be;
   h->stats.ir_iters = iters;
   h->stats.fp64_fallback = fb;
+  h->stats.fp64_fronts = nf64;
   h->stats.solve_s = secs;
   return result;
 }
@@ -181,6 +183,7 @@ SNU_API void snu_default_opts(snu_opts* o) {
   o->ir_max_iter = 10;
   o->device = 0;
   o->mem_budget = 0;
+  o->fp64_growth = 1e3;
 }
 
 SNU_API snu_status snu_create(snu_handle** out, const snu_opts* opts) {
@@ -193,7 +196,8 @@ SNU_API snu_status snu_create(snu_handle** out, const snu_opts* opts) {
     return fail(nullptr, SNU_EINVAL, "nleaves must be a power of two in 2..512");
   if (o.precision != SNU_FP64 && o.precision != SNU_FP32_IR)
     return fail(nullptr, SNU_EINVAL, "unknown precision");
-  if (!(o.pivot_eps >= 0) || !(o.ir_tol > 0) || o.ir_max_iter < 0)
+  if (!(o.pivot_eps >= 0) || !(o.ir_tol > 0) || o.ir_max_iter < 0 ||
+      !(o.fp64_growth >= 0))
     return fail(nullptr, SNU_EINVAL, "bad tolerance options");
   snu_handle* h = new (std::nothrow) snu_handle();
   if (!h) return fail(nullptr, SNU_ENOMEM, "out of host memory");
@@ -446,6 +450,7 @@ SNU_API snu_status snu_solve_device(snu_handle* h, const double* dB,
   h->stats.solve_s = rep.seconds;
   h->stats.ir_iters = rep.ir_iters;
   h->stats.fp64_fallback = rep.fp64_fallback;
+  h->stats.fp64_fronts = rep.fp64_fronts;
   h->stats.backward_error = rep.backward_error;
   h->stats.device_bytes = h->eng->device_bytes();
   {
@@ -475,6 +480,7 @@ SNU_API snu_status snu_solve_device_noalloc(snu_handle* h, const double* dB,
   h->stats.solve_s = rep.seconds;
   h->stats.ir_iters = rep.ir_iters;
   h->stats.fp64_fallback = 0;  // this path has no FP64 fallback
+  h->stats.fp64_fronts = 0;
   h->stats.backward_error = rep.backward_error;
   {
     int64_t fl = 0, sl = 0;
@@ -824,6 +830,7 @@ snu_status finish_construct(snu_handle* h, const double* vals, bool have_plan) {
   eo.pivot_eps = h->opts.pivot_eps;
   eo.ir_tol = h->opts.ir_tol;
   eo.ir_max_iter = h->opts.ir_max_iter;
+  eo.fp64_growth = h->opts.fp64_growth;
   eo.mem_budget = h->opts.mem_budget;
   eo.dist_rank = h->dist_rank;
   eo.dist_world = h->dist_world;

@@ -1,17 +1,22 @@
-// Tensor-core (tcgen05, kind::tf32) batched GEMM for the FP32 path:
-// C -= A B with C column-major in the front arena.
+// Tensor-core (tcgen05) batched GEMM for the FP32 path: C -= A B with C
+// column-major in the front arena.
 //
-// FP32 accuracy from TF32 tensor cores: every operand x is split into
-// hi = tf32(x) and lo = tf32(x - hi), and A B is formed as
-// A_hi B_hi + A_hi B_lo + A_lo B_hi (the lo*lo term is below FP32 rounding).
+// FP32 operands on low-precision tensor cores through a three-product
+// split: every operand x is split into hi + lo and A B is formed as
+// A_hi B_hi + A_hi B_lo + A_lo B_hi with FP32 accumulation in TMEM.  Two
+// splits, chosen per batch: TF32x3 (hi = tf32(x), lo = tf32(x - hi),
+// kind::tf32: FP32-level accuracy) and BF16x3 (bf16 hi and lo, kind::f16
+// with both operands bf16: about 2^-16 relative per product, twice the MMA
+// rate and half the operand bytes; FP64 refinement recovers the rest).
 // A pack kernel writes the three products as one GEMM of depth 3*kpad:
 // A' = [A_hi | A_hi | A_lo] and B' = [B_hi ; B_lo ; B_hi], both K-major
-// (row-major in K), kpad = k rounded up to 32.  The GEMM kernel then runs a
-// plain TF32 GEMM: TMA loads 128 x 32 (A') and BN x 32 (B') fp32 tiles with
-// 128-byte swizzle into a STAGES-deep shared-memory ring, one thread issues
-// tcgen05.mma (M=128, N=BN, K=8) into a TMEM accumulator, and the four warps
-// read the accumulator back with tcgen05.ld and subtract it from C (or,
-// for the panel products, store it: C = A B).
+// (row-major in K), kpad = k rounded up to one 128-byte row (32 tf32, 64
+// bf16).  The GEMM kernel then runs a plain GEMM: TMA loads 128 x 128-byte
+// (A') and BN x 128-byte (B') tiles with 128-byte swizzle into a
+// STAGES-deep shared-memory ring, one thread issues tcgen05.mma (M=128,
+// N=BN) into a TMEM accumulator, and the four warps read the accumulator
+// back with tcgen05.ld and subtract it from C (or, for the panel products,
+// store it: C = A B).
 //
 // Every wait on an mbarrier is bounded; on timeout the kernel records the
 // failure in err[0], lets its in-flight work drain (bounded), frees its TMEM
@@ -27,7 +32,8 @@ constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_STAGES = 3;
 constexpr long TC_SPIN_LIMIT = 1L << 24;
 
 struct TcProb {
-  int m, n, k, kpad;
+  int m, n, k;
+  int kpad, kpadb;  // k rounded up to 32 (TF32 split) and to 64 (BF16 split)
   int64_t a, b, c;  // element offsets of A, B, C in the front arena
   int lda, ldb, ldc;
   int64_t apack, bpack;  // byte offsets of A', B' in the pack workspace
@@ -58,6 +64,7 @@ template <>
 struct Split<false> {
   typedef float E;
   static constexpr int KB = 32;  // elements per 128-byte row of a tile
+  __device__ __forceinline__ static int kpad(const TcProb& p) { return p.kpad; }
   __device__ __forceinline__ static void apply(float v, E& hi, E& lo) {
     hi = tf32_rna(v);
     lo = tf32_rna(v - hi);
@@ -67,6 +74,7 @@ template <>
 struct Split<true> {
   typedef __nv_bfloat16 E;
   static constexpr int KB = 64;
+  __device__ __forceinline__ static int kpad(const TcProb& p) { return p.kpadb; }
   __device__ __forceinline__ static void apply(float v, E& hi, E& lo) {
     hi = __float2bfloat16_rn(v);
     lo = __float2bfloat16_rn(v - __bfloat162float(hi));
@@ -83,8 +91,9 @@ __global__ void k_tc_pack_a(const TcProb* __restrict__ probs,
   typedef typename Split<BF>::E E;
   __shared__ float t[32][33];
   const TcProb pr = probs[blockIdx.z];
+  const int kp = Split<BF>::kpad(pr);
   const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
-  if (r0 >= pr.m || c0 >= pr.kpad) return;
+  if (r0 >= pr.m || c0 >= kp) return;
   const float* A = F + pr.a;
   for (int cc = threadIdx.y; cc < 32; cc += 8) {
     int r = r0 + threadIdx.x, c = c0 + cc;
@@ -92,7 +101,7 @@ __global__ void k_tc_pack_a(const TcProb* __restrict__ probs,
   }
   __syncthreads();
   E* out = reinterpret_cast<E*>(P + pr.apack);
-  const int64_t kk = 3 * (int64_t)pr.kpad;
+  const int64_t kk = 3 * (int64_t)kp;
   for (int rr = threadIdx.y; rr < 32; rr += 8) {
     int r = r0 + rr, c = c0 + threadIdx.x;
     if (r >= pr.m) continue;
@@ -100,8 +109,8 @@ __global__ void k_tc_pack_a(const TcProb* __restrict__ probs,
     Split<BF>::apply(t[threadIdx.x][rr], hi, lo);
     E* row = out + r * kk;
     row[c] = hi;
-    row[pr.kpad + c] = hi;
-    row[2 * pr.kpad + c] = lo;
+    row[kp + c] = hi;
+    row[2 * kp + c] = lo;
   }
 }
 
@@ -117,13 +126,14 @@ __global__ void k_tc_pack_b(const TcProb* __restrict__ probs,
   const int c = blockIdx.x * 8 + warp;
   if (c >= pr.n) return;
   const float* B = F + pr.b + (int64_t)c * pr.ldb;
-  E* row = reinterpret_cast<E*>(P + pr.bpack) + (int64_t)c * 3 * pr.kpad;
-  for (int kk = lane; kk < pr.kpad; kk += 32) {
+  const int kp = Split<BF>::kpad(pr);
+  E* row = reinterpret_cast<E*>(P + pr.bpack) + (int64_t)c * 3 * kp;
+  for (int kk = lane; kk < kp; kk += 32) {
     E hi, lo;
     Split<BF>::apply(kk < pr.k ? B[kk] : 0.f, hi, lo);
     row[kk] = hi;
-    row[pr.kpad + kk] = lo;
-    row[2 * pr.kpad + kk] = hi;
+    row[kp + kk] = lo;
+    row[2 * kp + kk] = hi;
   }
 }
 
@@ -261,7 +271,7 @@ __global__ void __launch_bounds__(128, 1)
   const TcTile tl = tiles[blockIdx.x];
   const TcProb pr = probs[tl.prob];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nk = 3 * pr.kpad / Split<BF>::KB;
+  const int nk = 3 * Split<BF>::kpad(pr) / Split<BF>::KB;
 
   if (threadIdx.x == 0) {
     failed_s = 0;
@@ -472,7 +482,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
       const TcProb pr = probs[tl.prob];
       const CUtensorMap* am = amaps + tl.prob;
       const CUtensorMap* bm = bmaps + tl.prob;
-      const int nk = 3 * pr.kpad / Split<BF>::KB;
+      const int nk = 3 * Split<BF>::kpad(pr) / Split<BF>::KB;
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g % TC_STAGES;
         if (g >= TC_STAGES &&
@@ -502,7 +512,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const TcProb pr = probs[tiles[t].prob];
-      const int nk = 3 * pr.kpad / Split<BF>::KB;
+      const int nk = 3 * Split<BF>::kpad(pr) / Split<BF>::KB;
       const uint32_t d = tmem + (uint32_t)(a * BN);
       bool ok = true;
       for (int kb = 0; kb < nk; kb++, g++) {

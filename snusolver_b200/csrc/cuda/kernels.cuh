@@ -431,4 +431,47 @@ __global__ void k_copy_cols(int n, int nrhs, const double* __restrict__ X,
   Y[i + (int64_t)r * ldy] = X[i + (int64_t)r * ldx];
 }
 
+// ------------------------------------------- FP64 refactor of some fronts
+
+// Largest |L| entry of each front (the multipliers below the diagonal of
+// its pivot columns, L11 and L21): the growth that no-pivot elimination
+// let through, where a small pivot met large entries of its column.  One
+// CTA per (front, 32 pivot columns); a non-finite entry counts as
+// infinite.  out[f] holds float bits (non-negative floats order as
+// unsigned integers) and starts at 0.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_front_lmax(const int2* __restrict__ tasks,
+                 const FrontDev* __restrict__ fr, const T* __restrict__ F,
+                 unsigned* __restrict__ out) {
+  const int2 t = tasks[blockIdx.x];
+  const FrontDev f = fr[t.x];
+  const int dim = f.p + f.q;
+  const int k1 = min(f.p, t.y + 32);
+  float m = 0.f;
+  for (int k = t.y; k < k1; k++) {
+    const T* col = F + f.off + (int64_t)k * f.ld;
+    for (int i = k + 1 + threadIdx.x; i < dim; i += blockDim.x) {
+      const float a = fabsf((float)col[i]);
+      m = (a == a) ? fmaxf(m, a) : INFINITY;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ float wm[8];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < 8; w++) m = fmaxf(m, wm[w]);
+    atomicMax(out + t.x, __float_as_uint(m));
+  }
+}
+
+// D[i] = S[i] (FP32 -> FP64), grid-stride.
+__global__ void k_upcast(const float* __restrict__ S, double* __restrict__ D,
+                         int64_t count) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (; i < count; i += stride) D[i] = (double)S[i];
+}
+
 }  // namespace snu

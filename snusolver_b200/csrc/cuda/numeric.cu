@@ -93,18 +93,19 @@ struct GemmBatch {
   // FP32 path: problems large enough for the tensor cores, and the rest
   std::vector<TcProb> tc_host;
   TcProb* tcp = nullptr;
-  // per tile width (index 0: BN = 128, 1: BN = 64): tiles and B maps
+  // per tile width (index 0: BN = 128, 1: BN = 64): tiles; TMA maps per
+  // split (index 0: TF32x3, 1: BF16x3) of A', and of B' per split and width
   TcTile* tct[2] = {nullptr, nullptr};
-  CUtensorMap* amaps = nullptr;
-  CUtensorMap* bmaps[2] = {nullptr, nullptr};
+  CUtensorMap* amaps[2] = {nullptr, nullptr};
+  CUtensorMap* bmaps[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int ntcp = 0, ntct[2] = {0, 0}, tc_maxm = 0, tc_maxn = 0, tc_maxkpad = 0;
   GemmProb* rprobs = nullptr;  // SIMT remainder of the FP32 path
   GemmTile* rtiles = nullptr;
   int nrtiles = 0;
   // tensor-core kernel variant: bit 0 -- 0 one CTA per tile, 1 persistent
-  // and warp-specialised; bit 1 -- tile width 128 (0) or 64 (1); a
-  // heuristic default (width 128, persistent for a long mean K) unless the
-  // autotuner timed all four
+  // and warp-specialised; bit 1 -- tile width 128 (0) or 64 (1); bit 2 --
+  // TF32x3 (0) or BF16x3 (1) split; a heuristic default (width 128,
+  // persistent for a long mean K, BF16x3) unless the autotuner timed them
   int variant = 0;
   double ktiles = 0;  // sum of kpad over tiles (for the heuristic)
 };
@@ -256,10 +257,13 @@ class CudaEngine : public Engine {
       // child rank) and the solve's products without split-K atomics
       const char* de = getenv("SNU_DETERMINISTIC");
       deterministic_ = de && de[0] == '1';
-      // SNU_SPLIT=bf16: FP32 GEMMs with the BF16x3 split (kind::f16)
-      // instead of TF32x3 (kind::tf32)
+      // SNU_SPLIT=tf32 or bf16: every FP32 tensor-core batch with the
+      // TF32x3 (kind::tf32) or the BF16x3 (kind::f16) split; unset: BF16x3
+      // unless the autotuner picks TF32x3 for a batch
       const char* sp = getenv("SNU_SPLIT");
-      split_bf16_ = sp && (sp[0] == 'b' || sp[0] == 'B');
+      force_split_ = !sp || !sp[0] ? -1
+                     : (sp[0] == 'b' || sp[0] == 'B') ? 1
+                     : (sp[0] == 't' || sp[0] == 'T') ? 0 : -1;
       // SNU_DMMA=0: FP64 GEMMs on the SIMT kernel instead of mma.sync f64
       const char* dm = getenv("SNU_DMMA");
       use_dmma_ = !(dm && dm[0] == '0');
@@ -494,7 +498,7 @@ class CudaEngine : public Engine {
       anorm_seg_[0] = *std::max_element(part.begin(), part.end());
     }
     for (int b = 0; b < nseg_; b++) anorm_ = std::max(anorm_, anorm_seg_[b]);
-    have64_ = have32_ = false;
+    have64_ = have32_ = mixed64_ = false;
     CK(cudaStreamSynchronize(stream_));
     return ENG_OK;
   }
@@ -521,6 +525,7 @@ class CudaEngine : public Engine {
   int factor_run(int precision, int phase, double* seconds) {
     CK(cudaSetDevice(opt_.device));
     int rc;
+    mixed64_ = false;  // (new factors: the promoted copy is stale)
     if (precision == 0) {
       if (!d_F64_ && (rc = alloc(d_F64_, (size_t)arena_))) return rc;
       if (!d_I64_ && (rc = alloc(d_I64_, (size_t)invtot_))) return rc;
@@ -865,12 +870,13 @@ class CudaEngine : public Engine {
 
  private:
   // Picks the tensor-core kernel variant of every FP32 GEMM batch -- one CTA
-  // per tile or persistent, tile width 128 or 64: from the cache file when
-  // it holds this pattern, else by timing four complete factorizations
-  // (every batch with variant 0, 1, 2, then 3; the factorization is
+  // per tile or persistent, tile width 128 or 64, TF32x3 or BF16x3 split
+  // (the split only when SNU_SPLIT does not fix it): from the cache file
+  // when it holds this pattern, else by timing one complete factorization
+  // per variant (every batch with that variant; the factorization is
   // recomputed from the values each time, so nothing is lost) and keeping
-  // the fastest variant per batch.  The choice is baked into the
-  // factorization's CUDA graph.
+  // the fastest variant per batch (its pack and GEMM launches).  The
+  // choice is baked into the factorization's CUDA graph.
   int autotune() {
     tuned_ = true;
     const size_t nb = tc_batches_.size();
@@ -883,16 +889,18 @@ class CudaEngine : public Engine {
         bool hit = false;
         while (fscanf(f, "%63s %65535s", k, v) == 2)
           if (!strcmp(k, keyhex) && strlen(v) == nb) {
-            for (size_t i = 0; i < nb; i++) tc_batches_[i]->variant = v[i] - '0';
+            for (size_t i = 0; i < nb; i++) tc_batches_[i]->variant = (v[i] - '0') & 7;
             hit = true;
           }
         fclose(f);
         if (hit) return ENG_OK;
       }
     }
-    constexpr int NV = 4;  // {one CTA per tile, persistent} x {128, 64}
+    // {one CTA per tile, persistent} x {128, 64} x {TF32x3, BF16x3}
+    constexpr int NV = 8;
     std::vector<double> t(NV * nb, 0.0);
     for (int v = 0; v < NV; v++) {
+      if (force_split_ >= 0 && ((v >> 2) & 1) != force_split_) continue;
       for (GemmBatch* gb : tc_batches_) gb->variant = v;
       tuning_ = true;
       tune_rec_.clear();
@@ -913,9 +921,11 @@ class CudaEngine : public Engine {
     }
     std::string choice(nb, '0');
     for (size_t i = 0; i < nb; i++) {
-      int best = 0;
-      for (int v = 1; v < NV; v++)
-        if (t[NV * i + v] < t[NV * i + best]) best = v;
+      int best = -1;
+      for (int v = 0; v < NV; v++) {
+        if (force_split_ >= 0 && ((v >> 2) & 1) != force_split_) continue;
+        if (best < 0 || t[NV * i + v] < t[NV * i + best]) best = v;
+      }
       tc_batches_[i]->variant = best;
       choice[i] = (char)('0' + best);
     }
@@ -1259,6 +1269,7 @@ class CudaEngine : public Engine {
     int rc;
     if ((rc = upload(gb.probs, probs))) return rc;
     if ((rc = upload(gb.tiles, tiles))) return rc;
+    if (fp64_only_build_) return ENG_OK;  // (FP64 schedules: tiles only)
     // FP32 split
     std::vector<GemmProb> rest;
     int64_t apos = 0;
@@ -1269,23 +1280,25 @@ class CudaEngine : public Engine {
         continue;
       }
       TcProb t;
-      // (K rounded up to one 128-byte row of a tile: 32 tf32 / 64 bf16)
-      const int kbe = split_bf16_ ? 64 : 32;
-      const int64_t esz = split_bf16_ ? 2 : 4;
-      t.m = g.m, t.n = g.n, t.k = g.k, t.kpad = (g.k + kbe - 1) / kbe * kbe;
+      // (K rounded up to one 128-byte row of a tile: 32 tf32 / 64 bf16; the
+      // pack slot holds either split's operands)
+      t.m = g.m, t.n = g.n, t.k = g.k;
+      t.kpad = (g.k + 31) / 32 * 32;
+      t.kpadb = (g.k + 63) / 64 * 64;
+      const int64_t row = 3 * std::max<int64_t>(4 * t.kpad, 2 * t.kpadb);
       t.a = g.a, t.b = g.b, t.c = g.c;
       t.lda = g.lda, t.ldb = g.ldb, t.ldc = g.ldc;
       t.pc = g.pc, t.rel = g.rel, t.pld = g.pld, t.mode = g.pad;
       t.apack = apos;  // (bytes)
-      apos += (int64_t)g.m * 3 * t.kpad * esz;
+      apos += (int64_t)g.m * row;
       apos = (apos + 255) / 256 * 256;
       t.bpack = apos;
-      apos += (int64_t)g.n * 3 * t.kpad * esz;
+      apos += (int64_t)g.n * row;
       apos = (apos + 255) / 256 * 256;
       gb.tc_host.push_back(t);
       gb.tc_maxm = std::max(gb.tc_maxm, g.m);
       gb.tc_maxn = std::max(gb.tc_maxn, g.n);
-      gb.tc_maxkpad = std::max(gb.tc_maxkpad, t.kpad);
+      gb.tc_maxkpad = std::max({gb.tc_maxkpad, t.kpad, t.kpadb});
     }
     pack_need_ = std::max(pack_need_, apos);
     if (!gb.tc_host.empty()) tc_batches_.push_back(&gb);
@@ -1316,43 +1329,50 @@ class CudaEngine : public Engine {
     EncodeTiledFn enc = (EncodeTiledFn)fn;
     for (GemmBatch* gb : tc_batches_) {
       const size_t np = gb->tc_host.size();
-      std::vector<CUtensorMap> am(np), bm[2] = {std::vector<CUtensorMap>(np),
-                                                std::vector<CUtensorMap>(np)};
+      std::vector<CUtensorMap> am[2], bm[2][2];
+      for (int sp = 0; sp < 2; sp++) {
+        am[sp].resize(np);
+        bm[sp][0].resize(np);
+        bm[sp][1].resize(np);
+      }
       std::vector<TcTile> tiles[2];
       for (size_t k = 0; k < np; k++) {
         const TcProb& t = gb->tc_host[k];
-        const cuuint64_t kk = 3 * (cuuint64_t)t.kpad;
-        const CUtensorMapDataType dt = split_bf16_
-                                           ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                           : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-        const cuuint32_t kbe = split_bf16_ ? 64 : 32;  // one 128-byte row
-        cuuint64_t dimA[2] = {kk, (cuuint64_t)t.m}, dimB[2] = {kk, (cuuint64_t)t.n};
-        cuuint64_t stride[1] = {kk * (split_bf16_ ? 2 : 4)};
-        cuuint32_t boxA[2] = {kbe, TC_BM};
-        cuuint32_t es[2] = {1, 1};
-        CUresult r1 = enc(&am[k], dt, 2, d_pack_ + t.apack, dimA, stride, boxA, es,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          CU_TENSOR_MAP_SWIZZLE_128B,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r1 != CUDA_SUCCESS) {
-          err_ = "tensor map encoding failed";
-          return ENG_ECUDA;
-        }
         const int tm = (t.m + TC_BM - 1) / TC_BM;
-        for (int w = 0; w < 2; w++) {
-          const int bn = w ? 64 : 128;
-          cuuint32_t boxB[2] = {kbe, (cuuint32_t)bn};
-          CUresult r2 = enc(&bm[w][k], dt, 2, d_pack_ + t.bpack, dimB, stride,
-                            boxB, es,
-                            CU_TENSOR_MAP_INTERLEAVE_NONE,
+        for (int sp = 0; sp < 2; sp++) {  // TF32x3, BF16x3
+          const cuuint64_t kk = 3 * (cuuint64_t)(sp ? t.kpadb : t.kpad);
+          const CUtensorMapDataType dt = sp ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                            : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+          const cuuint32_t kbe = sp ? 64 : 32;  // one 128-byte row
+          cuuint64_t dimA[2] = {kk, (cuuint64_t)t.m}, dimB[2] = {kk, (cuuint64_t)t.n};
+          cuuint64_t stride[1] = {kk * (sp ? 2 : 4)};
+          cuuint32_t boxA[2] = {kbe, TC_BM};
+          cuuint32_t es[2] = {1, 1};
+          CUresult r1 = enc(&am[sp][k], dt, 2, d_pack_ + t.apack, dimA, stride,
+                            boxA, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                             CU_TENSOR_MAP_SWIZZLE_128B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-          if (r2 != CUDA_SUCCESS) {
+          if (r1 != CUDA_SUCCESS) {
             err_ = "tensor map encoding failed";
             return ENG_ECUDA;
           }
+          for (int w = 0; w < 2; w++) {
+            const int bn = w ? 64 : 128;
+            cuuint32_t boxB[2] = {kbe, (cuuint32_t)bn};
+            CUresult r2 = enc(&bm[sp][w][k], dt, 2, d_pack_ + t.bpack, dimB,
+                              stride, boxB, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r2 != CUDA_SUCCESS) {
+              err_ = "tensor map encoding failed";
+              return ENG_ECUDA;
+            }
+          }
+        }
+        for (int w = 0; w < 2; w++) {
+          const int bn = w ? 64 : 128;
           const int tn = (t.n + bn - 1) / bn;
           if (!w) gb->ktiles += (double)t.kpad * tm * tn;
           for (int b = 0; b < tn; b++)
@@ -1364,13 +1384,17 @@ class CudaEngine : public Engine {
       gb->ntct[1] = (int)tiles[1].size();
       // long K per tile: the persistent kernel hides each epilogue behind
       // the next tile's MMAs; short K: one CTA per tile balances better
-      gb->variant = gb->ktiles / std::max(1, gb->ntct[0]) >= 512 ? 1 : 0;
+      // (the BF16x3 split by default: half the operand bytes and twice
+      // the MMA rate of TF32x3; refinement recovers its 2^-16 products)
+      gb->variant = (gb->ktiles / std::max(1, gb->ntct[0]) >= 512 ? 1 : 0) | 4;
       if ((rc = upload(gb->tcp, gb->tc_host))) return rc;
-      if ((rc = upload(gb->amaps, am))) return rc;
-      for (int w = 0; w < 2; w++) {
-        if ((rc = upload(gb->tct[w], tiles[w]))) return rc;
-        if ((rc = upload(gb->bmaps[w], bm[w]))) return rc;
+      for (int sp = 0; sp < 2; sp++) {
+        if ((rc = upload(gb->amaps[sp], am[sp]))) return rc;
+        for (int w = 0; w < 2; w++)
+          if ((rc = upload(gb->bmaps[sp][w], bm[sp][w]))) return rc;
       }
+      for (int w = 0; w < 2; w++)
+        if ((rc = upload(gb->tct[w], tiles[w]))) return rc;
     }
     return ENG_OK;
   }
@@ -1531,7 +1555,11 @@ class CudaEngine : public Engine {
     invb_base_ = (arena_ + 63) / 64 * 64;
     invb_need_ = 0;
     obc_ = 0;
-    if (opt_.dist_world <= 1) return build_levels(lv_, nullptr);
+    if (opt_.dist_world <= 1) {
+      const int rc = build_levels(lv_, nullptr);
+      obc_main_ = obc_;
+      return rc;
+    }
     // separator-tree distribution: this rank's subtree fronts (phase 1)
     // and the shared top fronts (phase 2, every rank)
     std::vector<char> own(nfronts_, 0), shared(nfronts_, 0);
@@ -1864,41 +1892,31 @@ class CudaEngine : public Engine {
     if (persistent && !w)
       k_gemm_tcp<128, BF><<<std::min(nt, tcp_cap_[0]), TCP_THREADS,
                             tc_smem_bytes<128>(), st>>>(
-          gb.tct[0], nt, gb.tcp, gb.amaps, gb.bmaps[0], F, d_flags_ + 2, d_rel_);
+          gb.tct[0], nt, gb.tcp, gb.amaps[BF], gb.bmaps[BF][0], F, d_flags_ + 2,
+          d_rel_);
     else if (persistent)
       k_gemm_tcp<64, BF><<<std::min(nt, tcp_cap_[1]), TCP_THREADS,
                            tc_smem_bytes<64>(), st>>>(
-          gb.tct[1], nt, gb.tcp, gb.amaps, gb.bmaps[1], F, d_flags_ + 2, d_rel_);
+          gb.tct[1], nt, gb.tcp, gb.amaps[BF], gb.bmaps[BF][1], F, d_flags_ + 2,
+          d_rel_);
     else if (!w)
       k_gemm_tc<128, BF><<<nt, 128, tc_smem_bytes<128>(), st>>>(
-          gb.tct[0], gb.tcp, gb.amaps, gb.bmaps[0], F, d_flags_ + 2, d_rel_);
+          gb.tct[0], gb.tcp, gb.amaps[BF], gb.bmaps[BF][0], F, d_flags_ + 2, d_rel_);
     else
       k_gemm_tc<64, BF><<<nt, 128, tc_smem_bytes<64>(), st>>>(
-          gb.tct[1], gb.tcp, gb.amaps, gb.bmaps[1], F, d_flags_ + 2, d_rel_);
+          gb.tct[1], gb.tcp, gb.amaps[BF], gb.bmaps[BF][1], F, d_flags_ + 2, d_rel_);
   }
 
   int factor_gemm(const GemmBatch& gb, float* F, cudaStream_t st, int fam) {
     if (gb.ntiles == 0) return ENG_OK;
     if (!use_tc_ || gb.ntcp == 0) return launch_gemm<float>(gb, F, F, F, 0, st, fam);
     int pi = prof_begin(fam, st);
-    dim3 ga(gb.tc_maxkpad / 32, (gb.tc_maxm + 31) / 32, gb.ntcp);
-    dim3 gbp((gb.tc_maxn + 7) / 8, gb.ntcp);
-    if (split_bf16_) {
-      k_tc_pack_a<true><<<ga, dim3(32, 8), 0, st>>>(gb.tcp, F, d_pack_);
-      CKL();
-      k_tc_pack_b<true><<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
-      CKL();
-    } else {
-      k_tc_pack_a<false><<<ga, dim3(32, 8), 0, st>>>(gb.tcp, F, d_pack_);
-      CKL();
-      k_tc_pack_b<false><<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
-      CKL();
-    }
     const int variant =
         (force_tcp_ >= 0 ? force_tcp_ : (gb.variant & 1)) |
-        ((force_width_ >= 0 ? force_width_ : (gb.variant >> 1) & 1) << 1);
+        ((force_width_ >= 0 ? force_width_ : (gb.variant >> 1) & 1) << 1) |
+        ((force_split_ >= 0 ? force_split_ : (gb.variant >> 2) & 1) << 2);
     int te = -1;
-    if (tuning_) {  // autotuner: time this launch
+    if (tuning_) {  // autotuner: time this batch's pack and GEMM
       te = (int)tune_events_.size();
       for (int q = 0; q < 2; q++) {
         cudaEvent_t e;
@@ -1907,11 +1925,22 @@ class CudaEngine : public Engine {
       }
       CK(cudaEventRecord(tune_events_[te], st));
     }
+    dim3 ga(gb.tc_maxkpad / 32, (gb.tc_maxm + 31) / 32, gb.ntcp);
+    dim3 gbp((gb.tc_maxn + 7) / 8, gb.ntcp);
     const int w = (variant >> 1) & 1;  // tile width 128 or 64
-    if (split_bf16_)
+    if (variant & 4) {  // BF16x3
+      k_tc_pack_a<true><<<ga, dim3(32, 8), 0, st>>>(gb.tcp, F, d_pack_);
+      CKL();
+      k_tc_pack_b<true><<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
+      CKL();
       launch_tc<true>(gb, variant & 1, w, F, st);
-    else
+    } else {  // TF32x3
+      k_tc_pack_a<false><<<ga, dim3(32, 8), 0, st>>>(gb.tcp, F, d_pack_);
+      CKL();
+      k_tc_pack_b<false><<<gbp, 256, 0, st>>>(gb.tcp, F, d_pack_);
+      CKL();
       launch_tc<false>(gb, variant & 1, w, F, st);
+    }
     if (te >= 0) {
       CK(cudaEventRecord(tune_events_[te + 1], st));
       tune_rec_.push_back({(const GemmBatch*)&gb, te});
@@ -1928,14 +1957,15 @@ class CudaEngine : public Engine {
 
   template <typename T>
   // phase 0: the whole factorization (one GPU); 1 / 2: a distributed
-  // run's subtree / shared phase (see Engine::dist_factor)
+  // run's subtree / shared phase (see Engine::dist_factor); 3: the fronts
+  // selected for an FP64 refactor (assembled by the caller)
   int run_factor(T* F, T* I, int phase = 0) {
     cudaStream_t st = stream_;
     const double es = sizeof(T);
     int rc;
     // every front zeroed and assembled first: children's Schur updates add
     // into their parents directly (extend-add fused into the Schur GEMM)
-    if (phase != 2) {
+    if (phase == 0 || phase == 1) {
       const int64_t na = phase == 1 ? na1_ : fp_->asm_level[nlevels_];
       const int64_t* apos = phase == 1 ? d_asm1_pos_ : d_asm_pos_;
       const int* aval = phase == 1 ? d_asm1_val_ : d_asm_val_;
@@ -1949,7 +1979,8 @@ class CudaEngine : public Engine {
       }
       prof_end(pi, KF_ASSEMBLE, st, 0, es * arena_ + (20.0 + es) * na);
     }
-    std::vector<LevelSched>& lvs = phase == 1 ? lv1_ : phase == 2 ? lv2_ : lv_;
+    std::vector<LevelSched>& lvs =
+        phase == 1 ? lv1_ : phase == 2 ? lv2_ : phase == 3 ? lvsel_ : lv_;
     for (int l = 0; l < nlevels_; l++) {
       LevelSched& L = lvs[l];
       cur_level_ = l;
@@ -2422,8 +2453,12 @@ class CudaEngine : public Engine {
     return rc;
   }
 
-  // FP32 factors + FP64 residual refinement; FP64 factorization on
-  // stagnation or when the iteration budget runs out.
+  // FP32 factors + FP64 residual refinement.  On stagnation (two steps
+  // without halving the backward error) or when the step budget runs out,
+  // the refinement goes on with FP64 solves: first over the FP32 factors
+  // with the fronts that spoiled them refactored in FP64 (see
+  // refactor_fp64_fronts), then, if that stalls too or no front stands
+  // out, over the FP64 factorization of the whole matrix.
   int refine(const double* B, int ldb, double* X, int ldx, int nrhs,
              cudaStream_t st, SolveReport* rep) {
     int rc;
@@ -2434,45 +2469,251 @@ class CudaEngine : public Engine {
                                       nrhs, st)))
       return rc;
     double be = 0, prev = INFINITY;
-    int it = 0, stagnant = 0;
+    int it = 0, steps = 0, stagnant = 0;
+    int mode = 0;  // 0: FP32 factors; 1: FP32 + FP64-refactored fronts; 2: FP64
     for (;;) {
       if ((rc = residual_norms(B, ldb, X, ldx, nrhs, st, &be))) return rc;
       if (be <= opt_.ir_tol) break;
-      if (it >= opt_.ir_max_iter || stagnant >= 2) {
-        // FP64 fallback: factor in FP64 and solve the correction exactly
-        if (!have64_) {
-          CK(cudaStreamSynchronize(st));
-          double sec;
-          int frc = factorize(0, &sec);
-          if (frc) return frc;
+      const int budget = mode == 0 ? opt_.ir_max_iter : std::max(opt_.ir_max_iter, 3);
+      if (steps >= budget || stagnant >= 2) {
+        if (mode == 2) break;  // FP64 factors: the backward error stands
+        CK(cudaStreamSynchronize(st));
+        int nsel = 0;
+        if (mode == 0 && !have64_) {
+          if ((rc = refactor_fp64_fronts(st, &nsel))) return rc;
         }
-        if ((rc = ensure_solve(nrhs, true))) return rc;
-        if ((rc = tree_solve_cols<double>(d_F64_, d_I64_, d_W64_, d_Y64_, d_R_, n_,
-                                          d_D_, n_, nrhs, st)))
-          return rc;
-        int pi = prof_begin(KF_RESIDUAL, st);
-        k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
-        CKL();
-        prof_end(pi, KF_RESIDUAL, st, (double)total, 24.0 * total);
-        if ((rc = residual_norms(B, ldb, X, ldx, nrhs, st, &be))) return rc;
+        if (nsel > 0) {
+          mode = 1;
+          rep->fp64_fronts = nsel;
+        } else {
+          if (!have64_) {
+            double sec;
+            int frc = factorize(0, &sec);
+            if (frc) return frc;
+          }
+          mode = 2;
+          rep->fp64_fronts = nfronts_;
+        }
         rep->fp64_fallback = 1;
-        break;
+        if ((rc = ensure_solve(nrhs, true))) return rc;
+        steps = stagnant = 0;
+        prev = INFINITY;
       }
       if (be > 0.5 * prev) stagnant++;
       else stagnant = 0;
       prev = be;
-      // d = solve32(r); x += d
-      if ((rc = tree_solve_cols<float>(d_F32_, d_I32_, d_W32_, d_Y32_, d_R_, n_, d_D_,
-                                      n_, nrhs, st)))
-        return rc;
+      // d = solve(r) with the current factors; x += d
+      if (mode == 0)
+        rc = tree_solve_cols<float>(d_F32_, d_I32_, d_W32_, d_Y32_, d_R_, n_, d_D_,
+                                    n_, nrhs, st);
+      else
+        rc = tree_solve_cols<double>(d_F64_, d_I64_, d_W64_, d_Y64_, d_R_, n_, d_D_,
+                                     n_, nrhs, st);
+      if (rc) return rc;
       int pi = prof_begin(KF_RESIDUAL, st);
       k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, d_D_, n_, X, ldx);
       CKL();
       prof_end(pi, KF_RESIDUAL, st, (double)total, 24.0 * total);
       it++;
+      steps++;
     }
     rep->ir_iters = it;
     rep->backward_error = be;
+    return ENG_OK;
+  }
+
+  // Front of every assembly entry (fronts are laid out in arena order;
+  // among fronts at one offset the empty ones sort first).
+  const std::vector<int>& asm_fronts() {
+    const FrontPlan& fp = *fp_;
+    if (asm_front_.size() == fp.asm_pos.size()) return asm_front_;
+    auto size_of = [&](int f) {
+      return (int64_t)fp.fronts[f].ld * (fp.fronts[f].p + fp.fronts[f].q);
+    };
+    std::vector<int> byoff(nfronts_);
+    for (int f = 0; f < nfronts_; f++) byoff[f] = f;
+    std::sort(byoff.begin(), byoff.end(), [&](int a, int b) {
+      const int64_t oa = fp.fronts[a].offset, ob = fp.fronts[b].offset;
+      return oa != ob ? oa < ob : size_of(a) < size_of(b);
+    });
+    std::vector<int64_t> sorted(nfronts_);
+    for (int k = 0; k < nfronts_; k++) sorted[k] = fp.fronts[byoff[k]].offset;
+    asm_front_.resize(fp.asm_pos.size());
+    for (size_t k = 0; k < fp.asm_pos.size(); k++) {
+      const int idx = (int)(std::upper_bound(sorted.begin(), sorted.end(),
+                                             fp.asm_pos[k]) - sorted.begin()) - 1;
+      asm_front_[k] = byoff[std::max(idx, 0)];
+    }
+    return asm_front_;
+  }
+
+  // The fronts to refactor in FP64: those whose largest |L| entry (the
+  // multipliers of no-pivot elimination, k_front_lmax over the FP32
+  // factors) exceeds fp64_growth, and every ancestor of one (their
+  // assembled values take the refactored updates).  nsel = 0 when no
+  // front stands out.
+  int select_fp64_fronts(cudaStream_t st, std::vector<char>& sel, int& nsel) {
+    const FrontPlan& fp = *fp_;
+    nsel = 0;
+    sel.assign(nfronts_, 0);
+    if (!(opt_.fp64_growth > 0)) return ENG_OK;
+    int rc;
+    if (!d_lmax_) {
+      std::vector<int2> t;
+      for (int f = 0; f < nfronts_; f++)
+        for (int k = 0; k < fp.fronts[f].p; k += 32) t.push_back(make_int2(f, k));
+      nlmaxt_ = (int)t.size();
+      if ((rc = alloc(d_lmax_, (size_t)nfronts_))) return rc;
+      if ((rc = upload(d_lmaxt_, t))) return rc;
+    }
+    CK(cudaMemsetAsync(d_lmax_, 0, sizeof(unsigned) * nfronts_, st));
+    if (nlmaxt_) {
+      k_front_lmax<float><<<nlmaxt_, 256, 0, st>>>(d_lmaxt_, d_fr_, d_F32_, d_lmax_);
+      CKL();
+    }
+    lmax_.assign(nfronts_, 0.f);
+    CK(cudaMemcpyAsync(lmax_.data(), d_lmax_, sizeof(float) * nfronts_,
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int f = 0; f < nfronts_; f++) {
+      if (!(lmax_[f] > opt_.fp64_growth)) continue;
+      for (int a = f; a >= 0 && !sel[a]; a = fp.fronts[a].parent) {
+        sel[a] = 1;
+        nsel++;
+      }
+    }
+    return ENG_OK;
+  }
+
+  // FP64 refactor of the selected fronts, in d_F64_ / d_I64_: every FP32
+  // factor and tile inverse promoted to FP64; the selected fronts zeroed,
+  // their original values assembled, the updates of their unselected
+  // children added (recomputed in FP64 from those children's promoted
+  // factors: F22 - L21 U12; in the deterministic mode F22 already holds
+  // it), then factored level by level with the FP64 kernels, their own
+  // children's updates fused as in a full factorization.  *nsel = 0 (and
+  // nothing done) when no front stands out, when every front would be
+  // refactored, or on the per-step panel path.
+  int refactor_fp64_fronts(cudaStream_t st, int* nsel) {
+    const FrontPlan& fp = *fp_;
+    *nsel = 0;
+    if (!use_block_ || opt_.dist_world > 1) return ENG_OK;
+    std::vector<char> sel;
+    int ns = 0, rc;
+    if ((rc = select_fp64_fronts(st, sel, ns))) return rc;
+    if (ns == 0 || ns == nfronts_) return ENG_OK;
+    if (!d_F64_ && (rc = alloc(d_F64_, (size_t)arena_))) return rc;
+    if (!d_I64_ && (rc = alloc(d_I64_, (size_t)invtot_))) return rc;
+    if (sel != sel_) {
+      // the schedule of the selected fronts, in one device blob (the
+      // previous set's blob freed)
+      if (selblob_) {
+        release_ptr(selblob_);
+        selblob_ = nullptr;
+      }
+      sel_.clear();
+      deferring_ = true;
+      fp64_only_build_ = true;
+      obc_ = obc_main_;  // (task counters after the main schedule's)
+      rc = build_levels(lvsel_, &sel);
+      fp64_only_build_ = false;
+      std::vector<int64_t> pos;
+      std::vector<int> val;
+      if (!rc) {
+        const std::vector<int>& af = asm_fronts();
+        for (size_t k = 0; k < af.size(); k++)
+          if (sel[af[k]]) {
+            pos.push_back(fp.asm_pos[k]);
+            val.push_back(fp.asm_val[k]);
+          }
+        nasel_ = (int64_t)pos.size();
+        rc = upload(d_asel_pos_, pos);
+      }
+      if (!rc) rc = upload(d_asel_val_, val);
+      // unselected children of selected fronts: their updates
+      std::vector<GemmProb> probs;
+      const int mc = std::max(fp.max_children, 1);
+      std::vector<std::vector<EaTask>> ea(mc);
+      std::vector<int> kid_rank(nfronts_, 0);
+      for (int c = 0; c < nfronts_ && !rc; c++) {
+        const FrontInfo& ci = fp.fronts[c];
+        if (ci.parent < 0) continue;
+        const int r = kid_rank[ci.parent]++;  // (child order: front index)
+        if (sel[c] || !sel[ci.parent] || ci.q == 0) continue;
+        if (deterministic_) {
+          for (int j = 0; j < ci.q; j++) ea[r % mc].push_back({c, j});
+        } else {
+          const FrontInfo& par = fp.fronts[ci.parent];
+          const int64_t o = ci.offset, ld = ci.ld;
+          GemmProb g{ci.q, ci.q, ci.p, ci.ld, ci.ld, ci.ld, o + ci.p,
+                     o + ci.p * ld, o + ci.p + ci.p * ld};
+          g.pc = par.offset;
+          g.pld = par.ld;
+          g.rel = ci.rel_offset;
+          probs.push_back(g);
+        }
+      }
+      selb_ = GemmBatch();
+      fp64_only_build_ = true;
+      if (!rc) rc = gemm_batch(probs, selb_);
+      fp64_only_build_ = false;
+      selea_.assign(mc, nullptr);
+      nselea_.assign(mc, 0);
+      for (int r = 0; r < mc && !rc; r++) {
+        nselea_[r] = (int)ea[r].size();
+        if (!ea[r].empty()) rc = upload(selea_[r], ea[r]);
+      }
+      const size_t before = ptrs_.size();
+      const int frc = flush_uploads();
+      if (ptrs_.size() > before) selblob_ = ptrs_.back();
+      if (rc || (rc = frc)) return rc;
+      sel_ = sel;
+    }
+    cudaStream_t ms = stream_;
+    const int64_t grid = 148 * 16;
+    k_upcast<<<grid, 256, 0, ms>>>(d_F32_, d_F64_, arena_);
+    CKL();
+    k_upcast<<<grid, 256, 0, ms>>>(d_I32_, d_I64_, invtot_);
+    CKL();
+    for (int f = 0; f < nfronts_; f++)
+      if (sel[f]) {
+        const FrontInfo& fi = fp.fronts[f];
+        CK(cudaMemsetAsync(d_F64_ + fi.offset, 0,
+                           sizeof(double) * fi.ld * (fi.p + fi.q), ms));
+      }
+    if (nasel_ > 0) {
+      const int b = (int)std::min<int64_t>((nasel_ + 255) / 256, grid);
+      k_assemble<double><<<b, 256, 0, ms>>>(d_asel_pos_, d_asel_val_, d_vals_,
+                                            d_F64_, nasel_);
+      CKL();
+    }
+    if ((rc = launch_gemm<double>(selb_, d_F64_, d_F64_, d_F64_, 0, ms,
+                                  KF_GEMM_SCHUR)))
+      return rc;
+    for (size_t r = 0; r < nselea_.size(); r++)
+      if (nselea_[r]) {
+        k_extend_add<double><<<nselea_[r], 256, 0, ms>>>(selea_[r], d_fr_, d_rel_,
+                                                         d_F64_);
+        CKL();
+      }
+    CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 4 * ntileflags_, ms));
+    CK(cudaMemsetAsync(d_flags_, 0, 4 * sizeof(int), ms));
+    CK(cudaMemsetAsync(d_flags_ + 5, 0, sizeof(int), ms));
+    if ((rc = run_factor<double>(d_F64_, d_I64_, 3))) return rc;
+    int flags[8];
+    CK(cudaMemcpyAsync(flags, d_flags_, sizeof flags, cudaMemcpyDeviceToHost, ms));
+    CK(cudaStreamSynchronize(ms));
+    prof_collect();
+    if (flags[2] || flags[5]) {
+      err_ = "FP64 front refactor: a device wait timed out";
+      return ENG_ETIMEOUT;
+    }
+    if (flags[1]) {
+      err_ = "FP64 front refactor: zero or non-finite pivot";
+      return ENG_ESINGULAR;
+    }
+    mixed64_ = true;
+    *nsel = nsel_ = ns;
     return ENG_OK;
   }
 
@@ -2556,7 +2797,7 @@ class CudaEngine : public Engine {
   int force_tcp_ = -1;  // tensor-core kernel variant forced (-1: per batch)
   int force_width_ = -1;  // tensor-core tile width forced (0: 128, 1: 64)
   bool use_dmma_ = true;  // FP64 GEMMs on the FP64 tensor cores
-  bool split_bf16_ = false;  // BF16x3 split of the FP32 GEMMs (else TF32x3)
+  int force_split_ = -1;  // FP32 GEMM split for every batch: 0 TF32x3, 1 BF16x3
   bool deterministic_ = false;  // fixed-order reductions (SNU_DETERMINISTIC)
   int tcp_cap_[2] = {148, 148};  // persistent grid per tile width
   // autotuner of the tensor-core kernel variant per GEMM batch
@@ -2586,6 +2827,30 @@ class CudaEngine : public Engine {
   double *d_W64_ = nullptr, *d_R_ = nullptr, *d_D_ = nullptr;
   float* d_W32_ = nullptr;
   bool have64_ = false, have32_ = false;
+  // FP64 refactor of selected fronts (refinement stagnation): their level
+  // schedule, assembly entries and the updates of their unselected
+  // children (GEMMs, or extend-add tasks per child rank in the
+  // deterministic mode), all in one device blob; the largest |L| entry of
+  // every front; d_F64_ / d_I64_ hold the promoted mixed factors while
+  // mixed64_ is set
+  std::vector<LevelSched> lvsel_;
+  std::vector<char> sel_;
+  int nsel_ = 0;
+  bool mixed64_ = false;
+  void* selblob_ = nullptr;
+  int64_t* d_asel_pos_ = nullptr;
+  int* d_asel_val_ = nullptr;
+  int64_t nasel_ = 0;
+  GemmBatch selb_;
+  std::vector<EaTask*> selea_;
+  std::vector<int> nselea_;
+  int2* d_lmaxt_ = nullptr;
+  int nlmaxt_ = 0;
+  unsigned* d_lmax_ = nullptr;
+  std::vector<float> lmax_;
+  std::vector<int> asm_front_;
+  int obc_main_ = 0;               // outer-block launches of the main schedule
+  bool fp64_only_build_ = false;   // gemm_batch: no FP32 tensor-core split
   int tiny_ = 0;
   double anorm_ = 0;
   // deferred uploads of the set-up (see upload / flush_uploads)

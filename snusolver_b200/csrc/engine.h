@@ -26,6 +26,9 @@ struct EngineOptions {
   double pivot_eps = 1e-15;
   double ir_tol = 1e-10;
   int ir_max_iter = 10;
+  // FP32_IR stagnation: fronts whose largest |L| entry exceeds this are
+  // refactored in FP64 with their ancestors (0: the whole matrix)
+  double fp64_growth = 1e3;
   int64_t mem_budget = 0;
   // separator-tree distribution over dist_world ranks (1: off): this
   // engine factors the fronts of its rank's subtree, then (after the
@@ -37,6 +40,7 @@ struct EngineOptions {
 struct SolveReport {
   int ir_iters = 0;
   int fp64_fallback = 0;
+  int fp64_fronts = 0;  // fronts refactored in FP64 by the fallback
   double backward_error = 0;
   double seconds = 0;
 };
