@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <atomic>
 #include <thread>
+#include <tuple>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -89,6 +90,132 @@ bool valid_csr(int n, int nnz, const int* rowptr, const int* colidx,
 
 }  // namespace
 
+// Host memcpy of a list of (dst, src, count) runs on up to 8 host threads
+// (a thread per at least 1 MiB).
+static void copy_runs(const std::vector<std::tuple<double*, const double*, size_t>>& runs) {
+  size_t total = 0;
+  for (const auto& r : runs) total += std::get<2>(r);
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>({8, hw, std::max<size_t>(1, total >> 17)});
+  auto part = [&](size_t lo, size_t hi) {  // elements [lo, hi) of the runs
+    size_t at = 0;
+    for (const auto& r : runs) {
+      const size_t n = std::get<2>(r);
+      const size_t a = std::max(lo, at), b = std::min(hi, at + n);
+      if (a < b)
+        std::memcpy(std::get<0>(r) + (a - at), std::get<1>(r) + (a - at),
+                    (b - a) * sizeof(double));
+      at += n;
+    }
+  };
+  if (nt <= 1) return part(0, total);
+  std::vector<std::thread> th;
+  for (size_t t = 1; t < nt; t++)
+    th.emplace_back(part, total * t / nt, total * (t + 1) / nt);
+  part(0, total / nt);
+  for (auto& x : th) x.join();
+}
+
+// The handle's pinned ring: two slots of up to 8 MiB (fewer for a small
+// transfer), made at the first host solve that needs them.
+static bool pin_ring(snu_handle* h, size_t want_elems) {
+  const size_t slot = std::min<size_t>(want_elems, (size_t)1 << 20);
+  if (h->hpin && h->pin_elems >= slot) return true;
+  if (h->hpin) cudaFreeHost(h->hpin);
+  h->hpin = nullptr;
+  h->pin_elems = 0;
+  if (cudaHostAlloc((void**)&h->hpin, 2 * slot * sizeof(double),
+                    cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    h->hpin = nullptr;
+    return false;
+  }
+  for (int k = 0; k < 2; k++)
+    if (!h->pin_ev[k] &&
+        cudaEventCreateWithFlags((cudaEvent_t*)&h->pin_ev[k],
+                                 cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+  h->pin_elems = slot;
+  return true;
+}
+
+// Host columns -> the contiguous device range dev[0, nc n) (column r of the
+// range from cols[r]), through the pinned ring: host threads fill a slot
+// while the other slot's copy runs.  Without a ring, plain copies.
+static bool columns_to_device(snu_handle* h, const double* const* cols, int nc, int n,
+                       double* dev, cudaStream_t st) {
+  const size_t total = (size_t)nc * n;
+  if (!pin_ring(h, total)) {
+    for (int r = 0; r < nc; r++)
+      if (cudaMemcpyAsync(dev + (size_t)r * n, cols[r], sizeof(double) * n,
+                          cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return false;
+    return true;
+  }
+  const size_t se = h->pin_elems;
+  int k = 0;
+  for (size_t off = 0; off < total; off += se, k ^= 1) {
+    const size_t len = std::min(se, total - off);
+    double* slot = h->hpin + (size_t)k * se;
+    if (cudaEventSynchronize((cudaEvent_t)h->pin_ev[k]) != cudaSuccess) return false;
+    std::vector<std::tuple<double*, const double*, size_t>> runs;
+    for (size_t e = off; e < off + len;) {  // (piece of column e / n)
+      const size_t r = e / n, i = e % n, m = std::min(n - i, off + len - e);
+      runs.emplace_back(slot + (e - off), cols[r] + i, m);
+      e += m;
+    }
+    copy_runs(runs);
+    if (cudaMemcpyAsync(dev + off, slot, sizeof(double) * len,
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaEventRecord((cudaEvent_t)h->pin_ev[k], st) != cudaSuccess)
+      return false;
+  }
+  return true;
+}
+
+// The contiguous device range dev[0, nc n) -> host columns, through the
+// pinned ring: the copy into one slot runs while host threads empty the
+// other.  Returns with the host columns written.
+static bool columns_to_host(snu_handle* h, const double* dev, int nc, int n,
+                     double* const* cols, cudaStream_t st) {
+  const size_t total = (size_t)nc * n;
+  if (!pin_ring(h, total)) {
+    for (int r = 0; r < nc; r++)
+      if (cudaMemcpyAsync(cols[r], dev + (size_t)r * n, sizeof(double) * n,
+                          cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return false;
+    return cudaStreamSynchronize(st) == cudaSuccess;
+  }
+  const size_t se = h->pin_elems;
+  auto drain = [&](size_t off, size_t len, int k) {
+    if (cudaEventSynchronize((cudaEvent_t)h->pin_ev[k]) != cudaSuccess) return false;
+    const double* slot = h->hpin + (size_t)k * se;
+    std::vector<std::tuple<double*, const double*, size_t>> runs;
+    for (size_t e = off; e < off + len;) {
+      const size_t r = e / n, i = e % n, m = std::min(n - i, off + len - e);
+      runs.emplace_back(cols[r] + i, slot + (e - off), m);
+      e += m;
+    }
+    copy_runs(runs);
+    return true;
+  };
+  size_t poff = 0, plen = 0;
+  int k = 0, pk = 0;
+  for (size_t off = 0; off < total; off += se, k ^= 1) {
+    const size_t len = std::min(se, total - off);
+    // (slot k was drained before the copy that last used it was drained)
+    if (cudaMemcpyAsync(h->hpin + (size_t)k * se, dev + off, sizeof(double) * len,
+                        cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaEventRecord((cudaEvent_t)h->pin_ev[k], st) != cudaSuccess)
+      return false;
+    if (plen && !drain(poff, plen, pk)) return false;
+    poff = off, plen = len, pk = k;
+  }
+  return !plen || drain(poff, plen, pk);
+}
+
 namespace snu {
 snu_status solve_pieces(snu_handle* h, const std::vector<SolvePiece>& pieces) {
   if (!h) return fail(nullptr, SNU_EINVAL, "null handle");
@@ -127,11 +254,14 @@ snu_status solve_pieces(snu_handle* h, const std::vector<SolvePiece>& pieces) {
     const int nc = std::min(chunk, nrhs - c0);
     double* dB = h->dB;
     double* dX = h->dB + (size_t)n * nc;
-    for (int r = 0; r < nc; r++)
-      if (cudaMemcpyAsync(dB + (size_t)r * n, cols[c0 + r].first,
-                          sizeof(double) * n, cudaMemcpyHostToDevice,
-                          st) != cudaSuccess)
-        return fail(h, SNU_ECUDA, "host to device copy failed");
+    std::vector<const double*> src(nc);
+    std::vector<double*> dst(nc);
+    for (int r = 0; r < nc; r++) {
+      src[r] = cols[c0 + r].first;
+      dst[r] = cols[c0 + r].second;
+    }
+    if (!columns_to_device(h, src.data(), nc, n, dB, st))
+      return fail(h, SNU_ECUDA, "host to device copy failed");
     snu_status s = snu_solve_device(h, dB, dX, nc, n, st);
     if (s != SNU_OK && s != SNU_ENOTCONV) return s;
     if (s != SNU_OK) result = s;
@@ -140,13 +270,8 @@ snu_status solve_pieces(snu_handle* h, const std::vector<SolvePiece>& pieces) {
     fb |= h->stats.fp64_fallback;
     nf64 = std::max(nf64, h->stats.fp64_fronts);
     secs += h->stats.solve_s;
-    for (int r = 0; r < nc; r++)
-      if (cudaMemcpyAsync(cols[c0 + r].second, dX + (size_t)r * n,
-                          sizeof(double) * n, cudaMemcpyDeviceToHost,
-                          st) != cudaSuccess)
-        return fail(h, SNU_ECUDA, "device to host copy failed");
-    if (cudaStreamSynchronize(st) != cudaSuccess)
-      return fail(h, SNU_ECUDA, "stream synchronize failed");
+    if (!columns_to_host(h, dX, nc, n, dst.data(), st))
+      return fail(h, SNU_ECUDA, "device to host copy failed");
   }
   h->stats.backward_error = be;
   h->stats.ir_iters = iters;
@@ -210,6 +335,9 @@ SNU_API snu_status snu_create(snu_handle** out, const snu_opts* opts) {
 SNU_API snu_status snu_destroy(snu_handle* h) {
   if (!h) return SNU_OK;
   if (h->dB) cudaFree(h->dB);
+  if (h->hpin) cudaFreeHost(h->hpin);
+  for (void* e : h->pin_ev)
+    if (e) cudaEventDestroy((cudaEvent_t)e);
   h->eng.reset();
   delete h;
   return SNU_OK;

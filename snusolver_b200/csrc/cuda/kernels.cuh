@@ -332,13 +332,15 @@ __global__ void __launch_bounds__(256)
   const int dimc = c.p + c.q, dimp = pf.p + pf.q;
   const T* src = W + c.w_off * nrhs + c.p + i;
   T* dst = W + pf.w_off * nrhs + rel[c.rel_off + i];
-  T v[16];
+  for (int k0 = 0; k0 < nrhs; k0 += 16) {  // (16 loads in flight)
+    T v[16];
 #pragma unroll
-  for (int k = 0; k < 16; k++)
-    if (k < nrhs) v[k] = src[(int64_t)k * dimc];
+    for (int k = 0; k < 16; k++)
+      if (k0 + k < nrhs) v[k] = src[(int64_t)(k0 + k) * dimc];
 #pragma unroll
-  for (int k = 0; k < 16; k++)
-    if (k < nrhs) atomicAdd(dst + (int64_t)k * dimp, v[k]);
+    for (int k = 0; k < 16; k++)
+      if (k0 + k < nrhs) atomicAdd(dst + (int64_t)(k0 + k) * dimp, v[k]);
+  }
 }
 
 // ------------------------------------------------ FP64 refinement helpers

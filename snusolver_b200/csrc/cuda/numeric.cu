@@ -397,7 +397,9 @@ class CudaEngine : public Engine {
       // solve sweeps: one flag per tile and direction, then one task
       // counter per level and direction
       // (two sets of counters: a distributed run sweeps two schedules)
-      tflags_size_ = 2 * ntileflags_ + 4 * (int64_t)nlevels_ + 2;
+      // (per column group of a pass: SWEEP_GROUPS sets of tile flags)
+      tflags_size_ =
+          2 * SWEEP_GROUPS * ntileflags_ + 4 * (int64_t)nlevels_ + 2;
       if ((rc = alloc(d_tflags_, (size_t)tflags_size_))) return rc;
       // fused panel path: two flags per tile, then one task counter per
       // outer-block launch (a level has no more outer blocks than tiles)
@@ -624,9 +626,9 @@ class CudaEngine : public Engine {
       err_ = "solve before factorize";
       return ENG_ESTATE;
     }
-    // all columns in one pass: the sweeps run in groups of up to RG columns
-    // through work vectors sized for one group, the residual, norms and
-    // refinement cover every column at once
+    // all columns at once: the sweeps run in passes of up to 64 columns
+    // (pass_cols) through work vectors sized for one pass; the residual,
+    // norms and refinement cover every column together
     cudaStream_t st = stream ? (cudaStream_t)stream : stream_;
     int rc;
     if ((rc = ensure_solve(nrhs, precision == 0))) return rc;
@@ -1013,8 +1015,10 @@ class CudaEngine : public Engine {
   int diag_launch(bool fwd, const SweepTask* tasks, int ntasks, const T* F,
                   const T* I, int nrhs, T* W, T* Y, cudaStream_t st) {
     auto k = fwd ? k_fwd_diag<T, R> : k_bwd_diag<T, R>;
+    // one task chain per column group of R columns
+    const int ngroups = (nrhs + R - 1) / R;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(std::min(ntasks, coop_cap_[(const void*)k]));
+    cfg.gridDim = dim3(std::min(ntasks * ngroups, coop_cap_[(const void*)k]));
     cfg.blockDim = dim3(DIAG_ROWS);
     cfg.dynamicSmemBytes = sweep_smem<T>();
     cfg.stream = st;
@@ -1023,13 +1027,14 @@ class CudaEngine : public Engine {
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    int* fl = d_tflags_ + (fwd ? 0 : ntileflags_);
-    int* ctr = d_tflags_ + 2 * ntileflags_ + ctr_off_ +
+    int* fl = d_tflags_ + (fwd ? 0 : SWEEP_GROUPS * ntileflags_);
+    int* ctr = d_tflags_ + 2 * SWEEP_GROUPS * ntileflags_ + ctr_off_ +
                2 * std::max(cur_level_, 0) + (fwd ? 0 : 1);
     ++launches_;
-    CK(cudaLaunchKernelEx(&cfg, k, tasks, ntasks, (const FrontDev*)d_fr_, F, I,
-                          (const int64_t*)d_flag_off_, nrhs, W, Y, fl, ctr,
-                          d_flags_ + 4));
+    CK(cudaLaunchKernelEx(&cfg, k, tasks, ntasks, ngroups,
+                          (const FrontDev*)d_fr_, F, I,
+                          (const int64_t*)d_flag_off_, (int64_t)ntileflags_,
+                          nrhs, W, Y, fl, ctr, d_flags_ + 4));
     return ENG_OK;
   }
   template <typename T, int R>
@@ -1091,8 +1096,8 @@ class CudaEngine : public Engine {
   template <typename T>
   int diag_sweep(bool fwd, const SweepTask* tasks, int ntasks, const T* F,
                  const T* I, int nrhs, T* W, T* Y, cudaStream_t st) {
-    if (nrhs > RG) {  // the kernels hold a chunk's W rows for <= RG columns
-      err_ = "pivot-block sweep called with more than 16 right-hand sides";
+    if (nrhs > SOLVE_COLS) {
+      err_ = "pivot-block sweep called with more than 64 right-hand sides";
       return ENG_EINVAL;
     }
     if (nrhs <= 1) return diag_launch<T, 1>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
@@ -1819,7 +1824,7 @@ class CudaEngine : public Engine {
   }
 
   // Work vectors of a solve of nrhs columns: W and Y (FP64 for fp64, else
-  // FP32) for one group of up to RG columns, the FP64 residual and
+  // FP32) for one pass of up to pass_cols() columns, the FP64 residual and
   // correction for all columns.  Buffers only grow; a grown
   // buffer replaces (and frees) the smaller one.
   template <typename T>
@@ -1836,7 +1841,7 @@ class CudaEngine : public Engine {
   }
   int ensure_solve(int nrhs, bool fp64) {
     int rc;
-    const size_t g = (size_t)std::min(nrhs, RG);  // one column group
+    const size_t g = (size_t)std::min(nrhs, pass_cols());  // one pass
     const size_t w = (size_t)wtot_ * g, y = (size_t)ytot_ * g;
     const size_t r = (size_t)n_ * nrhs;
     if (fp64) {
@@ -2047,14 +2052,22 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
-  // tree_solve over column groups of at most RG right-hand sides (the
-  // pivot-block sweeps hold a chunk's rows for RG columns); W and Y are
-  // reused by every group.
+  // Columns per solve pass: SOLVE_COLS for the level-by-level sweeps, RG
+  // for the whole-tree sweeps (they hold a chunk's rows for RG columns).
+  int pass_cols() const { return fused_solve_ ? RG : SOLVE_COLS; }
+  // Register groups of a pass of nrhs columns (the sweep kernels' R is
+  // nrhs rounded up to a power of two up to RG, then RG).
+  static int col_groups(int nrhs) { return nrhs <= RG ? 1 : (nrhs + RG - 1) / RG; }
+
+  // tree_solve over passes of at most `group` columns (0: pass_cols());
+  // W and Y, sized for one pass, are reused by every pass.
   template <typename T>
   int tree_solve_cols(const T* F, const T* I, T* W, T* Y, const double* B,
-                      int ldb, double* X, int ldx, int nrhs, cudaStream_t st) {
-    for (int c0 = 0; c0 < nrhs; c0 += RG) {
-      const int nc = std::min(RG, nrhs - c0);
+                      int ldb, double* X, int ldx, int nrhs, cudaStream_t st,
+                      int group = 0) {
+    const int g = group > 0 ? std::min(group, pass_cols()) : pass_cols();
+    for (int c0 = 0; c0 < nrhs; c0 += g) {
+      const int nc = std::min(g, nrhs - c0);
       int rc = fused_solve_
                    ? tree_solve_fused<T>(F, I, W, Y, B + (size_t)c0 * ldb, ldb,
                                          X + (size_t)c0 * ldx, ldx, nc, st)
@@ -2159,8 +2172,8 @@ class CudaEngine : public Engine {
   template <typename T>
   int tree_solve(const T* F, const T* I, T* W, T* Y, const double* B, int ldb,
                  double* X, int ldx, int nrhs, cudaStream_t st) {
-    if (nrhs < 1 || nrhs > RG) {  // the kernels hold at most RG columns
-      err_ = "tree solve of more than 16 columns at once";
+    if (nrhs < 1 || nrhs > SOLVE_COLS) {
+      err_ = "tree solve of more than 64 columns at once";
       return ENG_EINVAL;
     }
     CK(cudaMemsetAsync(d_tflags_, 0, sizeof(int) * tflags_size_, st));
@@ -2218,8 +2231,8 @@ class CudaEngine : public Engine {
         }
         if (L.ngl) {
           pi = prof_begin(KF_SOLVE_GEMM, st);
-          SNU_RG_DISPATCH(nrhs, k_gemv_l21, T, (L.ngl, 256, 0, st),
-                          (L.gl, d_fr_, F, nrhs, W, Y));
+          SNU_RG_DISPATCH(nrhs, k_gemv_l21, T, (L.ngl * col_groups(nrhs), 256, 0, st),
+                          (L.gl, L.ngl, d_fr_, F, nrhs, W, Y));
           CKL();
           prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
                    L.gq_elems * es);
@@ -2238,8 +2251,8 @@ class CudaEngine : public Engine {
         prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
         if (L.ngq) {
           pi = prof_begin(KF_SOLVE_GEMM, st);
-          SNU_RG_DISPATCH(nrhs, k_gemv_u12, T, (L.ngq, 256, 0, st),
-                          (L.gq, d_fr_, F, nrhs, W, Y));
+          SNU_RG_DISPATCH(nrhs, k_gemv_u12, T, (L.ngq * col_groups(nrhs), 256, 0, st),
+                          (L.gq, L.ngq, d_fr_, F, nrhs, W, Y));
           CKL();
           prof_end(pi, KF_SOLVE_GEMM, st, 2.0 * L.gq_elems * nrhs,
                    L.gq_elems * es);
@@ -2361,8 +2374,8 @@ class CudaEngine : public Engine {
     }
     const size_t es = precision == 0 ? sizeof(double) : sizeof(float);
     auto up = [](size_t b) { return (b + 255) / 256 * 256; };
-    // W and Y serve one column group (at most RG columns) at a time; the
-    // residual R and correction D hold every column
+    // W and Y serve one pass of at most RG columns at a time (the static
+    // array is small); the residual R and correction D hold every column
     const size_t gc = (size_t)std::min(nrhs, RG);
     const size_t bw = up((size_t)wtot_ * gc * es), by = up((size_t)ytot_ * gc * es);
     const size_t br = up((size_t)n_ * nrhs * sizeof(double));
@@ -2407,7 +2420,7 @@ class CudaEngine : public Engine {
       if (precision == 0) {
         if ((rc = tree_solve_cols<double>(d_F64_, d_I64_, (double*)pW,
                                           (double*)pY, dB, ldb, dX, ldb, nrhs,
-                                          st)))
+                                          st, RG)))
           break;
         rc = berr(dX);
         break;
@@ -2415,7 +2428,7 @@ class CudaEngine : public Engine {
       float* W = (float*)pW;
       float* Y = (float*)pY;
       if ((rc = tree_solve_cols<float>(d_F32_, d_I32_, W, Y, dB, ldb, dX, ldb,
-                                       nrhs, st)))
+                                       nrhs, st, RG)))
         break;
       double prev = INFINITY;
       int it = 0, stagnant = 0;
@@ -2432,7 +2445,7 @@ class CudaEngine : public Engine {
         stagnant = r.backward_error > 0.5 * prev ? stagnant + 1 : 0;
         prev = r.backward_error;
         if ((rc = tree_solve_cols<float>(d_F32_, d_I32_, W, Y, R, n_, D, n_,
-                                         nrhs, st)))
+                                         nrhs, st, RG)))
           break;
         k_axpy_cols<<<blocks, 256, 0, st>>>(n_, nrhs, D, n_, dX, ldb);
         CKL();

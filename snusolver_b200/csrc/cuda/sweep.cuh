@@ -21,6 +21,11 @@
 namespace snu {
 
 constexpr int RG = 16;          // right-hand sides per register group
+// columns per pass of the level-by-level sweeps: the pivot-block sweeps run
+// the pass's register groups as independent task chains of one launch (a
+// group's tasks after the previous group's), each with its own tile flags
+constexpr int SOLVE_COLS = 64;
+constexpr int SWEEP_GROUPS = SOLVE_COLS / RG;
 constexpr int DIAG_ROWS = 128;  // rows of a pivot-block chunk (= threads)
 constexpr long WAVE_SPIN_LIMIT = 1L << 22;
 
@@ -119,17 +124,17 @@ __device__ __forceinline__ void tile_apply(const T* Xs, T (*in)[R],
 // while tile s waits for its flag and is applied.
 template <typename T, int R>
 __global__ void __launch_bounds__(DIAG_ROWS)
-    k_fwd_diag(const SweepTask* __restrict__ tasks, int ntasks,
+    k_fwd_diag(const SweepTask* __restrict__ tasks, int nbase, int ngroups,
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                const T* __restrict__ INV, const int64_t* __restrict__ flag_off,
-               int nrhs, T* __restrict__ W, T* __restrict__ Y, int* flags,
-               int* next_task, int* err) {
+               int64_t gstride, int nrhs, T* __restrict__ W,
+               T* __restrict__ Y, int* flags, int* next_task, int* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls0 = reinterpret_cast<T*>(smem_raw);  // [2][NB][DIAG_ROWS]
   T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;         // [2][NB * NB]
   __shared__ T ws[NB][R];
   __shared__ T ys[NB][R];
-  __shared__ T Wc[R][DIAG_ROWS];  // this chunk's rows of W (nrhs <= R)
+  __shared__ T Wc[R][DIAG_ROWS];  // this chunk's rows of W (its group's columns)
   __shared__ int bad, s_task;
   const int tid = threadIdx.x;
   constexpr int V = 16 / sizeof(T);
@@ -140,13 +145,17 @@ __global__ void __launch_bounds__(DIAG_ROWS)
     if (tid == 0) s_task = atomicAdd(next_task, 1);
     __syncthreads();
     const int task = s_task;
-    if (task >= ntasks) break;
-    const SweepTask t = tasks[task];
+    if (task >= nbase * ngroups) break;
+    // task = group g's copy of base task task - g nbase: columns
+    // [g R, g R + nr) of the pass, with the group's own tile flags
+    const int g = task / nbase;
+    const SweepTask t = tasks[task - g * nbase];
+    const int r0 = g * R, nr = min(R, nrhs - r0);
     const FrontDev f = fr[t.front];
     const int dim = f.p + f.q;
     const int c0 = t.chunk * DIAG_ROWS, c1 = min(f.p, c0 + DIAG_ROWS);
     const int ntiles = (f.p + NB - 1) / NB;
-    int* fl = flags + flag_off[t.front];
+    int* fl = flags + g * gstride + flag_off[t.front];
     T* Wf = W + f.w_off * nrhs;
     T* Yf = Y + f.y_off * nrhs;
     const int row = c0 + tid;
@@ -167,7 +176,8 @@ __global__ void __launch_bounds__(DIAG_ROWS)
     // so the chunk keeps its rows in shared memory and never writes them back
 #pragma unroll
     for (int r = 0; r < R; r++)
-      Wc[r][tid] = (row < c1 && r < nrhs) ? Wf[row + (int64_t)r * dim] : (T)0;
+      Wc[r][tid] =
+          (row < c1 && r < nr) ? Wf[row + (int64_t)(r0 + r) * dim] : (T)0;
     for (int s = 0; s < ntiles; s++) {
       const int k0 = s * NB, kb = min(NB, f.p - k0), k1 = k0 + kb;
       if (k0 >= c1) break;  // owned by a later chunk; updates no row of ours
@@ -181,17 +191,16 @@ __global__ void __launch_bounds__(DIAG_ROWS)
       cp_async_wait_prev();  // tile s staged (tile s+1 may still be in flight)
       __syncthreads();
       if (bad) return;
-      for (int r0 = 0; r0 < nrhs; r0 += R) {
-        const int nr = min(R, nrhs - r0);
+      {
         if (owner) {
           for (int e = tid; e < NB * R; e += blockDim.x) {
             const int i = e % NB, r = e / NB;
-            ws[i][r] = (i < kb && r < nr) ? Wc[r0 + r][k0 - c0 + i] : (T)0;
+            ws[i][r] = (i < kb && r < nr) ? Wc[r][k0 - c0 + i] : (T)0;
           }
           __syncthreads();
           tile_apply<T, R>(Xs, ws, ys, Yf, f.p, k0, kb, r0, nr);
           __syncthreads();  // raise_flag's fence publishes the CTA's Y stores
-          if (tid == 0 && r0 + R >= nrhs) raise_flag(fl + s);
+          if (tid == 0) raise_flag(fl + s);
         } else {
           for (int e = tid; e < NB * R; e += blockDim.x) {
             const int i = e % NB, r = e / NB;
@@ -213,7 +222,7 @@ __global__ void __launch_bounds__(DIAG_ROWS)
           }
 #pragma unroll
           for (int r = 0; r < R; r++)
-            if (r < nr) Wc[r0 + r][tid] -= acc[r];
+            if (r < nr) Wc[r][tid] -= acc[r];
         }
         __syncthreads();
       }
@@ -229,17 +238,17 @@ __global__ void __launch_bounds__(DIAG_ROWS)
 // tile s-1 overlaps tile s as in the forward sweep.
 template <typename T, int R>
 __global__ void __launch_bounds__(DIAG_ROWS)
-    k_bwd_diag(const SweepTask* __restrict__ tasks, int ntasks,
+    k_bwd_diag(const SweepTask* __restrict__ tasks, int nbase, int ngroups,
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                const T* __restrict__ INV, const int64_t* __restrict__ flag_off,
-               int nrhs, T* __restrict__ W, T* __restrict__ Y, int* flags,
-               int* next_task, int* err) {
+               int64_t gstride, int nrhs, T* __restrict__ W,
+               T* __restrict__ Y, int* flags, int* next_task, int* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls0 = reinterpret_cast<T*>(smem_raw);
   T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;
   __shared__ T ws[NB][R];
   __shared__ T xs[NB][R];
-  __shared__ T Wc[R][DIAG_ROWS];  // this chunk's rows of W (nrhs <= R)
+  __shared__ T Wc[R][DIAG_ROWS];  // this chunk's rows of W (its group's columns)
   __shared__ int bad, s_task;
   const int tid = threadIdx.x;
   if (tid == 0) bad = 0;
@@ -248,13 +257,17 @@ __global__ void __launch_bounds__(DIAG_ROWS)
     if (tid == 0) s_task = atomicAdd(next_task, 1);
     __syncthreads();
     const int task = s_task;
-    if (task >= ntasks) break;
-    const SweepTask t = tasks[task];
+    if (task >= nbase * ngroups) break;
+    // task = group g's copy of base task task - g nbase: columns
+    // [g R, g R + nr) of the pass, with the group's own tile flags
+    const int g = task / nbase;
+    const SweepTask t = tasks[task - g * nbase];
+    const int r0 = g * R, nr = min(R, nrhs - r0);
     const FrontDev f = fr[t.front];
     const int dim = f.p + f.q;
     const int c0 = t.chunk * DIAG_ROWS, c1 = min(f.p, c0 + DIAG_ROWS);
     const int ntiles = (f.p + NB - 1) / NB;
-    int* fl = flags + flag_off[t.front];
+    int* fl = flags + g * gstride + flag_off[t.front];
     T* Wf = W + f.w_off * nrhs;
     T* Yf = Y + f.y_off * nrhs;
     const int row = c0 + tid;
@@ -271,7 +284,8 @@ __global__ void __launch_bounds__(DIAG_ROWS)
     cp_async_commit();
 #pragma unroll
     for (int r = 0; r < R; r++)
-      Wc[r][tid] = (row < c1 && r < nrhs) ? Wf[row + (int64_t)r * dim] : (T)0;
+      Wc[r][tid] =
+          (row < c1 && r < nr) ? Wf[row + (int64_t)(r0 + r) * dim] : (T)0;
     for (int s = ntiles - 1; s >= 0; s--) {
       const int k0 = s * NB, kb = min(NB, f.p - k0);
       if (k0 < c0) break;  // tile lies above our rows: nothing left
@@ -285,17 +299,16 @@ __global__ void __launch_bounds__(DIAG_ROWS)
       cp_async_wait_prev();
       __syncthreads();
       if (bad) return;
-      for (int r0 = 0; r0 < nrhs; r0 += R) {
-        const int nr = min(R, nrhs - r0);
+      {
         if (owner) {
           for (int e = tid; e < NB * R; e += blockDim.x) {
             const int i = e % NB, r = e / NB;
-            ws[i][r] = (i < kb && r < nr) ? Wc[r0 + r][k0 - c0 + i] : (T)0;
+            ws[i][r] = (i < kb && r < nr) ? Wc[r][k0 - c0 + i] : (T)0;
           }
           __syncthreads();
           tile_apply<T, R>(Xs, ws, xs, Yf, f.p, k0, kb, r0, nr);
           __syncthreads();
-          if (tid == 0 && r0 + R >= nrhs) raise_flag(fl + s);
+          if (tid == 0) raise_flag(fl + s);
         } else {
           for (int e = tid; e < NB * R; e += blockDim.x) {
             const int i = e % NB, r = e / NB;
@@ -317,7 +330,7 @@ __global__ void __launch_bounds__(DIAG_ROWS)
           }
 #pragma unroll
           for (int r = 0; r < R; r++)
-            if (r < nr) Wc[r0 + r][tid] -= acc[r];
+            if (r < nr) Wc[r][tid] -= acc[r];
         }
         __syncthreads();
       }
@@ -361,8 +374,11 @@ constexpr int GEMV_ROWS = 64, GEMV_K = 256;
 // writer (the bit-reproducible schedule).
 //   FWD:  W[p + i] -= L21[i, :] Y        (i < q, over the p pivot columns)
 //   !FWD: W[i]     -= U12[i, :] W[p:dim] (i < p, over the q update columns)
+// Blocks [g ntasks, (g + 1) ntasks) take columns [g R, g R + R) of the
+// pass (R >= nrhs: one group, every column).
 template <typename T, int R, bool FWD>
 __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
+                                         int ntasks,
                                          const FrontDev* __restrict__ fr,
                                          const T* __restrict__ F, int nrhs,
                                          T* __restrict__ W,
@@ -374,7 +390,8 @@ __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
   __shared__ __align__(16) unsigned char smb[YS > RED ? YS : RED];
   T(*ys)[R] = reinterpret_cast<T(*)[R]>(smb);
   T(*red)[GEMV_ROWS][R + 1] = reinterpret_cast<T(*)[GEMV_ROWS][R + 1]>(smb);
-  const SweepTask t = tasks[blockIdx.x];
+  const int cg = blockIdx.x / ntasks;  // column group
+  const SweepTask t = tasks[blockIdx.x - cg * ntasks];
   const FrontDev f = fr[t.front];
   const int dim = f.p + f.q;
   const int nrows = FWD ? f.q : f.p, nk = FWD ? f.p : f.q;
@@ -388,7 +405,7 @@ __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
   const int lds = FWD ? f.p : dim;
   const T* a = FWD ? F + f.off + f.p + i : F + f.off + i + (int64_t)f.p * f.ld;
   T* dst = FWD ? Wf + f.p : Wf;
-  for (int r0 = 0; r0 < nrhs; r0 += R) {
+  for (int r0 = cg * R; r0 < min(nrhs, cg * R + R); r0 += R) {
     const int nr = min(R, nrhs - r0);
     T acc[R];
 #pragma unroll
@@ -438,18 +455,18 @@ __device__ __forceinline__ void gemv_off(const SweepTask* __restrict__ tasks,
 
 template <typename T, int R>
 __global__ void __launch_bounds__(256)
-    k_gemv_l21(const SweepTask* __restrict__ tasks,
+    k_gemv_l21(const SweepTask* __restrict__ tasks, int ntasks,
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                int nrhs, T* __restrict__ W, const T* __restrict__ Y) {
-  gemv_off<T, R, true>(tasks, fr, F, nrhs, W, Y);
+  gemv_off<T, R, true>(tasks, ntasks, fr, F, nrhs, W, Y);
 }
 
 template <typename T, int R>
 __global__ void __launch_bounds__(256)
-    k_gemv_u12(const SweepTask* __restrict__ tasks,
+    k_gemv_u12(const SweepTask* __restrict__ tasks, int ntasks,
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                int nrhs, T* __restrict__ W, const T* __restrict__ Y) {
-  gemv_off<T, R, false>(tasks, fr, F, nrhs, W, Y);
+  gemv_off<T, R, false>(tasks, ntasks, fr, F, nrhs, W, Y);
 }
 
 // X[gidx[t]] = Y[t] for the pivot rows of every front of a level.

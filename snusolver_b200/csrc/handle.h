@@ -23,6 +23,11 @@ struct snu_handle {
   snu_stats stats;
   double* dB = nullptr;  // staging for host solves
   size_t dcap = 0;
+  // pinned two-slot ring for the host copies of host solves (the caller's
+  // pageable arrays go through it in slot-sized pieces)
+  double* hpin = nullptr;
+  size_t pin_elems = 0;  // per slot
+  void* pin_ev[2] = {nullptr, nullptr};  // cudaEvent_t of each slot's copy
   void* stream = nullptr;    // user stream (applied at construct)
   unsigned prof_mask = 0;    // profiling families (applied at construct)
   int autotune = 0;          // tune the GEMM variants at the next factorize

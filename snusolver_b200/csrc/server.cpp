@@ -26,6 +26,7 @@
 //   that matrix) and solves their columns together, one refinement loop
 //   for all of them.
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -134,17 +135,17 @@ struct Parked {
   int64_t bytes = 0;
 };
 
-// Columns of one merged solve: the sweeps take 16 columns per pass, so
-// requests merge while their columns fit one pass (merging wider work only
-// serialises what the slots would run side by side: measured on the
-// serving stream, 64-column merges raised the solve service median from 41
-// to 124 ms)
-constexpr int MERGE_COLUMNS = 16;
+// Columns of one merged solve (requests on one matrix run one at a time, so
+// merging them into one pass of the sweeps saves their passes and
+// refinement loops while the pass stays within its 64 columns, whose four
+// register groups run side by side); SNU_MERGE_COLUMNS overrides it
+constexpr int MERGE_COLUMNS = 64;
 
 }  // namespace
 
 struct snu_server {
   snu_server_opts o;
+  int merge_cols = MERGE_COLUMNS;
   std::mutex mu;
   std::condition_variable cv_work;  // queue changed / matrix freed / stop
   std::condition_variable cv_done;  // a completion was posted
@@ -206,7 +207,7 @@ struct snu_server {
 
   // Oldest queued request whose matrix is idle (factor requests always
   // are), and for a solve the solve requests queued behind it on the same
-  // matrix (up to MERGE_COLUMNS columns, none past another request of that
+  // matrix (up to merge_cols columns, none past another request of that
   // matrix).
   std::vector<std::unique_ptr<Request>> take() {
     std::vector<std::unique_ptr<Request>> out;
@@ -225,7 +226,7 @@ struct snu_server {
           ++it;
           continue;
         }
-        if ((*it)->type != SNU_REQ_SOLVE || cols + (*it)->nrhs > MERGE_COLUMNS)
+        if ((*it)->type != SNU_REQ_SOLVE || cols + (*it)->nrhs > merge_cols)
           break;
         cols += (*it)->nrhs;
         out.push_back(std::move(*it));
@@ -612,6 +613,8 @@ SNU_API snu_status snu_server_create(snu_server** out, const snu_server_opts* o)
   }
   auto* s = new snu_server();
   s->o = d;
+  if (const char* e = std::getenv("SNU_MERGE_COLUMNS"))
+    s->merge_cols = std::max(1, std::atoi(e));
   s->budget = std::min<int64_t>(d.mem_budget, (int64_t)(0.9 * (double)fr));
   for (int i = 0; i < d.slots; i++)
     s->workers.emplace_back([s, i] { s->worker_loop(i); });

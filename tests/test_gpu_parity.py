@@ -417,3 +417,31 @@ def test_deterministic_mode_is_bit_reproducible(gpu, monkeypatch, precision):
             for r in range(3):
                 assert rel_resid(rp, ci, v, X1[:, r], B[:, r]) <= 1e-10
         assert np.array_equal(runs[0], runs[1])
+
+
+@pytest.mark.parametrize("precision,tol,res", [(snu.FP64, 1e-12, 1e-12),
+                                               (snu.FP32_IR, 1e-9, 1e-10)])
+def test_wide_solve_passes_and_host_copies(gpu, precision, tol, res):
+    # 70 columns through the host API: one pass of 64 columns (the sweeps
+    # run four register groups per staged tile, W rows in global memory)
+    # and one of 6, the columns crossing the pinned ring's 1 Mi-element
+    # slots mid-column; every column equals its own single-column solve
+    rp, ci, v = generators.laplace2d_perturbed(200, 200, seed=31)
+    n = len(rp) - 1
+    B = generators.rhs(n, 70, seed=32)
+    s = snu.Solver(nleaves=8, precision=precision).construct(rp, ci, v)
+    X = s.factorize().solve(B)
+    assert s.stats()["backward_error"] <= res
+    for c in (0, 15, 16, 40, 63, 64, 69):
+        x1 = s.solve(B[:, c])
+        err = np.abs(X[:, c] - x1).max() / np.abs(x1).max()
+        assert err <= tol, (c, err)
+        assert rel_resid(rp, ci, v, X[:, c], B[:, c]) <= res
+    # the device API, 40 columns in one pass, equals the host API's result
+    import torch
+    dB = torch.from_numpy(np.ascontiguousarray(B[:, :40].T)).cuda()
+    dX = torch.empty_like(dB)
+    s.solve_device(dB.data_ptr(), dX.data_ptr(), 40, n)
+    torch.cuda.synchronize()
+    Xd = dX.cpu().numpy().T
+    assert np.abs(Xd - X[:, :40]).max() <= tol * np.abs(X[:, :40]).max()
