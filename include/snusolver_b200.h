@@ -78,8 +78,19 @@ typedef struct snu_opts {
                            and refinement goes on with FP64 solves; no front
                            above it, or 0: the whole matrix in FP64.
                            default 1e3 */
-  int reserved[6];
+  int gemm_split;       /* FP32 tensor-core GEMM split: SNU_SPLIT_AUTO (BF16x3,
+                           or per batch by the autotuner), SNU_SPLIT_TF32
+                           (TF32x3: FP32-level products, fewer refinement
+                           steps on harder matrices) or SNU_SPLIT_BF16;
+                           the environment's SNU_SPLIT overrides it.
+                           default SNU_SPLIT_AUTO */
+  int reserved[5];
 } snu_opts;
+
+/* FP32 tensor-core GEMM splits (snu_opts.gemm_split). */
+#define SNU_SPLIT_AUTO 0
+#define SNU_SPLIT_TF32 1
+#define SNU_SPLIT_BF16 2
 
 typedef struct snu_stats {
   int n, nnz, nleaves, nfronts, nlevels;
@@ -324,7 +335,7 @@ typedef struct snu_server snu_server;
 
 typedef struct snu_server_opts {
   int device;           /* CUDA device; default 0 */
-  int slots;            /* requests on the GPU at once; default 4 */
+  int slots;            /* requests on the GPU at once; default 8 */
   int64_t mem_budget;   /* device bytes for resident factors and work;
                            default 120 GB, capped at 90% of the free memory */
   int nleaves;          /* as snu_opts; default 8 */
@@ -332,7 +343,10 @@ typedef struct snu_server_opts {
   double ir_tol;        /* as snu_opts; default 1e-10 */
   int ir_max_iter;      /* as snu_opts; default 10 */
   int plan_cache;       /* host plans kept by pattern; default 64 */
-  int reserved[8];
+  int gemm_split;       /* as snu_opts; default SNU_SPLIT_TF32 (requests are
+                           mostly solves, which TF32x3 factors serve with
+                           fewer refinement steps) */
+  int reserved[7];
 } snu_server_opts;
 
 typedef enum snu_request_type {

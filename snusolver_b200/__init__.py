@@ -23,9 +23,10 @@ import numpy as np
 
 __all__ = ["SnuError", "Solver", "CsrMatrix", "read_matrix", "initialize",
            "solve", "SnuMat", "library_path", "load_library", "FP64", "FP32_IR",
-           "STATUS"]
+           "SPLIT_AUTO", "SPLIT_TF32", "SPLIT_BF16", "STATUS"]
 
 FP64, FP32_IR = 0, 1
+SPLIT_AUTO, SPLIT_TF32, SPLIT_BF16 = 0, 1, 2  # FP32 tensor-core GEMM split
 STATUS = {0: "SNU_OK", 1: "SNU_EINVAL", 2: "SNU_ENOMEM", 3: "SNU_ESINGULAR",
           4: "SNU_ETIMEOUT", 5: "SNU_ECUDA", 6: "SNU_ESTATE", 7: "SNU_ENOTCONV"}
 
@@ -50,7 +51,7 @@ class _Opts(C.Structure):
                 ("pivot_eps", C.c_double), ("ir_tol", C.c_double),
                 ("ir_max_iter", C.c_int), ("device", C.c_int),
                 ("mem_budget", C.c_int64), ("fp64_growth", C.c_double),
-                ("reserved", C.c_int * 6)]
+                ("gemm_split", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class _Stats(C.Structure):
@@ -158,7 +159,7 @@ class Solver:
 
     def __init__(self, nleaves=8, precision=FP64, pivot_eps=1e-15,
                  ir_tol=1e-10, ir_max_iter=10, device=0, mem_budget=0,
-                 fp64_growth=1e3):
+                 fp64_growth=1e3, gemm_split=0):
         self._lib = load_library()
         o = _Opts()
         self._lib.snu_default_opts(C.byref(o))
@@ -166,6 +167,7 @@ class Solver:
         o.pivot_eps, o.ir_tol, o.ir_max_iter = pivot_eps, ir_tol, ir_max_iter
         o.device, o.mem_budget = device, mem_budget
         o.fp64_growth = fp64_growth
+        o.gemm_split = gemm_split  # SPLIT_AUTO, SPLIT_TF32 or SPLIT_BF16
         h = C.c_void_p()
         st = self._lib.snu_create(C.byref(h), C.byref(o))
         if st:

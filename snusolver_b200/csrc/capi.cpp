@@ -309,6 +309,7 @@ SNU_API void snu_default_opts(snu_opts* o) {
   o->device = 0;
   o->mem_budget = 0;
   o->fp64_growth = 1e3;
+  o->gemm_split = SNU_SPLIT_AUTO;
 }
 
 SNU_API snu_status snu_create(snu_handle** out, const snu_opts* opts) {
@@ -322,7 +323,7 @@ SNU_API snu_status snu_create(snu_handle** out, const snu_opts* opts) {
   if (o.precision != SNU_FP64 && o.precision != SNU_FP32_IR)
     return fail(nullptr, SNU_EINVAL, "unknown precision");
   if (!(o.pivot_eps >= 0) || !(o.ir_tol > 0) || o.ir_max_iter < 0 ||
-      !(o.fp64_growth >= 0))
+      !(o.fp64_growth >= 0) || o.gemm_split < 0 || o.gemm_split > 2)
     return fail(nullptr, SNU_EINVAL, "bad tolerance options");
   snu_handle* h = new (std::nothrow) snu_handle();
   if (!h) return fail(nullptr, SNU_ENOMEM, "out of host memory");
@@ -959,6 +960,7 @@ snu_status finish_construct(snu_handle* h, const double* vals, bool have_plan) {
   eo.ir_tol = h->opts.ir_tol;
   eo.ir_max_iter = h->opts.ir_max_iter;
   eo.fp64_growth = h->opts.fp64_growth;
+  eo.gemm_split = h->opts.gemm_split;
   eo.mem_budget = h->opts.mem_budget;
   eo.dist_rank = h->dist_rank;
   eo.dist_world = h->dist_world;

@@ -261,9 +261,9 @@ class CudaEngine : public Engine {
       // TF32x3 (kind::tf32) or the BF16x3 (kind::f16) split; unset: BF16x3
       // unless the autotuner picks TF32x3 for a batch
       const char* sp = getenv("SNU_SPLIT");
-      force_split_ = !sp || !sp[0] ? -1
-                     : (sp[0] == 'b' || sp[0] == 'B') ? 1
-                     : (sp[0] == 't' || sp[0] == 'T') ? 0 : -1;
+      force_split_ = opt_.gemm_split == 1 ? 0 : opt_.gemm_split == 2 ? 1 : -1;
+      if (sp && (sp[0] == 'b' || sp[0] == 'B')) force_split_ = 1;
+      if (sp && (sp[0] == 't' || sp[0] == 'T')) force_split_ = 0;
       // SNU_DMMA=0: FP64 GEMMs on the SIMT kernel instead of mma.sync f64
       const char* dm = getenv("SNU_DMMA");
       use_dmma_ = !(dm && dm[0] == '0');

@@ -29,6 +29,9 @@ struct EngineOptions {
   // FP32_IR stagnation: fronts whose largest |L| entry exceeds this are
   // refactored in FP64 with their ancestors (0: the whole matrix)
   double fp64_growth = 1e3;
+  // FP32 tensor-core GEMM split: 0 auto (BF16x3 or the autotuner's per
+  // batch), 1 TF32x3, 2 BF16x3 (SNU_SPLIT overrides)
+  int gemm_split = 0;
   int64_t mem_budget = 0;
   // separator-tree distribution over dist_world ranks (1: off): this
   // engine factors the fronts of its rank's subtree, then (after the

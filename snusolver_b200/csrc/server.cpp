@@ -360,6 +360,7 @@ int snu_server::run_factor(Request& r, cudaStream_t st, double t_start) {
   ho.precision = o.precision;
   ho.ir_tol = o.ir_tol;
   ho.ir_max_iter = o.ir_max_iter;
+  ho.gemm_split = o.gemm_split;
   ho.device = o.device;
   const uint64_t key = pattern_hash(r.n, r.nnz, r.rowptr.data(), r.colidx.data());
   {
@@ -584,13 +585,14 @@ SNU_API void snu_server_default_opts(snu_server_opts* o) {
   if (!o) return;
   std::memset(o, 0, sizeof *o);
   o->device = 0;
-  o->slots = 4;
+  o->slots = 8;
   o->mem_budget = 120ll << 30;
   o->nleaves = 8;
   o->precision = SNU_FP32_IR;
   o->ir_tol = 1e-10;
   o->ir_max_iter = 10;
   o->plan_cache = 64;
+  o->gemm_split = SNU_SPLIT_TF32;
 }
 
 SNU_API snu_status snu_server_create(snu_server** out, const snu_server_opts* o) {

@@ -28,7 +28,7 @@ class _ServerOpts(C.Structure):
                 ("mem_budget", C.c_int64), ("nleaves", C.c_int),
                 ("precision", C.c_int), ("ir_tol", C.c_double),
                 ("ir_max_iter", C.c_int), ("plan_cache", C.c_int),
-                ("reserved", C.c_int * 8)]
+                ("gemm_split", C.c_int), ("reserved", C.c_int * 7)]
 
 
 class _Completion(C.Structure):
@@ -78,15 +78,17 @@ def _bind(lib):
 class Server:
     """A request server on one GPU (see the module docstring)."""
 
-    def __init__(self, device=0, slots=4, mem_budget=120 << 30, nleaves=8,
+    def __init__(self, device=0, slots=8, mem_budget=120 << 30, nleaves=8,
                  precision=FP32_IR, ir_tol=1e-10, ir_max_iter=10,
-                 plan_cache=64):
+                 plan_cache=64, gemm_split=None):
         self._lib = _bind(load_library())
         o = _ServerOpts()
         self._lib.snu_server_default_opts(C.byref(o))
         o.device, o.slots, o.mem_budget = device, slots, mem_budget
         o.nleaves, o.precision = nleaves, precision
         o.ir_tol, o.ir_max_iter, o.plan_cache = ir_tol, ir_max_iter, plan_cache
+        if gemm_split is not None:  # (default: the library's, TF32x3)
+            o.gemm_split = gemm_split
         s = C.c_void_p()
         st = self._lib.snu_server_create(C.byref(s), C.byref(o))
         if st:
@@ -232,7 +234,7 @@ def rescale_values(rowptr, colidx, vals, rng, lo=0.5, hi=2.0):
 
 
 def run_stream(rate=200.0, duration=5.0, seed=5, mix=(0.05, 0.10, 0.85),
-               slots=4, mem_budget=120 << 30, max_resident=4, warm=True,
+               slots=8, mem_budget=120 << 30, max_resident=4, warm=True,
                shapes=SERVE_SHAPES, device=0):
     """The serving workload: Poisson arrivals (mean `rate` per second, seeded)
     for `duration` seconds, mixing new-factor requests on 2D / 3D lognormal

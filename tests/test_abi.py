@@ -34,6 +34,25 @@ def test_bad_options_rejected():
         snu.Solver(nleaves=1024)
 
 
+def test_precision_option_defaults_and_checks():
+    # snu_opts: fp64_growth 1e3 and the automatic GEMM split by default;
+    # the server's handles default to TF32x3; out-of-range values refused
+    from snusolver_b200.server import _ServerOpts
+    lib = snu.load_library()
+    o = snu._Opts()
+    lib.snu_default_opts(C.byref(o))
+    assert o.fp64_growth == 1e3 and o.gemm_split == snu.SPLIT_AUTO
+    assert C.sizeof(snu._Opts) == 72 and C.sizeof(snu._Stats) == 120
+    so = _ServerOpts()
+    lib.snu_server_default_opts(C.byref(so))
+    assert so.gemm_split == snu.SPLIT_TF32
+    for kw in ({"gemm_split": 3}, {"gemm_split": -1}, {"fp64_growth": -1.0}):
+        with pytest.raises(snu.SnuError) as e:
+            snu.Solver(**kw)
+        assert e.value.status == 1, kw
+    snu.Solver(gemm_split=snu.SPLIT_TF32, fp64_growth=0.0).close()
+
+
 def test_bad_csr_rejected():
     s = snu.Solver(nleaves=2)
     with pytest.raises(snu.SnuError) as e:
