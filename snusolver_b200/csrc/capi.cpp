@@ -116,6 +116,20 @@ static void copy_runs(const std::vector<std::tuple<double*, const double*, size_
   for (auto& x : th) x.join();
 }
 
+// True when every column lies in page-locked (or device-visible) memory:
+// such columns are copied by DMA directly, not through the ring.
+static bool all_pinned(const double* const* cols, int nc) {
+  for (int r = 0; r < nc; r++) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, cols[r]) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (a.type == cudaMemoryTypeUnregistered) return false;
+  }
+  return true;
+}
+
 // The handle's pinned ring: two slots of up to 8 MiB (fewer for a small
 // transfer), made at the first host solve that needs them.
 static bool pin_ring(snu_handle* h, size_t want_elems) {
@@ -147,7 +161,7 @@ static bool pin_ring(snu_handle* h, size_t want_elems) {
 static bool columns_to_device(snu_handle* h, const double* const* cols, int nc, int n,
                        double* dev, cudaStream_t st) {
   const size_t total = (size_t)nc * n;
-  if (!pin_ring(h, total)) {
+  if (all_pinned(cols, nc) || !pin_ring(h, total)) {
     for (int r = 0; r < nc; r++)
       if (cudaMemcpyAsync(dev + (size_t)r * n, cols[r], sizeof(double) * n,
                           cudaMemcpyHostToDevice, st) != cudaSuccess)
@@ -181,7 +195,7 @@ static bool columns_to_device(snu_handle* h, const double* const* cols, int nc, 
 static bool columns_to_host(snu_handle* h, const double* dev, int nc, int n,
                      double* const* cols, cudaStream_t st) {
   const size_t total = (size_t)nc * n;
-  if (!pin_ring(h, total)) {
+  if (all_pinned(cols, nc) || !pin_ring(h, total)) {
     for (int r = 0; r < nc; r++)
       if (cudaMemcpyAsync(cols[r], dev + (size_t)r * n, sizeof(double) * n,
                           cudaMemcpyDeviceToHost, st) != cudaSuccess)
