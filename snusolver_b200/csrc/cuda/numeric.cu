@@ -1734,15 +1734,28 @@ class CudaEngine : public Engine {
           if (fi.p > O.K0 && inset(f))
             maxrows = std::max(maxrows, (fi.p + fi.q - O.K0 + NB - 1) / NB);
         }
+        // fronts with the longest tile chains in this block first (then
+        // the most rows), so the level's tail is short; every round of
+        // row chunks still follows the previous one, so a task waits only
+        // on tasks of lower index
+        std::vector<int> ford;
+        for (int f = L.f0; f < L.f1; f++)
+          if (inset(f) && fp.fronts[f].p > O.K0) ford.push_back(f);
+        auto tiles_in = [&](int f) {
+          return (std::min(OB, fp.fronts[f].p - O.K0) + NB - 1) / NB;
+        };
+        std::stable_sort(ford.begin(), ford.end(), [&](int x, int y) {
+          const int tx = tiles_in(x), ty = tiles_in(y);
+          if (tx != ty) return tx > ty;
+          return fp.fronts[x].p + fp.fronts[x].q > fp.fronts[y].p + fp.fronts[y].q;
+        });
         for (int r = 0; r < maxrows; r++)
-          for (int f = L.f0; f < L.f1; f++) {
+          for (int f : ford) {
             const FrontInfo& fi = fp.fronts[f];
-            if (inset(f) && fi.p > O.K0 && O.K0 + r * NB < fi.p + fi.q)
-              bt.push_back({f, 0, r});
+            if (O.K0 + r * NB < fi.p + fi.q) bt.push_back({f, 0, r});
           }
-        for (int f = L.f0; f < L.f1; f++) {
+        for (int f : ford) {
           const FrontInfo& fi = fp.fronts[f];
-          if (fi.p <= O.K0 || !inset(f)) continue;
           const int K0 = O.K0, K1 = std::min(K0 + OB, fi.p), dim = fi.p + fi.q;
           for (int c = 0; K1 + c * NB < dim; c++) bt.push_back({f, 1, c});
           const int64_t o = fi.offset, ld = fi.ld;
