@@ -214,6 +214,7 @@ class CudaEngine : public Engine {
     CK(cudaEventCreate(&ev1_));
     CK(cudaEventCreate(&sev0_));
     CK(cudaEventCreate(&sev1_));
+    for (cudaEvent_t& e : stev_) CK(cudaEventCreate(&e));
     CK(cudaFuncSetAttribute(k_diag_lu_inv<double>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)diag_smem<double>()));
@@ -637,6 +638,12 @@ class CudaEngine : public Engine {
     CK(cudaMemsetAsync(d_flags_ + 4, 0, sizeof(int), st));
     CK(cudaEventRecord(sev0_, st));
     SolveReport r;
+    // (the sweep form may be timed on this path only)
+    struct TuneScope {
+      bool& f;
+      explicit TuneScope(bool& x) : f(x) { f = true; }
+      ~TuneScope() { f = false; }
+    } tune_scope(sweep_tune_ok_);
     if (precision == 0) {
       if ((rc = tree_solve_cols<double>(d_F64_, d_I64_, d_W64_, d_Y64_, dB,
                                         ldb, dX, ldb, nrhs, st)))
@@ -1223,6 +1230,10 @@ class CudaEngine : public Engine {
     if (sev0_) cudaEventDestroy(sev0_);
     if (sev1_) cudaEventDestroy(sev1_);
     sev0_ = sev1_ = nullptr;
+    for (cudaEvent_t& e : stev_) {
+      if (e) cudaEventDestroy(e);
+      e = nullptr;
+    }
     for (cudaEvent_t e : pev_) cudaEventDestroy(e);
     pev_.clear();
     // autotuner events left by a tuning pass that stopped on an error
@@ -2081,11 +2092,38 @@ class CudaEngine : public Engine {
     const int g = group > 0 ? std::min(group, pass_cols()) : pass_cols();
     for (int c0 = 0; c0 < nrhs; c0 += g) {
       const int nc = std::min(g, nrhs - c0);
-      int rc = fused_solve_
-                   ? tree_solve_fused<T>(F, I, W, Y, B + (size_t)c0 * ldb, ldb,
-                                         X + (size_t)c0 * ldx, ldx, nc, st)
-                   : tree_solve<T>(F, I, W, Y, B + (size_t)c0 * ldb, ldb,
-                                   X + (size_t)c0 * ldx, ldx, nc, st);
+      // (per precision and register-group width 1, 2, 4, 8, 16)
+      const int wcls = nc <= 1 ? 0 : nc <= 2 ? 1 : nc <= 4 ? 2 : nc <= 8 ? 3 : 4;
+      int& pick = sweep_pick_[sizeof(T) == 8 ? 1 : 0][wcls];
+      const double* Bc = B + (size_t)c0 * ldb;
+      double* Xc = X + (size_t)c0 * ldx;
+      // a pass of <= RG columns: the whole-tree sweeps where they are the
+      // faster form for this handle (timed on its first such pass: they
+      // win where launches dominate, small fronts and few columns)
+      bool fused = fused_solve_;
+      if (!fused && nc <= RG && !deterministic_) {
+        if (pick < 0 && sweep_tune_ok_ && !prof_mask_) {
+          int rc;
+          CK(cudaEventRecord(stev_[0], st));
+          if ((rc = tree_solve<T>(F, I, W, Y, Bc, ldb, Xc, ldx, nc, st))) return rc;
+          CK(cudaEventRecord(stev_[1], st));
+          if ((rc = tree_solve_fused<T>(F, I, W, Y, Bc, ldb, Xc, ldx, nc, st)))
+            return rc;
+          CK(cudaEventRecord(stev_[2], st));
+          CK(cudaEventSynchronize(stev_[2]));
+          float a = 0, b = 0;
+          CK(cudaEventElapsedTime(&a, stev_[0], stev_[1]));
+          CK(cudaEventElapsedTime(&b, stev_[1], stev_[2]));
+          pick = b < a ? 1 : 0;
+          if (verbose_)
+            fprintf(stderr, "snusolver: sweeps of %d columns: level by level "
+                    "%.3f ms, whole tree %.3f ms\n", nc, a, b);
+          continue;  // (X holds the second, equal solve)
+        }
+        fused = pick == 1;
+      }
+      int rc = fused ? tree_solve_fused<T>(F, I, W, Y, Bc, ldb, Xc, ldx, nc, st)
+                     : tree_solve<T>(F, I, W, Y, Bc, ldb, Xc, ldx, nc, st);
       if (rc) return rc;
     }
     return ENG_OK;
@@ -2853,6 +2891,12 @@ class CudaEngine : public Engine {
   double *d_W64_ = nullptr, *d_R_ = nullptr, *d_D_ = nullptr;
   float* d_W32_ = nullptr;
   bool have64_ = false, have32_ = false;
+  // sweep form of passes of <= RG columns, per precision (FP32, FP64) and
+  // register-group width (1, 2, 4, 8, 16): -1 untimed, 0 level by level,
+  // 1 whole tree; timed only inside solve()
+  int sweep_pick_[2][5] = {{-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1}};
+  bool sweep_tune_ok_ = false;
+  cudaEvent_t stev_[3] = {nullptr, nullptr, nullptr};
   // FP64 refactor of selected fronts (refinement stagnation): their level
   // schedule, assembly entries and the updates of their unselected
   // children (GEMMs, or extend-add tasks per child rank in the
