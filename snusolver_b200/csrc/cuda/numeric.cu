@@ -277,7 +277,7 @@ class CudaEngine : public Engine {
       // (the distributed schedules have the fused panel path only)
       use_block_ = !(pbk && pbk[0] == '0') || opt_.dist_world > 1;
       // SNU_TC_PANEL=N: FP32 panel products on the tensor cores for levels
-      // with at least N fronts (0: never)
+      // with at least N fronts (0: never); unset: the levels tc_level picks
       const char* tcp = getenv("SNU_TC_PANEL");
       if (tcp) tcpanel_min_ = atoi(tcp);
     }
@@ -1415,6 +1415,36 @@ class CudaEngine : public Engine {
     return ENG_OK;
   }
 
+  // Whether a level's FP32 panel products go to the tensor cores (block
+  // inverses, then L21 / U12 as GEMM batches; see tc_panel_schedule).
+  // SNU_TC_PANEL=N: levels of at least N fronts, 0: none.  By default the
+  // levels where it measured faster (64^3 7-point and 96^3 27-point): at
+  // least 4 fronts with pivots (levels of 1-2 fronts are bound by their
+  // tile chains, which this does not shorten) and at least 25 GFLOP of
+  // such products, at least 50 MFLOP per eligible front block (below that
+  // the block inverses cost more than the products save).
+  bool tc_level(const LevelSched& L) const {
+    if (tcpanel_min_ > 0) return L.f1 - L.f0 >= tcpanel_min_;
+    if (tcpanel_min_ == 0) return false;
+    const FrontPlan& fp = *fp_;
+    double fl = 0;
+    int nb = 0, nf = 0;
+    for (int f = L.f0; f < L.f1; f++) {
+      const FrontInfo& fi = fp.fronts[f];
+      if (fi.p <= 0) continue;
+      nf++;
+      const int dim = fi.p + fi.q;
+      for (int K0 = 0; K0 < fi.p; K0 += OB) {
+        const int K1 = std::min(K0 + OB, fi.p), KB = K1 - K0;
+        const int Rs = K0 + (KB + NB - 1) / NB * NB;
+        if (KB < 64 || dim - Rs < 64 || dim - K1 < 64) continue;
+        nb++;
+        fl += 2.0 * (dim - Rs) * KB * KB + 2.0 * (dim - K1) * KB * KB;
+      }
+    }
+    return nf >= 4 && fl >= 25e9 && fl >= 50e6 * nb;
+  }
+
   // The FP32 tensor-core panel variant of outer block O (see OuterBlock).
   // A front takes it when both panel products are large enough for the
   // tensor cores: KB >= 64 pivot columns in the block, >= 64 rows below its
@@ -1732,6 +1762,7 @@ class CudaEngine : public Engine {
       // fused path: per outer block the cooperative panel tasks and the
       // rank-(K1-K0) update of the rest of the pivot rows and columns
       const int nob = (maxp + OB - 1) / OB;
+      const bool tc_lev = !in && use_tc_ && tc_level(L);
       L.ob.assign(nob, OuterBlock());
       for (int b = 0; b < nob; b++) {
         OuterBlock& O = L.ob[b];
@@ -1787,8 +1818,7 @@ class CudaEngine : public Engine {
         O.ntasks = (int)bt.size();
         if (!bt.empty() && (rc = upload(O.tasks, bt))) return rc;
         if ((rc = gemm_batch(og, O.outer))) return rc;
-        if (!in && use_tc_ && tcpanel_min_ > 0 && L.f1 - L.f0 >= tcpanel_min_ &&
-            (rc = tc_panel_schedule(L, O, maxrows)))
+        if (!in && use_tc_ && tc_lev && (rc = tc_panel_schedule(L, O, maxrows)))
           return rc;
       }
       if (verbose_) {
@@ -2837,11 +2867,9 @@ class CudaEngine : public Engine {
   bool use_tc_ = true;
   bool use_graphs_ = true;
   bool use_block_ = true;
-  // FP32 tensor-core panel products for levels with at least this many
-  // fronts; off unless SNU_TC_PANEL sets it (on the 64^3 workload the
-  // inverse-based tensor-core products measured 0.5 ms slower per
-  // factorization than the fused kernel's SIMT products at leaf levels)
-  int tcpanel_min_ = 0;
+  // FP32 tensor-core panel products: levels with at least this many
+  // fronts (SNU_TC_PANEL); 0 none; -1 (default) the levels tc_level picks
+  int tcpanel_min_ = -1;
   int64_t invb_base_ = 0, invb_need_ = 0;  // triangle-inverse scratch (FP32)
   bool verbose_ = false;  // SNU_VERBOSE=1: set-up phase timings on stderr
   static double wall_s() {

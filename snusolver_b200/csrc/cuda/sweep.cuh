@@ -55,21 +55,26 @@ __device__ __forceinline__ void cp_async_wait_prev() {
 }
 
 // Spins (bounded) until *flag is set; on timeout sets *err and returns false.
+// The load is an acquire at GPU scope: the caller's CTA barrier after it
+// orders the CTA's reads of the published data after the flag.
 __device__ __forceinline__ bool wait_flag(const int* flag, int* err) {
   for (long it = 0; it < WAVE_SPIN_LIMIT; it++) {
-    if (*(const volatile int*)flag) {
-      __threadfence();  // order the flag read before the reads of Y
-      return true;
-    }
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(flag)
+                 : "memory");
+    if (v) return true;
     __nanosleep(64);
   }
   atomicExch(err, 1);
   return false;
 }
 
+// Sets *flag with a release at GPU scope (called by one thread after the
+// CTA barrier that follows the CTA's writes of the published data, which
+// the release orders before the flag).
 __device__ __forceinline__ void raise_flag(int* flag) {
-  __threadfence();
-  atomicExch(flag, 1);
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flag), "r"(1)
+               : "memory");
 }
 
 // Stages rows [r0, r1) of factor columns [k0, k0 + kb) of front f into
