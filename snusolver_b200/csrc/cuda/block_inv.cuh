@@ -53,7 +53,6 @@ __global__ void __launch_bounds__(256, 2)
   const float* Fo = F + f.off;
   const float* inv0 = INV + f.inv_off + (int64_t)(K0 / NB) * 2 * NB * NB +
                       (tk.tri ? NB * NB : 0);  // tile t: + t * 2 NB^2
-  const int r0 = PbMap<float>::r0(), c0 = PbMap<float>::c0();
   // the strip starts as zeros with the diagonal tile's inverse in place
   for (int e = threadIdx.x; e < T * TE; e += 256) X[e] = 0.f;
   __syncthreads();
@@ -82,7 +81,8 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
     for (int b = 0; b < 4; b++)
 #pragma unroll
-      for (int a = 0; a < 4; a++) S1[r0 + a + (c0 + 8 * b) * P] = tot[a][b];
+      for (int a = 0; a < 4; a++)
+        S1[PbMap<float>::row(a) + PbMap<float>::col(b) * P] = tot[a][b];
     // X(i) = -inv_i S1
     pb_load(S0, inv0 + (int64_t)i * 2 * NB * NB, (int64_t)NB, NB, NB);
     __syncthreads();
@@ -92,7 +92,8 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
     for (int b = 0; b < 4; b++)
 #pragma unroll
-      for (int a = 0; a < 4; a++) xi[r0 + a + (c0 + 8 * b) * P] = -acc[a][b];
+      for (int a = 0; a < 4; a++)
+        xi[PbMap<float>::row(a) + PbMap<float>::col(b) * P] = -acc[a][b];
     __syncthreads();
   }
   // the strip to global memory: tiles 0..T-1 of column strip j

@@ -38,23 +38,27 @@ struct BlockTask {
   int front, kind, chunk;  // kind 0: row chunk, 1: column chunk
 };
 
-// Register tile of a thread in the 64 x 64 products: rows r0 + RS a,
-// columns c0 + CS b (a, b < 4).  FP32: four contiguous rows (one vector
-// load), columns 8 apart, a warp covers 16 rows x 32 columns.  FP64 keeps
-// scalar loads (the products are bound by the FP64 pipe, not by shared
-// memory): rows 16 apart, columns 16 apart.
+// Register tile of a thread in the 64 x 64 products: rows row(a), columns
+// col(b) (a, b < 4).  FP32 holds the accumulator fragments of the tensor-
+// core products (pb_mm): rows r0 + {0, 1, 8, 9}, columns c0 + 8 b, a warp
+// covering 16 rows x 32 columns.  FP64 keeps scalar products (bound by the
+// FP64 pipe, not by shared memory): rows 16 apart, columns 16 apart.
 template <typename T>
 struct PbMap {
-  static constexpr int RS = sizeof(T) == 4 ? 1 : 16;
-  static constexpr int CS = sizeof(T) == 4 ? 8 : 16;
   __device__ __forceinline__ static int r0() {
     return sizeof(T) == 4
-               ? ((threadIdx.x >> 5) & 3) * 16 + (threadIdx.x & 3) * 4
+               ? ((threadIdx.x >> 5) & 3) * 16 + (threadIdx.x & 3) * 2
                : (threadIdx.x & 15);
   }
   __device__ __forceinline__ static int c0() {
     return sizeof(T) == 4 ? (threadIdx.x >> 7) * 32 + ((threadIdx.x >> 2) & 7)
                           : (threadIdx.x >> 4);
+  }
+  __device__ __forceinline__ static int row(int a) {
+    return sizeof(T) == 4 ? r0() + (a & 1) + 8 * (a >> 1) : r0() + 16 * a;
+  }
+  __device__ __forceinline__ static int col(int b) {
+    return c0() + (sizeof(T) == 4 ? 8 : 16) * b;
   }
 };
 
@@ -100,22 +104,42 @@ __device__ __forceinline__ void pb_load(T* S, const T* src, int64_t ld, int nr,
   }
 }
 
+// One value split into TF32 hi + lo (round to nearest, ties away):
+// hi carries the leading 11 bits, lo the next 11.
+__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+  const float r = x - __uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4],
+                                         uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
 // acc = A B for NB x NB shared tiles (leading dimension PLD, inner
-// dimension kk).  A is read four rows at a time, B two k at a time; the
-// operands are zero (or finite identity padding against zeros) past kk, so
-// the loop runs to kk rounded up to 8.
+// dimension kk); the operands are zero (or finite identity padding against
+// zeros) past kk, so the loop runs to kk rounded up to 8.
+// FP32: on the tensor cores, mma.sync m16n8k8 TF32 with the three-product
+// split (A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 accumulation: FP32-level
+// products), formed as C^T = B^T A^T so that each thread's accumulator
+// fragments are its PbMap elements.  A warp's 16 x 32 block is 2 x 2 MMA
+// tiles (16 columns x 8 rows each).  FP64: scalar FMA, 4 x 4 per thread.
 template <typename T>
 __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
                                       int kk) {
   constexpr int P = pld<T>();
-  const int r0 = PbMap<T>::r0(), c0 = PbMap<T>::c0();
-  const T* Ar = A + r0;
-  const T* Bc = B + c0 * P;
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b < 4; b++) acc[a][b] = (T)0;
   if constexpr (sizeof(T) == 8) {
+    const T* Ar = A + PbMap<T>::r0();
+    const T* Bc = B + PbMap<T>::c0() * P;
 #pragma unroll 8
     for (int m = 0; m < kk; m++) {
       T av[4], bv[4];
@@ -129,77 +153,118 @@ __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
         for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
     }
     return;
-  }
-  const int k8 = (kk + 7) & ~7;
+  } else {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int rb = 16 * (w & 3), cb = 32 * (w >> 2);
+    // d[i][j]: columns cb + 16 i + {g, g + 8}, rows rb + 8 j + 2 t + {0, 1}
+    float d[2][2][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) d[i][j][e] = 0.f;
+    const int k8 = (kk + 7) & ~7;
 #pragma unroll 2
-  for (int m = 0; m < k8; m += 2) {
-    T a0[4], a1[4], b0[4], b1[4];
-    ld4(Ar + m * P, a0);
-    ld4(Ar + (m + 1) * P, a1);
+    for (int k0 = 0; k0 < k8; k0 += 8) {
+      // MMA A operand (16 x 8, row-major) = B^T: element (m, k) = B(k, m)
+      uint32_t ah[2][4], al[2][4];
 #pragma unroll
-    for (int b = 0; b < 4; b++) ld2(Bc + m + 8 * b * P, b0[b], b1[b]);
-#pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-      for (int b = 0; b < 4; b++) {
-        acc[a][b] += a0[a] * b0[b];
-        acc[a][b] += a1[a] * b1[b];
+      for (int i = 0; i < 2; i++) {
+        const float* Bm = B + (k0 + t) + (cb + 16 * i + g) * P;
+        tf32_split(Bm[0], ah[i][0], al[i][0]);          // (g,     t)
+        tf32_split(Bm[8 * P], ah[i][1], al[i][1]);      // (g + 8, t)
+        tf32_split(Bm[4], ah[i][2], al[i][2]);          // (g,     t + 4)
+        tf32_split(Bm[4 + 8 * P], ah[i][3], al[i][3]);  // (g + 8, t + 4)
       }
+      // MMA B operand (8 x 8, column-major) = A^T: element (k, n) = A(n, k)
+      uint32_t bh[2][2], bl[2][2];
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const float* An = A + (rb + 8 * j + g) + (k0 + t) * P;
+        tf32_split(An[0], bh[j][0], bl[j][0]);      // (t,     g)
+        tf32_split(An[4 * P], bh[j][1], bl[j][1]);  // (t + 4, g)
+      }
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          mma_tf32(d[i][j], ah[i], bh[j][0], bh[j][1]);
+          mma_tf32(d[i][j], ah[i], bl[j][0], bl[j][1]);
+          mma_tf32(d[i][j], al[i], bh[j][0], bh[j][1]);
+        }
+    }
+    // fragment element e of tile (i, j): row 8 j + 2 t + (e & 1), column
+    // 16 i + g + 8 (e >> 1) -> acc[(e & 1) + 2 j][2 i + (e >> 1)]
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+          acc[(e & 1) + 2 * j][2 * i + (e >> 1)] = d[i][j][e];
   }
 }
 
 // dst(i, j) = acc (sub = false) or dst(i, j) -= acc (sub = true), i < nr,
 // j < nc; optionally the result also into the shared tile S (zero outside
-// nr x nc).  A thread's four rows of a column go as one vector when they
-// are all inside and 16-byte aligned.
+// nr x nc).  FP32: a thread's row pairs of a column go as one 8-byte vector
+// when both rows are inside and the pair is aligned.
 template <typename T>
 __device__ __forceinline__ void pb_store(T* dst, int64_t ld, int nr, int nc,
                                          const T (&acc)[4][4], bool sub,
                                          T* S) {
-  constexpr int P = pld<T>(), RS = PbMap<T>::RS, CS = PbMap<T>::CS;
-  const int r0 = PbMap<T>::r0(), c0 = PbMap<T>::c0();
-  const bool vec =
-      RS == 1 && aligned16(dst + r0) && (ld & 3) == 0 && r0 + 3 < nr;
+  constexpr int P = pld<T>();
+  const int r0 = PbMap<T>::r0();
+  const bool vec = sizeof(T) == 4 && ((reinterpret_cast<uintptr_t>(dst + r0) & 7) == 0) &&
+                   (ld & 1) == 0;
   T v[4][4];  // [b][a]
 #pragma unroll
   for (int b = 0; b < 4; b++) {
-    const int j = c0 + CS * b;
+    const int j = PbMap<T>::col(b);
     if (sub) {  // all reads in flight together
-      if (vec && j < nc) {
-        ldg4(dst + r0 + j * ld, v[b]);
-      } else {
 #pragma unroll
-        for (int a = 0; a < 4; a++) {
-          const int i = r0 + RS * a;
-          v[b][a] = (i < nr && j < nc) ? __ldcg(dst + i + j * ld) : (T)0;
+      for (int a = 0; a < 4; a += 2) {
+        const int i = PbMap<T>::row(a);
+        if (sizeof(T) == 4 && vec && j < nc && PbMap<T>::row(a + 1) < nr) {
+          const float2 q = __ldcg(reinterpret_cast<const float2*>(dst + i + j * ld));
+          v[b][a] = (T)q.x, v[b][a + 1] = (T)q.y;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const int ie = PbMap<T>::row(a + e);
+            v[b][a + e] = (ie < nr && j < nc) ? __ldcg(dst + ie + j * ld) : (T)0;
+          }
         }
       }
     }
   }
 #pragma unroll
   for (int b = 0; b < 4; b++) {
-    const int j = c0 + CS * b;
+    const int j = PbMap<T>::col(b);
 #pragma unroll
     for (int a = 0; a < 4; a++) {
-      const bool in = r0 + RS * a < nr && j < nc;
+      const bool in = PbMap<T>::row(a) < nr && j < nc;
       v[b][a] = in ? (sub ? v[b][a] - acc[a][b] : acc[a][b]) : (T)0;
     }
     if (j < nc) {
-      if (vec) {
-        st4(dst + r0 + j * ld, v[b]);
-      } else {
 #pragma unroll
-        for (int a = 0; a < 4; a++)
-          if (r0 + RS * a < nr) dst[r0 + RS * a + j * ld] = v[b][a];
+      for (int a = 0; a < 4; a += 2) {
+        const int i = PbMap<T>::row(a);
+        if (sizeof(T) == 4 && vec && PbMap<T>::row(a + 1) < nr) {
+          *reinterpret_cast<float2*>(dst + i + j * ld) =
+              make_float2((float)v[b][a], (float)v[b][a + 1]);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 2; e++)
+            if (PbMap<T>::row(a + e) < nr) dst[PbMap<T>::row(a + e) + j * ld] = v[b][a + e];
+        }
       }
     }
     if (S) {
-      if (RS == 1) {
-        st4(S + r0 + j * P, v[b]);
-      } else {
 #pragma unroll
-        for (int a = 0; a < 4; a++) S[r0 + RS * a + j * P] = v[b][a];
-      }
+      for (int a = 0; a < 4; a++) S[PbMap<T>::row(a) + j * P] = v[b][a];
     }
   }
 }
@@ -360,13 +425,11 @@ __global__ void __launch_bounds__(256, 2)
           __syncthreads();
           T acc[4][4];
           pb_mm(acc, S0, S1, NB);
-          const int r0 = PbMap<T>::r0(), c0 = PbMap<T>::c0();
 #pragma unroll
           for (int b = 0; b < 4; b++)
 #pragma unroll
             for (int a = 0; a < 4; a++)
-              S2[r0 + PbMap<T>::RS * a + (c0 + PbMap<T>::CS * b) * pld<T>()] -=
-                  acc[a][b];
+              S2[PbMap<T>::row(a) + PbMap<T>::col(b) * pld<T>()] -= acc[a][b];
           __syncthreads();
         }
         // U_t = Linv_t S2
