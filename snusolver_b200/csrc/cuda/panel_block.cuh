@@ -166,7 +166,7 @@ __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
 #pragma unroll
         for (int e = 0; e < 4; e++) d[i][j][e] = 0.f;
     const int k8 = (kk + 7) & ~7;
-#pragma unroll 2
+#pragma unroll 1
     for (int k0 = 0; k0 < k8; k0 += 8) {
       // MMA A operand (16 x 8, row-major) = B^T: element (m, k) = B(k, m)
       uint32_t ah[2][4], al[2][4];

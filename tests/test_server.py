@@ -17,7 +17,11 @@ from snusolver_b200 import generators
 from snusolver_b200.server import Server
 from util import rel_resid
 
-MIX_TOL = 1e-7
+# Both runs of a request refine to backward error <= 1e-10 from factors
+# that differ in rounding (sibling updates add with atomics in a different
+# order), so their solutions agree to about cond(A) x 1e-10; these
+# Laplacians have infinity-norm condition numbers of a few thousand.
+MIX_TOL = 1e-6
 
 
 def _mats():
