@@ -39,27 +39,21 @@ struct BlockTask {
 };
 
 // Register tile of a thread in the 64 x 64 products: rows row(a), columns
-// col(b) (a, b < 4).  FP32 holds the accumulator fragments of the tensor-
-// core products (pb_mm): rows r0 + {0, 1, 8, 9}, columns c0 + 8 b, a warp
-// covering 16 rows x 32 columns.  FP64 keeps scalar products (bound by the
-// FP64 pipe, not by shared memory): rows 16 apart, columns 16 apart.
+// col(b) (a, b < 4) -- the accumulator fragments of the tensor-core
+// products (pb_mm): rows r0 + {0, 1, 8, 9}, columns c0 + 8 b, a warp
+// covering 16 rows x 32 columns.
 template <typename T>
 struct PbMap {
   __device__ __forceinline__ static int r0() {
-    return sizeof(T) == 4
-               ? ((threadIdx.x >> 5) & 3) * 16 + (threadIdx.x & 3) * 2
-               : (threadIdx.x & 15);
+    return ((threadIdx.x >> 5) & 3) * 16 + (threadIdx.x & 3) * 2;
   }
   __device__ __forceinline__ static int c0() {
-    return sizeof(T) == 4 ? (threadIdx.x >> 7) * 32 + ((threadIdx.x >> 2) & 7)
-                          : (threadIdx.x >> 4);
+    return (threadIdx.x >> 7) * 32 + ((threadIdx.x >> 2) & 7);
   }
   __device__ __forceinline__ static int row(int a) {
-    return sizeof(T) == 4 ? r0() + (a & 1) + 8 * (a >> 1) : r0() + 16 * a;
+    return r0() + (a & 1) + 8 * (a >> 1);
   }
-  __device__ __forceinline__ static int col(int b) {
-    return c0() + (sizeof(T) == 4 ? 8 : 16) * b;
-  }
+  __device__ __forceinline__ static int col(int b) { return c0() + 8 * b; }
 };
 
 // S(i, j) = src(i, j) for i < nr, j < nc, zero elsewhere (NB x NB tile,
@@ -112,6 +106,14 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) 
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
 }
 
+__device__ __forceinline__ void mma_f64(double (&d)[2], double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, "
+      "{%0,%1};"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
 __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4],
                                          uint32_t b0, uint32_t b1) {
   asm volatile(
@@ -124,11 +126,12 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4],
 // acc = A B for NB x NB shared tiles (leading dimension PLD, inner
 // dimension kk); the operands are zero (or finite identity padding against
 // zeros) past kk, so the loop runs to kk rounded up to 8.
-// FP32: on the tensor cores, mma.sync m16n8k8 TF32 with the three-product
-// split (A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 accumulation: FP32-level
-// products), formed as C^T = B^T A^T so that each thread's accumulator
-// fragments are its PbMap elements.  A warp's 16 x 32 block is 2 x 2 MMA
-// tiles (16 columns x 8 rows each).  FP64: scalar FMA, 4 x 4 per thread.
+// On the tensor cores, formed as C^T = B^T A^T so that each thread's
+// accumulator fragments are its PbMap elements.  FP32: mma.sync m16n8k8
+// TF32 with the three-product split (A_hi B_hi + A_hi B_lo + A_lo B_hi,
+// FP32 accumulation: FP32-level products); a warp's 16 x 32 block is 2 x 2
+// MMA tiles (16 columns x 8 rows each).  FP64: mma.sync m8n8k4 f64 (exact
+// FP64 products); the block is 4 x 2 tiles (8 columns x 8 rows each).
 template <typename T>
 __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
                                       int kk) {
@@ -138,20 +141,37 @@ __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
 #pragma unroll
     for (int b = 0; b < 4; b++) acc[a][b] = (T)0;
   if constexpr (sizeof(T) == 8) {
-    const T* Ar = A + PbMap<T>::r0();
-    const T* Bc = B + PbMap<T>::c0() * P;
-#pragma unroll 8
-    for (int m = 0; m < kk; m++) {
-      T av[4], bv[4];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int rb = 16 * (w & 3), cb = 32 * (w >> 2);
+    // d[i][j]: column cb + 8 i + g, rows rb + 8 j + 2 t + {0, 1}
+    double d[4][2][2];
 #pragma unroll
-      for (int a = 0; a < 4; a++) av[a] = Ar[16 * a + m * P];
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-      for (int b = 0; b < 4; b++) bv[b] = Bc[m + 16 * b * P];
+      for (int j = 0; j < 2; j++) d[i][j][0] = d[i][j][1] = 0.0;
+    const int k4 = (kk + 3) & ~3;
+#pragma unroll 2
+    for (int k0 = 0; k0 < k4; k0 += 4) {
+      double av[4], bv[2];
 #pragma unroll
-      for (int a = 0; a < 4; a++)
+      for (int i = 0; i < 4; i++)  // MMA A = B^T: (m, k) = B(k, m), lane (g, t)
+        av[i] = B[(k0 + t) + (cb + 8 * i + g) * P];
 #pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
+      for (int j = 0; j < 2; j++)  // MMA B = A^T: (k, n) = A(n, k), lane (t, g)
+        bv[j] = A[(rb + 8 * j + g) + (k0 + t) * P];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) mma_f64(d[i][j], av[i], bv[j]);
     }
+    // element e of tile (i, j): row 8 j + 2 t + e, column 8 i + g
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) acc[e + 2 * j][i] = d[i][j][e];
     return;
   } else {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
