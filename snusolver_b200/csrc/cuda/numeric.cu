@@ -537,8 +537,10 @@ class CudaEngine : public Engine {
       if (!d_F32_ && (rc = alloc(d_F32_, (size_t)(invb_base_ + invb_need_)))) return rc;
       if (!d_I32_ && (rc = alloc(d_I32_, (size_t)invtot_))) return rc;
     }
+    // (the deterministic mode keeps the plan's default GEMM variants: a
+    // timed choice could differ from run to run)
     if (phase == 0 && precision == 1 && autotune_ && !tuned_ && force_tcp_ < 0 &&
-        force_width_ < 0) {
+        force_width_ < 0 && !deterministic_) {
       if ((rc = autotune())) return rc;
     }
     if (phase != 2) {  // (phase 2 adds to phase 1's counts)
