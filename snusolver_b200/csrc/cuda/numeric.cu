@@ -164,6 +164,8 @@ struct LevelSched {
   std::vector<EaTask*> ea_kids_r;
   std::vector<int> nea_kids_r;
   int* list = nullptr;  // fronts of the level (of the schedule's set)
+  int* list_all = nullptr;  // level 0 only: the schedule's fronts, all levels
+  int nlist_all = 0;
   int* listq = nullptr; // those with q > 0
   int nlist = 0, nlistq = 0;
   std::vector<Step> steps;
@@ -1022,7 +1024,8 @@ class CudaEngine : public Engine {
   // at most what the device holds at once, blocks stride over the tasks.
   template <typename T, int R>
   int diag_launch(bool fwd, const SweepTask* tasks, int ntasks, const T* F,
-                  const T* I, int nrhs, T* W, T* Y, cudaStream_t st) {
+                  const T* I, int nrhs, T* W, T* Y, double* X, int ldx,
+                  cudaStream_t st) {
     auto k = fwd ? k_fwd_diag<T, R> : k_bwd_diag<T, R>;
     // one task chain per column group of R columns
     const int ngroups = (nrhs + R - 1) / R;
@@ -1043,7 +1046,8 @@ class CudaEngine : public Engine {
     CK(cudaLaunchKernelEx(&cfg, k, tasks, ntasks, ngroups,
                           (const FrontDev*)d_fr_, F, I,
                           (const int64_t*)d_flag_off_, (int64_t)ntileflags_,
-                          nrhs, W, Y, fl, ctr, d_flags_ + 4));
+                          nrhs, W, Y, (const int*)d_gidx_, X, ldx, fl, ctr,
+                          d_flags_ + 4));
     return ENG_OK;
   }
   template <typename T, int R>
@@ -1103,17 +1107,20 @@ class CudaEngine : public Engine {
   }
 
   template <typename T>
+  // (X: the backward sweep's pivot solutions also go there, ldx apart;
+  // null for none)
   int diag_sweep(bool fwd, const SweepTask* tasks, int ntasks, const T* F,
-                 const T* I, int nrhs, T* W, T* Y, cudaStream_t st) {
+                 const T* I, int nrhs, T* W, T* Y, double* X, int ldx,
+                 cudaStream_t st) {
     if (nrhs > SOLVE_COLS) {
       err_ = "pivot-block sweep called with more than 64 right-hand sides";
       return ENG_EINVAL;
     }
-    if (nrhs <= 1) return diag_launch<T, 1>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
-    if (nrhs <= 2) return diag_launch<T, 2>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
-    if (nrhs <= 4) return diag_launch<T, 4>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
-    if (nrhs <= 8) return diag_launch<T, 8>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
-    return diag_launch<T, 16>(fwd, tasks, ntasks, F, I, nrhs, W, Y, st);
+    if (nrhs <= 1) return diag_launch<T, 1>(fwd, tasks, ntasks, F, I, nrhs, W, Y, X, ldx, st);
+    if (nrhs <= 2) return diag_launch<T, 2>(fwd, tasks, ntasks, F, I, nrhs, W, Y, X, ldx, st);
+    if (nrhs <= 4) return diag_launch<T, 4>(fwd, tasks, ntasks, F, I, nrhs, W, Y, X, ldx, st);
+    if (nrhs <= 8) return diag_launch<T, 8>(fwd, tasks, ntasks, F, I, nrhs, W, Y, X, ldx, st);
+    return diag_launch<T, 16>(fwd, tasks, ntasks, F, I, nrhs, W, Y, X, ldx, st);
   }
 
   // --------------------------------------------------------- profiling
@@ -1629,6 +1636,7 @@ class CudaEngine : public Engine {
     const FrontPlan& fp = *fp_;
     auto inset = [&](int f) { return in == nullptr || (*in)[f] != 0; };
     lvs.assign(nlevels_, LevelSched());
+    std::vector<int> all_fronts;
     int mc = fp.max_children;
     int rc;
     int& obc = obc_;  // outer-block launches so far (task counters)
@@ -1652,6 +1660,7 @@ class CudaEngine : public Engine {
       }
       L.nlist = (int)list.size();
       if ((rc = upload(L.list, list))) return rc;
+      all_fronts.insert(all_fronts.end(), list.begin(), list.end());
       L.nlistq = (int)listq.size();
       if ((rc = upload(L.listq, listq))) return rc;
       L.ea.assign(mc, nullptr);
@@ -1875,6 +1884,11 @@ class CudaEngine : public Engine {
       if (!gl.empty() && (rc = upload(L.gl, gl))) return rc;
       L.ngq = (int)gq.size();
       if (!gq.empty() && (rc = upload(L.gq, gq))) return rc;
+    }
+    if (nlevels_ > 0) {
+      lvs[0].nlist_all = (int)all_fronts.size();
+      if (!all_fronts.empty() && (rc = upload(lvs[0].list_all, all_fronts)))
+        return rc;
     }
     return ENG_OK;
   }
@@ -2282,16 +2296,23 @@ class CudaEngine : public Engine {
     int pi, rc;
     ctr_off_ = ctr_off;
     if (fwd) {
+      // every front's work vector starts as B's pivot rows and zeros, in
+      // one launch for the schedule (no level reads another's before its
+      // own level)
+      if (init && nlevels_ > 0 && lvs[0].nlist_all) {
+        cur_level_ = -1;
+        pi = prof_begin(KF_SOLVE_MISC, st);
+        k_solve_init<T><<<SOLVE_SPLIT * lvs[0].nlist_all, 256, 0, st>>>(
+            lvs[0].list_all, d_fr_, d_gidx_, B, ldb, nrhs, W);
+        CKL();
+        double el = 0;
+        for (int l = 0; l < nlevels_; l++) el += lvs[l].solve_elems;
+        prof_end(pi, KF_SOLVE_MISC, st, 0, el * nrhs * (es + 12));
+      }
       for (int l = 0; l < nlevels_; l++) {
         const LevelSched& L = lvs[l];
         cur_level_ = l;
-        const int nf = L.nlist;
         pi = prof_begin(KF_SOLVE_MISC, st);
-        if (init && nf) {
-          k_solve_init<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_,
-                                                       B, ldb, nrhs, W);
-          CKL();
-        }
         if (deterministic_) {
           for (size_t r = 0; r < L.nea_kids_r.size(); r++)
             if (L.nea_kids_r[r]) {
@@ -2307,7 +2328,8 @@ class CudaEngine : public Engine {
         prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
         if (L.nwf) {
           pi = prof_begin(KF_SOLVE_DIAG, st);
-          if ((rc = diag_sweep<T>(true, L.wf, L.nwf, F, I, nrhs, W, Y, st)))
+          if ((rc = diag_sweep<T>(true, L.wf, L.nwf, F, I, nrhs, W, Y, nullptr,
+                                  0, st)))
             return rc;
           prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.diag_elems * nrhs,
                    L.diag_elems * es);
@@ -2342,16 +2364,13 @@ class CudaEngine : public Engine {
         }
         if (L.nwb) {
           pi = prof_begin(KF_SOLVE_DIAG, st);
-          if ((rc = diag_sweep<T>(false, L.wb, L.nwb, F, I, nrhs, W, Y, st)))
+          // (the pivot solutions go to X there: the final unpermute)
+          if ((rc = diag_sweep<T>(false, L.wb, L.nwb, F, I, nrhs, W, Y, X, ldx,
+                                  st)))
             return rc;
           prof_end(pi, KF_SOLVE_DIAG, st, 2.0 * L.diag_elems * nrhs,
                    L.diag_elems * es);
         }
-        pi = prof_begin(KF_SOLVE_MISC, st);
-        k_scatter_y<T><<<SOLVE_SPLIT * nf, 256, 0, st>>>(L.list, d_fr_, d_gidx_, Y,
-                                                    nrhs, X, ldx);
-        CKL();
-        prof_end(pi, KF_SOLVE_MISC, st, 0, L.solve_elems * nrhs * (es + 12));
       }
     }
     cur_level_ = -1;

@@ -133,7 +133,9 @@ __global__ void __launch_bounds__(DIAG_ROWS)
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                const T* __restrict__ INV, const int64_t* __restrict__ flag_off,
                int64_t gstride, int nrhs, T* __restrict__ W,
-               T* __restrict__ Y, int* flags, int* next_task, int* err) {
+               T* __restrict__ Y, const int* __restrict__ gidx,
+               double* __restrict__ X, int ldx, int* flags, int* next_task,
+               int* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls0 = reinterpret_cast<T*>(smem_raw);  // [2][NB][DIAG_ROWS]
   T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;         // [2][NB * NB]
@@ -247,7 +249,9 @@ __global__ void __launch_bounds__(DIAG_ROWS)
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                const T* __restrict__ INV, const int64_t* __restrict__ flag_off,
                int64_t gstride, int nrhs, T* __restrict__ W,
-               T* __restrict__ Y, int* flags, int* next_task, int* err) {
+               T* __restrict__ Y, const int* __restrict__ gidx,
+               double* __restrict__ X, int ldx, int* flags, int* next_task,
+               int* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls0 = reinterpret_cast<T*>(smem_raw);
   T* Xs0 = Ls0 + 2 * NB * DIAG_ROWS;
@@ -314,6 +318,14 @@ __global__ void __launch_bounds__(DIAG_ROWS)
           tile_apply<T, R>(Xs, ws, xs, Yf, f.p, k0, kb, r0, nr);
           __syncthreads();
           if (tid == 0) raise_flag(fl + s);
+          if (X) {  // the tile's final solution also into X (original rows)
+            const int* g = gidx + f.idx_off;
+            for (int e = tid; e < NB * R; e += blockDim.x) {
+              const int i = e % NB, r = e / NB;
+              if (i < kb && r < nr)
+                X[g[k0 + i] + (int64_t)(r0 + r) * ldx] = (double)xs[i][r];
+            }
+          }
         } else {
           for (int e = tid; e < NB * R; e += blockDim.x) {
             const int i = e % NB, r = e / NB;
@@ -472,24 +484,6 @@ __global__ void __launch_bounds__(256)
                const FrontDev* __restrict__ fr, const T* __restrict__ F,
                int nrhs, T* __restrict__ W, const T* __restrict__ Y) {
   gemv_off<T, R, false>(tasks, ntasks, fr, F, nrhs, W, Y);
-}
-
-// X[gidx[t]] = Y[t] for the pivot rows of every front of a level.
-template <typename T>
-__global__ void k_scatter_y(const int* __restrict__ list,
-                            const FrontDev* __restrict__ fr,
-                            const int* __restrict__ gidx,
-                            const T* __restrict__ Y, int nrhs,
-                            double* __restrict__ X, int ldx) {
-  const FrontDev f = fr[list[blockIdx.x / SOLVE_SPLIT]];
-  const T* y = Y + f.y_off * nrhs;
-  const int* g = gidx + f.idx_off;
-  for (int t = (blockIdx.x % SOLVE_SPLIT) * blockDim.x + threadIdx.x; t < f.p;
-       t += SOLVE_SPLIT * blockDim.x) {
-    const int64_t gt = g[t];
-    for (int r = 0; r < nrhs; r++)
-      X[gt + (int64_t)r * ldx] = (double)y[t + (int64_t)r * f.p];
-  }
 }
 
 }  // namespace snu
