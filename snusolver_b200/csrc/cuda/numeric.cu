@@ -298,11 +298,11 @@ class CudaEngine : public Engine {
           (rc2 = fused_attr<float, 8>()) || (rc2 = fused_attr<float, 16>()))
         return rc2;
       // SNU_SOLVE_FUSED=1: whole-tree sweeps (one launch per direction)
-      // instead of the level-by-level sweeps.  Off by default: on the
-      // 64^3 workload they measured 0.5 ms slower per factor+solve (the
-      // chain through the tree levels, not launches, bounds both)
+      // for every pass; =0: the level-by-level sweeps for every pass;
+      // unset: each handle times both on its first pass of each width
       const char* sf = getenv("SNU_SOLVE_FUSED");
       fused_solve_ = sf && sf[0] == '1' && !deterministic_;
+      level_solve_ = sf && sf[0] == '0';
     }
     {
       int sms = 0;
@@ -2147,24 +2147,28 @@ class CudaEngine : public Engine {
       // faster form for this handle (timed on its first such pass: they
       // win where launches dominate, small fronts and few columns)
       bool fused = fused_solve_;
-      if (!fused && nc <= RG && !deterministic_) {
+      if (!fused && !level_solve_ && nc <= RG && !deterministic_) {
         if (pick < 0 && sweep_tune_ok_ && !prof_mask_) {
+          // each form twice, in the order L F F L (neither gains from
+          // running first or last), the faster of each pair compared
           int rc;
-          CK(cudaEventRecord(stev_[0], st));
-          if ((rc = tree_solve<T>(F, I, W, Y, Bc, ldb, Xc, ldx, nc, st))) return rc;
-          CK(cudaEventRecord(stev_[1], st));
-          if ((rc = tree_solve_fused<T>(F, I, W, Y, Bc, ldb, Xc, ldx, nc, st)))
-            return rc;
-          CK(cudaEventRecord(stev_[2], st));
-          CK(cudaEventSynchronize(stev_[2]));
-          float a = 0, b = 0;
-          CK(cudaEventElapsedTime(&a, stev_[0], stev_[1]));
-          CK(cudaEventElapsedTime(&b, stev_[1], stev_[2]));
+          float t[4];
+          for (int k = 0; k < 4; k++) {
+            CK(cudaEventRecord(stev_[0], st));
+            rc = (k == 1 || k == 2)
+                     ? tree_solve_fused<T>(F, I, W, Y, Bc, ldb, Xc, ldx, nc, st)
+                     : tree_solve<T>(F, I, W, Y, Bc, ldb, Xc, ldx, nc, st);
+            if (rc) return rc;
+            CK(cudaEventRecord(stev_[1], st));
+            CK(cudaEventSynchronize(stev_[1]));
+            CK(cudaEventElapsedTime(&t[k], stev_[0], stev_[1]));
+          }
+          const float a = std::min(t[0], t[3]), b = std::min(t[1], t[2]);
           pick = b < a ? 1 : 0;
           if (verbose_)
             fprintf(stderr, "snusolver: sweeps of %d columns: level by level "
                     "%.3f ms, whole tree %.3f ms\n", nc, a, b);
-          continue;  // (X holds the second, equal solve)
+          continue;  // (X holds the last, equal solve)
         }
         fused = pick == 1;
       }
@@ -2898,8 +2902,8 @@ class CudaEngine : public Engine {
                std::chrono::steady_clock::now().time_since_epoch())
         .count();
   }
-  // whole-tree sweeps instead of the level-by-level sweeps (SNU_SOLVE_FUSED)
-  bool fused_solve_ = false;
+  // whole-tree or level-by-level sweeps for every pass (SNU_SOLVE_FUSED)
+  bool fused_solve_ = false, level_solve_ = false;
   SolveTask* d_fwd_tasks_ = nullptr;
   SolveTask* d_bwd_tasks_ = nullptr;
   int nfwd_ = 0, nbwd_ = 0;

@@ -227,6 +227,7 @@ def test_autotuned_factorization_matches(gpu, tmp_path):
                                  ("SNU_TC_PERSIST", "1"), ("SNU_TC_PERSIST", "0"),
                                  ("SNU_GRAPHS", "0"), ("SNU_TC_PANEL", "0"),
                                  ("SNU_TC_PANEL", "1"), ("SNU_SOLVE_FUSED", "1"),
+                                 ("SNU_SOLVE_FUSED", "0"),
                                  ("SNU_TC_WIDTH", "64"), ("SNU_DMMA", "0"),
                                  ("SNU_SPLIT", "tf32"), ("SNU_SPLIT", "bf16"),
                                  ("SNU_DETERMINISTIC", "1")])
