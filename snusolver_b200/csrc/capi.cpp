@@ -139,7 +139,7 @@ static bool pin_ring(snu_handle* h, size_t want_elems) {
   h->hpin = nullptr;
   h->pin_elems = 0;
   if (cudaHostAlloc((void**)&h->hpin, 2 * slot * sizeof(double),
-                    cudaHostAllocDefault) != cudaSuccess) {
+                    cudaHostAllocPortable) != cudaSuccess) {
     cudaGetLastError();
     h->hpin = nullptr;
     return false;
@@ -245,6 +245,9 @@ snu_status solve_pieces(snu_handle* h, const std::vector<SolvePiece>& pieces) {
   }
   const int nrhs = (int)cols.size();
   if (nrhs == 0) return fail(h, SNU_EINVAL, "no right-hand sides");
+  // (staging, pinned ring and its events on the handle's device)
+  if (cudaSetDevice(h->opts.device) != cudaSuccess)
+    return fail(h, SNU_ECUDA, "cannot select the handle's device");
   // staged in chunks of up to 64 columns (one refinement loop per chunk),
   // so device staging stays bounded
   const int chunk = std::min(nrhs, 64);
