@@ -192,8 +192,7 @@ SNU_API snu_status snu_get_stats(const snu_handle* h, snu_stats* st);
    (every call rewrites what it reads), so calls whose GPU work overlaps
    (other streams, threads or handles on the same device) race.  The first
    call on a device looks up the array's device address
-   (cudaGetSymbolAddress); make that first call before any stream capture.
-   The call returns after the solve has finished on the stream.  With
+   (cudaGetSymbolAddress).  The call returns after the solve has finished on the stream.  With
    SNU_FP32_IR, refinement that would need the FP64 fallback (which
    allocates) stops with SNU_ENOTCONV instead; X then holds the refined
    FP32 solution and snu_get_stats its backward error. */
