@@ -404,10 +404,10 @@ class CudaEngine : public Engine {
       tflags_size_ =
           2 * SWEEP_GROUPS * ntileflags_ + 4 * (int64_t)nlevels_ + 2;
       if ((rc = alloc(d_tflags_, (size_t)tflags_size_))) return rc;
-      // fused panel path: two flags per tile, then one task counter per
+      // fused panel path: four flags per tile, then one task counter per
       // outer-block launch (a level has no more outer blocks than tiles)
       // (counters for the outer blocks of up to two schedules' launches)
-      if ((rc = alloc(d_fflags_, (size_t)(4 * ntileflags_)))) return rc;
+      if ((rc = alloc(d_fflags_, (size_t)(6 * ntileflags_)))) return rc;
     }
     if ((rc = upload(d_fr_, frh_))) return rc;
     if ((rc = upload(d_gidx_, fp.gidx))) return rc;
@@ -997,7 +997,7 @@ class CudaEngine : public Engine {
     CK(cudaLaunchKernelEx(&cfg, k, tasks, ntasks,
                           (const FrontDev*)d_fr_, F, I, O.K0, opt_.pivot_eps,
                           d_flags_, d_fflags_, (const int64_t*)d_flag_off_,
-                          d_fflags_ + 2 * ntileflags_ + O.ctr, d_flags_ + 5));
+                          d_fflags_ + 4 * ntileflags_ + O.ctr, d_flags_ + 5));
     return ENG_OK;
   }
 
@@ -2046,7 +2046,7 @@ class CudaEngine : public Engine {
       const int* aval = phase == 1 ? d_asm1_val_ : d_asm_val_;
       int pi = prof_begin(KF_ASSEMBLE, st);
       CK(cudaMemsetAsync(F, 0, sizeof(T) * arena_, st));
-      CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 4 * ntileflags_, st));
+      CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 6 * ntileflags_, st));
       if (na > 0) {
         int blocks = (int)std::min<int64_t>((na + 255) / 256, 148 * 16);
         k_assemble<T><<<blocks, 256, 0, st>>>(apos, aval, d_vals_, F, na);
@@ -2815,7 +2815,7 @@ class CudaEngine : public Engine {
                                                          d_F64_);
         CKL();
       }
-    CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 4 * ntileflags_, ms));
+    CK(cudaMemsetAsync(d_fflags_, 0, sizeof(int) * 6 * ntileflags_, ms));
     CK(cudaMemsetAsync(d_flags_, 0, 4 * sizeof(int), ms));
     CK(cudaMemsetAsync(d_flags_ + 5, 0, sizeof(int), ms));
     if ((rc = run_factor<double>(d_F64_, d_I64_, 3))) return rc;

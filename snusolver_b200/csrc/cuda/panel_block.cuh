@@ -6,15 +6,30 @@
 //
 // * row task r covers rows [K0 + 64 r, +64) of the front.  Task r < nt owns
 //   tile r: at step r it factors the diagonal tile (LU and the inverses of
-//   its triangles, the reference's getrf without pivoting), writes the U
-//   rows of the tile inside the block (U = Linv A, columns [k1, K1)) and
-//   raises the tile's flag.  At every earlier step t (and at every step for
-//   rows below the block) it waits for tile t's flag, forms its L block
+//   its triangles, the reference's getrf without pivoting), publishes it,
+//   and then writes the tile's U rows (U = Linv A) right of the next tile
+//   (columns [k1 + 64, K1)).  At every earlier step t (and at every step for
+//   rows below the block) it waits for tile t, forms its L block
 //   (L = A Uinv_t, the reference's trsm) and applies the rank-64 update of
 //   its rows inside the block (columns [k1, K1)).
+// * the next tile's owner (task t + 1 at step t) carries the chain: while
+//   tile t is factored it applies the previous step's update to tile t's
+//   rows in its own columns; once tile t is published it forms tile t's U
+//   rows there (Linv_t times that), its own L block, the update of its
+//   diagonal tile, and factors it.  Only one product lies between two tile
+//   factorizations on the chain's critical path besides the L and U blocks
+//   of the next tile.
 // * column task c covers columns [K1 + 64 c, +64): for every tile t it waits
-//   for the flag and forms U_t = Linv_t (A_t - sum_{s<t} L_ts U_s) for its
+//   for the tile and forms U_t = Linv_t (A_t - sum_{s<t} L_ts U_s) for its
 //   columns (the U12 rows of the block, right of it).
+//
+// Four flags per tile s: [4 s] tile s factored (the tile, its inverses and
+// every L block of its rows stored), [4 s + 1] its owner's U rows right of
+// the next tile stored, [4 s + 2] its U rows in the next tile's columns
+// stored (by the next tile's owner), [4 s + 3] the next tile's L block of
+// step s stored.  Every product is formed from the same operands in the
+// same order as by a single owner of the chain, so the factors do not
+// depend on which task forms them.
 //
 // The rest of the pivot rows / columns then takes one rank-(K1-K0) update
 // (a tensor-core GEMM) before the next outer block; F22 takes the rank-p
@@ -289,6 +304,28 @@ __device__ __forceinline__ void pb_store(T* dst, int64_t ld, int nr, int nc,
   }
 }
 
+// S(i, j) = S(i, j) - acc for i < nr, j < nc, zero elsewhere: the update
+// pb_store(sub) applies, on a tile already in shared memory; with dst, the
+// updated values (i < nr, j < nc) also go to dst (leading dimension ld).
+template <typename T>
+__device__ __forceinline__ void pb_sub(T* S, int nr, int nc,
+                                       const T (&acc)[4][4],
+                                       T* dst = nullptr, int64_t ld = 0) {
+  constexpr int P = pld<T>();
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    const int j = PbMap<T>::col(b);
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const int i = PbMap<T>::row(a);
+      const bool in = i < nr && j < nc;
+      const T v = in ? S[i + j * P] - acc[a][b] : (T)0;
+      S[i + j * P] = v;
+      if (dst && in) dst[i + j * ld] = v;
+    }
+  }
+}
+
 // Dynamic shared memory: three tile buffers (the diagonal-tile
 // factorization's D / Linv / Uinv, reused as product tiles).
 template <typename T>
@@ -322,39 +359,45 @@ __global__ void __launch_bounds__(256, 2)
     const int dim = f.p + f.q;
     const int K1 = min(K0 + OB_COLS, f.p);
     const int nt = (K1 - K0 + NB - 1) / NB;
-    // two flags per tile: [2 s] tile factored and its first U chunk (the
-    // next tile's columns) written, [2 s + 1] all its U rows written
-    int* fl = tflags + 2 * flag_off[tk.front];
+    // four flags per tile (above)
+    int* fl = tflags + 4 * flag_off[tk.front];
     T* Fo = F + f.off;
     const int64_t ld = f.ld;
     if (tk.kind == 0) {
       const int R0 = K0 + NB * tk.chunk, nr = min(NB, dim - R0);
-      int deferred = -1;  // step whose remaining column chunks wait
-      bool pre = false;   // S1 holds our updated diagonal tile
+      int deferred = -1;  // step whose update of our columns past the next
+                          // tile waits until our tile is factored
+      bool pre = false;   // S0 holds our updated diagonal tile
       for (int t = 0; t < nt; t++) {
         const int k0 = K0 + NB * t, kb = min(NB, f.p - k0), k1 = k0 + kb;
         const int step = k0 / NB;
+        // tile t's flags and inverses (Linv_t, then Uinv_t), formed where
+        // they are used
+        auto tflag = [&](int k) { return fl + 4 * step + k; };
+        auto tinv = [&](int u) {
+          return INV + f.inv_off + (int64_t)step * 2 * NB * NB + u * NB * NB;
+        };
         if (tk.chunk == t) {
           // owner: the diagonal tile (its columns are up to date)
-          // (Linv comes back in S0, product layout; the tile from S1 when
-          // our update of the previous step left it there)
+          // (Linv comes back in S0, product layout; the tile from S0 when
+          // our work as the next owner left it there)
           diag_tile<T>(f, F, INV, k0, step, eps, dflags, S0, S1, S2, S0,
-                       pre ? S1 : (const T*)nullptr);
+                       pre ? S0 : (const T*)nullptr);
           __syncthreads();
+          if (threadIdx.x == 0) raise_flag(tflag(0));
           const int pk0 = K0 + NB * max(deferred, 0);
           if (deferred >= 0) {
-            // the previous step's update of our rows right of this tile
-            if (threadIdx.x == 0 && !wait_flag(fl + 2 * (pk0 / NB) + 1, err))
+            // the previous step's update of our rows past the next tile
+            if (threadIdx.x == 0 && !wait_flag(fl + 4 * (pk0 / NB) + 1, err))
               bad = 1;
             __syncthreads();
             if (bad) return;
             pb_load(S1, Fo + R0 + pk0 * ld, ld, nr, NB);  // our L block
           }
-          // per column chunk right of the tile: the deferred update of our
-          // rows, then the U rows (U = Linv A); the first chunk (the next
-          // tile's columns) is published on its own, the next owner needs
-          // only it
-          for (int c0 = k1; c0 < K1; c0 += NB) {
+          // per column chunk past the next tile (whose U rows the next
+          // owner forms): the deferred update of our rows, then the U rows
+          // (U = Linv A)
+          for (int c0 = k1 + NB; c0 < K1; c0 += NB) {
             const int nc = min(NB, K1 - c0);
             T acc[4][4];
             bool have = false;  // S2 holds our updated rows of these columns
@@ -371,17 +414,12 @@ __global__ void __launch_bounds__(256, 2)
             pb_mm(acc, S0, S2, kb);  // Linv A
             pb_store(Fo + k0 + c0 * ld, ld, kb, nc, acc, false, (T*)nullptr);
             __syncthreads();
-            if (c0 == k1 && threadIdx.x == 0) raise_flag(fl + 2 * step);
           }
-          if (threadIdx.x == 0) {
-            if (k1 >= K1) raise_flag(fl + 2 * step);
-            raise_flag(fl + 2 * step + 1);
-          }
+          if (threadIdx.x == 0) raise_flag(tflag(1));
           // a partial last tile: the chunk's rows past it are L rows
           // (L = A Uinv); nothing is right of the block
           if (k1 < R0 + nr) {
-            pb_load(S1, INV + f.inv_off + (int64_t)step * 2 * NB * NB + NB * NB,
-                    (int64_t)NB, NB, NB);
+            pb_load(S1, tinv(1), (int64_t)NB, NB, NB);
             pb_load(S0, Fo + k1 + k0 * ld, ld, R0 + nr - k1, kb);
             __syncthreads();
             T acc[4][4];
@@ -392,16 +430,67 @@ __global__ void __launch_bounds__(256, 2)
           }
           break;  // the owner's rows are complete in this block
         }
-        // the next tile's owner only needs this tile's first U chunk now
-        const bool next_owner = tk.chunk == t + 1;
-        if (threadIdx.x == 0 &&
-            !wait_flag(fl + 2 * step + (next_owner ? 0 : 1), err))
-          bad = 1;
+        if (tk.chunk == t + 1 && k1 < K1) {
+          // the next tile's owner (a full tile t: the block goes on)
+          const int c0 = k1, nc = min(NB, K1 - c0);  // our tile's columns
+          T acc[4][4];
+          // (1) while tile t is factored: S2 = tile t's rows in our
+          // columns, with the previous step's update that its owner left
+          if (t > 0) {
+            // (step t - 1's flags [4 (step - 1) + 3] and [+ 1])
+            if (threadIdx.x == 0 && (!wait_flag(tflag(-1), err) ||
+                                     !wait_flag(tflag(-3), err)))
+              bad = 1;
+            __syncthreads();
+            if (bad) return;
+            pb_load(S0, Fo + k0 + (k0 - NB) * ld, ld, NB, NB);  // L_t,t-1
+            pb_load(S1, Fo + (k0 - NB) + c0 * ld, ld, NB, nc);  // U_t-1
+            __syncthreads();
+            pb_mm(acc, S0, S1, NB);
+            pb_load(S2, Fo + k0 + c0 * ld, ld, NB, nc);
+            __syncthreads();
+            pb_sub(S2, NB, nc, acc);
+          } else {
+            pb_load(S2, Fo + k0 + c0 * ld, ld, NB, nc);
+          }
+          // (2) tile t factored: its U rows here (Linv_t S2), our L block
+          // (A Uinv_t) and the update of our diagonal tile, kept in S0
+          if (threadIdx.x == 0 && !wait_flag(tflag(0), err)) bad = 1;
+          __syncthreads();
+          if (bad) return;
+          pb_load(S0, tinv(0), (int64_t)NB, NB, NB);        // Linv_t
+          pb_load(S1, Fo + R0 + k0 * ld, ld, nr, kb);   // our rows of tile t
+          __syncthreads();
+          pb_mm(acc, S0, S2, kb);
+          __syncthreads();
+          pb_store(Fo + k0 + c0 * ld, ld, kb, nc, acc, false, S2);  // S2 = U
+          pb_load(S0, tinv(1), (int64_t)NB, NB, NB);          // Uinv_t
+          __syncthreads();
+          if (threadIdx.x == 0) raise_flag(tflag(2));
+          pb_mm(acc, S1, S0, kb);
+          __syncthreads();
+          pb_store(Fo + R0 + k0 * ld, ld, nr, kb, acc, false, S1);  // S1 = L
+          pb_load(S0, Fo + R0 + c0 * ld, ld, nr, nc);               // our tile
+          __syncthreads();
+          if (threadIdx.x == 0) raise_flag(tflag(3));
+          // (the whole updated tile also goes back to the front: our rows
+          // past the front's last pivot, if any, are L rows that we read
+          // back from there as the tile's owner)
+          pb_mm(acc, S1, S2, kb);
+          pb_sub(S0, nr, nc, acc, Fo + R0 + c0 * ld, ld);
+          __syncthreads();
+          pre = true;
+          if (c0 + NB < K1) deferred = t;
+          continue;
+        }
+        // tile t factored: the L block of our rows (A Uinv_t), then the
+        // rank-64 update of our rows inside the block, columns [k1, K1):
+        // the next tile's U rows come from its owner, the rest from tile
+        // t's owner
+        if (threadIdx.x == 0 && !wait_flag(tflag(0), err)) bad = 1;
         __syncthreads();
         if (bad) return;
-        // L block of our rows: A Uinv_t
-        pb_load(S1, INV + f.inv_off + (int64_t)step * 2 * NB * NB + NB * NB,
-                (int64_t)NB, NB, NB);
+        pb_load(S1, tinv(1), (int64_t)NB, NB, NB);
         pb_load(S0, Fo + R0 + k0 * ld, ld, nr, kb);
         __syncthreads();
         T acc[4][4];
@@ -409,21 +498,18 @@ __global__ void __launch_bounds__(256, 2)
         __syncthreads();
         pb_store(Fo + R0 + k0 * ld, ld, nr, kb, acc, false, S0);  // S0 = L
         __syncthreads();
-        // rank-64 update of our rows inside the block: columns [k1, K1)
-        // (the next owner takes the first chunk now, the rest after its tile)
         for (int c0 = k1; c0 < K1; c0 += NB) {
-          if (next_owner && c0 > k1) {
-            deferred = t;
-            break;
+          if (c0 - k1 < 2 * NB) {
+            if (threadIdx.x == 0 && !wait_flag(tflag(c0 == k1 ? 2 : 1), err))
+              bad = 1;
+            __syncthreads();
+            if (bad) return;
           }
           const int nc = min(NB, K1 - c0);
-          pb_load(S2, Fo + k0 + c0 * ld, ld, kb, nc);  // U (from the owner)
+          pb_load(S2, Fo + k0 + c0 * ld, ld, kb, nc);  // U rows of tile t
           __syncthreads();
           pb_mm(acc, S0, S2, kb);
-          // the next owner keeps its updated tile in S1 (free: Uinv is used)
-          pb_store(Fo + R0 + c0 * ld, ld, nr, nc, acc, true,
-                   next_owner ? S1 : (T*)nullptr);
-          pre = next_owner;
+          pb_store(Fo + R0 + c0 * ld, ld, nr, nc, acc, true, (T*)nullptr);
           __syncthreads();
         }
       }
@@ -432,7 +518,8 @@ __global__ void __launch_bounds__(256, 2)
       for (int t = 0; t < nt; t++) {
         const int k0 = K0 + NB * t, kb = min(NB, f.p - k0);
         const int step = k0 / NB;
-        if (threadIdx.x == 0 && !wait_flag(fl + 2 * step + 1, err)) bad = 1;
+        // tile t factored (with every L block of its rows)
+        if (threadIdx.x == 0 && !wait_flag(fl + 4 * step, err)) bad = 1;
         __syncthreads();
         if (bad) return;
         // S2 = A_t - sum_{s<t} L_ts U_s  (our columns)
