@@ -418,6 +418,15 @@ SNU_API void snu_free(void* p);
    flag that nothing sets and returns its status: SNU_ETIMEOUT (after well
    under a second) is the expected answer; the device stays usable. */
 SNU_API snu_status snu_selftest_wait_timeout(int device);
+/* The FP32 tile factorization forms each pivot's reciprocal as a hardware
+   approximation refined by one Newton-Raphson step.  This compares it with
+   the correctly rounded reciprocal on n inputs drawn from seed (every sign,
+   mantissa and an exponent in [-120, 120]): *max_ulp = the largest
+   difference in units in the last place, *differ = the inputs where the
+   two differ. */
+SNU_API snu_status snu_selftest_pivot_reciprocal(int device, int64_t n,
+                                                uint64_t seed, int* max_ulp,
+                                                int64_t* differ);
 
 #ifdef __cplusplus
 }

@@ -956,6 +956,22 @@ SNU_API snu_status snu_selftest_wait_timeout(int device) {
   }
 }
 
+SNU_API snu_status snu_selftest_pivot_reciprocal(int device, int64_t n,
+                                                uint64_t seed, int* max_ulp,
+                                                int64_t* differ) {
+  if (n < 0 || !max_ulp || !differ)
+    return fail(nullptr, SNU_EINVAL, "bad arguments");
+  std::string err;
+  int m = 0;
+  int64_t dcount = 0;
+  int rc = snu::recip_selftest(device, n, seed, m, dcount, err);
+  g_err = err;
+  if (rc != snu::ENG_OK) return rc == snu::ENG_ENOMEM ? SNU_ENOMEM : SNU_ECUDA;
+  *max_ulp = m;
+  *differ = dcount;
+  return SNU_OK;
+}
+
 }  // extern "C"
 
 namespace snu {

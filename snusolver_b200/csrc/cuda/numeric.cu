@@ -3029,6 +3029,63 @@ int wait_selftest(int device, std::string& err) {
   return ENG_OK;
 }
 
+// out[0] = the largest difference in ulps between pivot_recip(x) and the
+// correctly rounded 1 / x, out[1] = the inputs where they differ.  Inputs:
+// sign, 23 mantissa bits and an exponent in [-120, 120] from the SplitMix64
+// mixer (Steele, Lea and Flood, 2014) applied to seed + index.
+__global__ void k_recip_selftest(int64_t n, uint64_t seed,
+                                 unsigned long long* out) {
+  unsigned long long mx = 0, cnt = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t z = seed + (uint64_t)i * 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    const uint32_t e = (uint32_t)((z >> 24) % 241u) + 7u;  // biased 7..247
+    const uint32_t bits =
+        ((uint32_t)(z >> 23) & 1u) << 31 | e << 23 | ((uint32_t)z & 0x7fffffu);
+    const float x = __uint_as_float(bits);
+    const int32_t a = __float_as_int(pivot_recip(x));
+    const int32_t b = __float_as_int(__frcp_rn(x));
+    // same sign and finite: the integer distance of the bit patterns
+    const unsigned long long d =
+        (a ^ b) < 0 ? ~0ull : (unsigned long long)(a > b ? a - b : b - a);
+    mx = d > mx ? d : mx;
+    cnt += d != 0;
+  }
+  atomicMax(out, mx);
+  atomicAdd(out + 1, cnt);
+}
+
+int recip_selftest(int device, int64_t n, uint64_t seed, int& max_ulp,
+                   int64_t& differ, std::string& err) {
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    err = "cannot select the device";
+    return ENG_ECUDA;
+  }
+  unsigned long long* d = nullptr;
+  if (cudaMalloc((void**)&d, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    err = "cudaMalloc failed";
+    return ENG_ENOMEM;
+  }
+  unsigned long long h[2] = {0, 0};
+  cudaMemset(d, 0, sizeof h);
+  k_recip_selftest<<<148 * 4, 256>>>(n, seed, d);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    err = cudaGetErrorString(e);
+    return ENG_ECUDA;
+  }
+  max_ulp = h[0] > 0x7fffffffull ? 0x7fffffff : (int)h[0];
+  differ = (int64_t)h[1];
+  return ENG_OK;
+}
+
 const char* kernel_family_name(int f) {
   static const char* names[KF_COUNT] = {
       "assemble", "extend_add", "diag_lu", "panel_trsm", "gemm_trail",

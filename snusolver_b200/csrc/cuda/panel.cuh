@@ -74,6 +74,23 @@ __device__ __forceinline__ bool aligned16(const T* p) {
 __device__ __forceinline__ float recip_rn(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double recip_rn(double x) { return __drcp_rn(x); }
 
+// The pivot reciprocal of the tile factorization, on the pivot chain.
+// FP32: the hardware approximation (rcp.approx.f32) refined by one
+// Newton-Raphson step in its FMA form, e = 1 - x r0, r = r0 + r0 e
+// (Markstein, "IA-64 and Elementary Functions", 2000): the refined value
+// is within one ulp of the correctly rounded reciprocal and nearly always
+// equal to it (snu_check_pivot_reciprocal measures both on the GPU), at
+// about half the latency of the correctly rounded one.  FP64: the correctly
+// rounded reciprocal.  A zero or infinite FP32 pivot gives NaN here; the
+// tile factorization flags such pivots either way.
+__device__ __forceinline__ float pivot_recip(float x) {
+  float r;
+  asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  const float e = fmaf(-x, r, 1.f);
+  return fmaf(r, e, r);
+}
+__device__ __forceinline__ double pivot_recip(double x) { return __drcp_rn(x); }
+
 // Dynamic shared memory of k_diag_lu_inv: the tile and its two inverses.
 template <typename T>
 constexpr size_t diag_smem() {
@@ -303,7 +320,7 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
         // (1 / +-eps is +-rteps exactly)
         const bool live = s0 + k < kb;
         const bool g = guard & live & (piv < teps) & (piv > -teps);
-        const T rraw = recip_rn(piv);
+        const T rraw = pivot_recip(piv);
         const T rp = g ? (piv < (T)0 ? -rteps : rteps) : rraw;
         piv = g ? (piv < (T)0 ? -teps : teps) : piv;
         nguard += g;
@@ -355,8 +372,36 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
         for (int i = 0; i < SB; i++) D[s0 + i + c * TLD] = y[i];
       }
       __syncthreads();
-      // (3) rank-SB update of the rest of the tile
+      // (3) rank-SB update of the rest of the tile; the first sub-block's
+      // 48 x 48 update in 3 x 3 register tiles (rows tx + 16 a, columns
+      // ty + 16 b: six shared loads per nine FMAs instead of one per FMA),
+      // the smaller ones one element at a time; every element takes the
+      // same FMAs in the same order either way
       const int tx = tid & 15, ty = tid >> 4;
+      if (rem == 3 * SB) {
+        T acc[3][3], l[3], u[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+          for (int b = 0; b < 3; b++)
+            acc[a][b] = D[s0 + SB + tx + 16 * a + (s0 + SB + ty + 16 * b) * TLD];
+#pragma unroll
+        for (int t = 0; t < SB; t++) {
+#pragma unroll
+          for (int a = 0; a < 3; a++) l[a] = D[s0 + SB + tx + 16 * a + (s0 + t) * TLD];
+#pragma unroll
+          for (int b = 0; b < 3; b++) u[b] = D[s0 + t + (s0 + SB + ty + 16 * b) * TLD];
+#pragma unroll
+          for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) acc[a][b] -= l[a] * u[b];
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+          for (int b = 0; b < 3; b++)
+            D[s0 + SB + tx + 16 * a + (s0 + SB + ty + 16 * b) * TLD] = acc[a][b];
+      } else
       for (int jj = ty; jj < rem; jj += 16) {
         const int j = s0 + SB + jj;
         T u[SB];

@@ -70,6 +70,10 @@ const char* kernel_family_name(int f);
 // Runs the bounded-wait self-test on a device (ENG_ETIMEOUT when the wait
 // ran out as it must).
 int wait_selftest(int device, std::string& err);
+// Compares the FP32 pivot reciprocal of the tile factorization with the
+// correctly rounded reciprocal on n generated inputs (see the C-ABI).
+int recip_selftest(int device, int64_t n, uint64_t seed, int& max_ulp,
+                   int64_t& differ, std::string& err);
 
 struct KernelStat {
   int64_t launches = 0;

@@ -6,6 +6,8 @@ relative residual <= 1e-12.  FP32+IR path: relative residual <= 1e-10.
 The references are the golden fixtures (made by oracle/_ref, the reference
 built from its sources) and the C restatement oracle/snu_oracle.c run live.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -446,3 +448,18 @@ def test_wide_solve_passes_and_host_copies(gpu, precision, tol, res):
     torch.cuda.synchronize()
     Xd = dX.cpu().numpy().T
     assert np.abs(Xd - X[:, :40]).max() <= tol * np.abs(X[:, :40]).max()
+
+
+def test_pivot_reciprocal_against_correctly_rounded(gpu):
+    # the FP32 tile factorization's pivot reciprocal (hardware approximation
+    # + one Newton-Raphson step) against CUDA's correctly rounded reciprocal
+    lib = C.CDLL(snu.library_path())
+    f = lib.snu_selftest_pivot_reciprocal
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int64, C.c_uint64, C.POINTER(C.c_int),
+                  C.POINTER(C.c_int64)]
+    n = 1 << 24
+    mx, nd = C.c_int(-1), C.c_int64(-1)
+    assert f(0, n, 11, C.byref(mx), C.byref(nd)) == 0
+    assert 0 <= mx.value <= 1, (mx.value, nd.value)  # within one ulp
+    assert 0 <= nd.value <= n // 10000, nd.value    # nearly always equal
