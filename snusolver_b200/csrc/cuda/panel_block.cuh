@@ -53,14 +53,23 @@ struct BlockTask {
   int front, kind, chunk;  // kind 0: row chunk, 1: column chunk
 };
 
+// The 16-row block of warp w in the 64 x 64 products: warps 0-3 take row
+// blocks 0, 1, 2, 3 and warps 4-7 (which share the SM sub-partitions of
+// warps 0-3) blocks 3, 2, 1, 0, so a product with a lower-triangular left
+// operand, whose row block r needs only the first 16 (r + 1) of the inner
+// dimension, gives every sub-partition the same work.
+__device__ __forceinline__ int pb_rb(int w) {
+  return 16 * ((w & 3) ^ (3 * (w >> 2)));
+}
+
 // Register tile of a thread in the 64 x 64 products: rows row(a), columns
 // col(b) (a, b < 4) -- the accumulator fragments of the tensor-core
 // products (pb_mm): rows r0 + {0, 1, 8, 9}, columns c0 + 8 b, a warp
-// covering 16 rows x 32 columns.
+// covering 16 rows (pb_rb) x 32 columns.
 template <typename T>
 struct PbMap {
   __device__ __forceinline__ static int r0() {
-    return ((threadIdx.x >> 5) & 3) * 16 + (threadIdx.x & 3) * 2;
+    return pb_rb(threadIdx.x >> 5) + (threadIdx.x & 3) * 2;
   }
   __device__ __forceinline__ static int c0() {
     return (threadIdx.x >> 7) * 32 + ((threadIdx.x >> 2) & 7);
@@ -140,16 +149,21 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4],
 
 // acc = A B for NB x NB shared tiles (leading dimension PLD, inner
 // dimension kk); the operands are zero (or finite identity padding against
-// zeros) past kk, so the loop runs to kk rounded up to 8.
+// zeros) past kk, so the loop runs to kk rounded up to 8.  tri = PB_LOWER_A:
+// A is lower triangular (a tile inverse Linv), so a warp's rows [rb, rb+16)
+// need the inner dimension below rb + 16 only; tri = PB_UPPER_B: B is upper
+// triangular (Uinv), a warp's columns [cb, cb + 32) need it below cb + 32.
+// The skipped products are exact zeros.
 // On the tensor cores, formed as C^T = B^T A^T so that each thread's
 // accumulator fragments are its PbMap elements.  FP32: mma.sync m16n8k8
 // TF32 with the three-product split (A_hi B_hi + A_hi B_lo + A_lo B_hi,
 // FP32 accumulation: FP32-level products); a warp's 16 x 32 block is 2 x 2
 // MMA tiles (16 columns x 8 rows each).  FP64: mma.sync m8n8k4 f64 (exact
 // FP64 products); the block is 4 x 2 tiles (8 columns x 8 rows each).
+constexpr int PB_FULL = 0, PB_LOWER_A = 1, PB_UPPER_B = 2;
 template <typename T>
 __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
-                                      int kk) {
+                                      int kk, int tri = PB_FULL) {
   constexpr int P = pld<T>();
 #pragma unroll
   for (int a = 0; a < 4; a++)
@@ -158,14 +172,16 @@ __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
   if constexpr (sizeof(T) == 8) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int rb = 16 * (w & 3), cb = 32 * (w >> 2);
+    const int rb = pb_rb(w), cb = 32 * (w >> 2);
     // d[i][j]: column cb + 8 i + g, rows rb + 8 j + 2 t + {0, 1}
     double d[4][2][2];
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
       for (int j = 0; j < 2; j++) d[i][j][0] = d[i][j][1] = 0.0;
-    const int k4 = (kk + 3) & ~3;
+    const int k4 = min((kk + 3) & ~3, tri == PB_LOWER_A   ? rb + 16
+                                      : tri == PB_UPPER_B ? cb + 32
+                                                          : NB);
 #pragma unroll 2
     for (int k0 = 0; k0 < k4; k0 += 4) {
       double av[4], bv[2];
@@ -191,7 +207,7 @@ __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
   } else {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int rb = 16 * (w & 3), cb = 32 * (w >> 2);
+    const int rb = pb_rb(w), cb = 32 * (w >> 2);
     // d[i][j]: columns cb + 16 i + {g, g + 8}, rows rb + 8 j + 2 t + {0, 1}
     float d[2][2][4];
 #pragma unroll
@@ -200,7 +216,9 @@ __device__ __forceinline__ void pb_mm(T (&acc)[4][4], const T* A, const T* B,
       for (int j = 0; j < 2; j++)
 #pragma unroll
         for (int e = 0; e < 4; e++) d[i][j][e] = 0.f;
-    const int k8 = (kk + 7) & ~7;
+    const int k8 = min((kk + 7) & ~7, tri == PB_LOWER_A   ? rb + 16
+                                      : tri == PB_UPPER_B ? cb + 32
+                                                          : NB);
 #pragma unroll 1
     for (int k0 = 0; k0 < k8; k0 += 8) {
       // MMA A operand (16 x 8, row-major) = B^T: element (m, k) = B(k, m)
@@ -411,7 +429,7 @@ __global__ void __launch_bounds__(256, 2)
             }
             if (!have) pb_load(S2, Fo + k0 + c0 * ld, ld, kb, nc);
             __syncthreads();
-            pb_mm(acc, S0, S2, kb);  // Linv A
+            pb_mm(acc, S0, S2, kb, PB_LOWER_A);  // Linv A
             pb_store(Fo + k0 + c0 * ld, ld, kb, nc, acc, false, (T*)nullptr);
             __syncthreads();
           }
@@ -423,7 +441,7 @@ __global__ void __launch_bounds__(256, 2)
             pb_load(S0, Fo + k1 + k0 * ld, ld, R0 + nr - k1, kb);
             __syncthreads();
             T acc[4][4];
-            pb_mm(acc, S0, S1, kb);
+            pb_mm(acc, S0, S1, kb, PB_UPPER_B);
             pb_store(Fo + k1 + k0 * ld, ld, R0 + nr - k1, kb, acc, false,
                      (T*)nullptr);
             __syncthreads();
@@ -461,13 +479,13 @@ __global__ void __launch_bounds__(256, 2)
           pb_load(S0, tinv(0), (int64_t)NB, NB, NB);        // Linv_t
           pb_load(S1, Fo + R0 + k0 * ld, ld, nr, kb);   // our rows of tile t
           __syncthreads();
-          pb_mm(acc, S0, S2, kb);
+          pb_mm(acc, S0, S2, kb, PB_LOWER_A);
           __syncthreads();
           pb_store(Fo + k0 + c0 * ld, ld, kb, nc, acc, false, S2);  // S2 = U
           pb_load(S0, tinv(1), (int64_t)NB, NB, NB);          // Uinv_t
           __syncthreads();
           if (threadIdx.x == 0) raise_flag(tflag(2));
-          pb_mm(acc, S1, S0, kb);
+          pb_mm(acc, S1, S0, kb, PB_UPPER_B);
           __syncthreads();
           pb_store(Fo + R0 + k0 * ld, ld, nr, kb, acc, false, S1);  // S1 = L
           pb_load(S0, Fo + R0 + c0 * ld, ld, nr, nc);               // our tile
@@ -494,7 +512,7 @@ __global__ void __launch_bounds__(256, 2)
         pb_load(S0, Fo + R0 + k0 * ld, ld, nr, kb);
         __syncthreads();
         T acc[4][4];
-        pb_mm(acc, S0, S1, kb);
+        pb_mm(acc, S0, S1, kb, PB_UPPER_B);
         __syncthreads();
         pb_store(Fo + R0 + k0 * ld, ld, nr, kb, acc, false, S0);  // S0 = L
         __syncthreads();
@@ -544,7 +562,7 @@ __global__ void __launch_bounds__(256, 2)
                 (int64_t)NB, NB, NB);
         __syncthreads();
         T acc[4][4];
-        pb_mm(acc, S0, S2, kb);
+        pb_mm(acc, S0, S2, kb, PB_LOWER_A);
         pb_store(Fo + k0 + C0 * ld, ld, kb, nc, acc, false, (T*)nullptr);
         __syncthreads();
       }
