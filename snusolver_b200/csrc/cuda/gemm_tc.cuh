@@ -8,10 +8,11 @@
 // kind::tf32: FP32-level accuracy) and BF16x3 (bf16 hi and lo, kind::f16
 // with both operands bf16: about 2^-16 relative per product, twice the MMA
 // rate and half the operand bytes; FP64 refinement recovers the rest).
-// A pack kernel writes the three products as one GEMM of depth 3*kpad:
-// A' = [A_hi | A_hi | A_lo] and B' = [B_hi ; B_lo ; B_hi], both K-major
-// (row-major in K), kpad = k rounded up to one 128-byte row (32 tf32, 64
-// bf16).  The GEMM kernel then runs a plain GEMM: TMA loads 128 x 128-byte
+// A pack kernel writes the two planes of each operand, A' = [A_hi | A_lo]
+// and B' = [B_hi | B_lo], both K-major (row-major in K), kpad = k rounded
+// up to one 128-byte row (32 tf32, 64 bf16).  The GEMM kernel then runs
+// the three products as one GEMM of depth 3*kpad, hi.hi, hi.lo, lo.hi: its
+// k-block kb takes the plane split_coords picks.  TMA loads 128 x 128-byte
 // (A') and BN x 128-byte (B') tiles with 128-byte swizzle into a
 // STAGES-deep shared-memory ring, one thread issues tcgen05.mma (M=128,
 // N=BN) into a TMEM accumulator, and the four warps read the accumulator
@@ -81,7 +82,20 @@ struct Split<true> {
   }
 };
 
-// A' (m rows x 3*kpad) from A (m x k, column-major): 32 x 32 blocks through
+// The x coordinates (elements along K) of k-block kb of the three-product
+// GEMM in the two-plane operands: thirds hi.hi, hi.lo, lo.hi of the depth
+// 3*kpad, so A takes planes hi, hi, lo and B planes hi, lo, hi.  Every x
+// is a multiple of one 128-byte row.
+template <bool BF>
+__device__ __forceinline__ void split_coords(const TcProb& p, int kb, int& xa,
+                                             int& xb) {
+  const int kp = Split<BF>::kpad(p), nkb = kp / Split<BF>::KB;
+  const int third = kb / nkb, off = (kb - third * nkb) * Split<BF>::KB;
+  xa = (third == 2 ? kp : 0) + off;
+  xb = (third == 1 ? kp : 0) + off;
+}
+
+// A' (m rows x 2*kpad) from A (m x k, column-major): 32 x 32 blocks through
 // shared memory so both the column-major reads and the row-major writes are
 // coalesced.  grid: (kpad/32, ceil(m/32), problems); block 32 x 8.
 template <bool BF>
@@ -101,7 +115,7 @@ __global__ void k_tc_pack_a(const TcProb* __restrict__ probs,
   }
   __syncthreads();
   E* out = reinterpret_cast<E*>(P + pr.apack);
-  const int64_t kk = 3 * (int64_t)kp;
+  const int64_t kk = 2 * (int64_t)kp;
   for (int rr = threadIdx.y; rr < 32; rr += 8) {
     int r = r0 + rr, c = c0 + threadIdx.x;
     if (r >= pr.m) continue;
@@ -109,12 +123,11 @@ __global__ void k_tc_pack_a(const TcProb* __restrict__ probs,
     Split<BF>::apply(t[threadIdx.x][rr], hi, lo);
     E* row = out + r * kk;
     row[c] = hi;
-    row[kp + c] = hi;
-    row[2 * kp + c] = lo;
+    row[kp + c] = lo;
   }
 }
 
-// B' (n rows x 3*kpad) from B (k x n, column-major): column c of B is row c
+// B' (n rows x 2*kpad) from B (k x n, column-major): column c of B is row c
 // of B', already contiguous.  grid: (ceil(n/8), problems); block 256.
 template <bool BF>
 __global__ void k_tc_pack_b(const TcProb* __restrict__ probs,
@@ -127,13 +140,12 @@ __global__ void k_tc_pack_b(const TcProb* __restrict__ probs,
   if (c >= pr.n) return;
   const float* B = F + pr.b + (int64_t)c * pr.ldb;
   const int kp = Split<BF>::kpad(pr);
-  E* row = reinterpret_cast<E*>(P + pr.bpack) + (int64_t)c * 3 * kp;
+  E* row = reinterpret_cast<E*>(P + pr.bpack) + (int64_t)c * 2 * kp;
   for (int kk = lane; kk < kp; kk += 32) {
     E hi, lo;
     Split<BF>::apply(kk < pr.k ? B[kk] : 0.f, hi, lo);
     row[kk] = hi;
     row[kp + kk] = lo;
-    row[2 * kp + kk] = hi;
   }
 }
 
@@ -307,9 +319,11 @@ __global__ void __launch_bounds__(128, 1)
         break;
       }
       mbar_expect_tx(&full_bar[s], (TC_BM + BN) * TC_BK * sizeof(float));
-      tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * Split<BF>::KB, tl.tm * TC_BM,
+      int xa, xb;
+      split_coords<BF>(pr, kb, xa, xb);
+      tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, xa, tl.tm * TC_BM,
                   &full_bar[s]);
-      tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, kb * Split<BF>::KB, tl.tn * BN,
+      tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, xb, tl.tn * BN,
                   &full_bar[s]);
       issued = kb + 1;
     }
@@ -491,10 +505,12 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
           break;
         }
         mbar_expect_tx(&full_bar[s], (TC_BM + BN) * TC_BK * sizeof(float));
-        tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, kb * Split<BF>::KB,
-                    tl.tm * TC_BM, &full_bar[s]);
-        tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, kb * Split<BF>::KB,
-                    tl.tn * BN, &full_bar[s]);
+        int xa, xb;
+        split_coords<BF>(pr, kb, xa, xb);
+        tma_load_2d(As + (size_t)s * TC_BM * TC_BK, am, xa, tl.tm * TC_BM,
+                    &full_bar[s]);
+        tma_load_2d(Bs + (size_t)s * BN * TC_BK, bm, xb, tl.tn * BN,
+                    &full_bar[s]);
       }
     }
     // every issued load has landed before the CTA may exit

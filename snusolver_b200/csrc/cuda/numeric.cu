@@ -1310,7 +1310,7 @@ class CudaEngine : public Engine {
       t.m = g.m, t.n = g.n, t.k = g.k;
       t.kpad = (g.k + 31) / 32 * 32;
       t.kpadb = (g.k + 63) / 64 * 64;
-      const int64_t row = 3 * std::max<int64_t>(4 * t.kpad, 2 * t.kpadb);
+      const int64_t row = 2 * std::max<int64_t>(4 * t.kpad, 2 * t.kpadb);
       t.a = g.a, t.b = g.b, t.c = g.c;
       t.lda = g.lda, t.ldb = g.ldb, t.ldc = g.ldc;
       t.pc = g.pc, t.rel = g.rel, t.pld = g.pld, t.mode = g.pad;
@@ -1365,7 +1365,7 @@ class CudaEngine : public Engine {
         const TcProb& t = gb->tc_host[k];
         const int tm = (t.m + TC_BM - 1) / TC_BM;
         for (int sp = 0; sp < 2; sp++) {  // TF32x3, BF16x3
-          const cuuint64_t kk = 3 * (cuuint64_t)(sp ? t.kpadb : t.kpad);
+          const cuuint64_t kk = 2 * (cuuint64_t)(sp ? t.kpadb : t.kpad);
           const CUtensorMapDataType dt = sp ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                             : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
           const cuuint32_t kbe = sp ? 64 : 32;  // one 128-byte row
