@@ -253,7 +253,10 @@ __device__ __forceinline__ void inv_join(const T* D, T* XL, T* XU, int tid,
 // Uinv (also written to INV), the factored tile is back in F and, when LP
 // is given (it may be D), Linv is also in LP with leading dimension PLD.
 // pre: the tile already in shared memory (leading dimension PLD), instead
-// of loading it from the front.
+// of loading it from the front.  dry: the same code on whatever D, XL, XU
+// and pre hold, writing nothing outside shared memory (no front, inverses
+// or pivot flags): run once, it brings this code into the SM's instruction
+// cache before a real call from the same call site.
 template <typename T>
 __device__ __forceinline__ void diag_tile(const FrontDev& f,
                                           T* __restrict__ F,
@@ -261,7 +264,8 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
                                           int step, double eps, int* flags,
                                           T* D, T* XL, T* XU,
                                           T* LP = nullptr,
-                                          const T* pre = nullptr) {
+                                          const T* pre = nullptr,
+                                          bool dry = false) {
   __shared__ T rdiag[NB];  // 1 / U[i][i]
   const int kb = min(NB, f.p - k0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -334,7 +338,7 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
         for (int j = k + 1; j < SB; j++) v[j] = upd ? v[j] - l * rowk[j] : v[j];
         if (lane == 0) rdiag[s0 + k] = rp;
       }
-      if (lane == 0) {
+      if (lane == 0 && !dry) {
         if (nguard) atomicAdd(flags, nguard);
         if (bad) flags[1] = 1;
       }
@@ -420,7 +424,9 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
   }
   // factored tile back to the front (four rows per vector store when the
   // tile is full and its columns are 16-byte aligned)
-  if (kb == NB && aligned16(base) && (f.ld & 3) == 0) {
+  if (dry) {
+    // (a dry run writes nothing outside shared memory)
+  } else if (kb == NB && aligned16(base) && (f.ld & 3) == 0) {
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int e = tid + 256 * q, i = (e & 15) * 4, j = e >> 4;
@@ -468,7 +474,9 @@ __device__ __forceinline__ void diag_tile(const FrontDev& f,
   // stage B: the off-diagonal blocks
   inv_join<T>(D, XL, XU, tid, nbk);
   T* inv = INV + f.inv_off + (int64_t)step * 2 * NB * NB;
-  if (aligned16(inv)) {
+  if (dry) {
+    // (nor the inverses)
+  } else if (aligned16(inv)) {
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int e = tid + 256 * q, i = (e & 15) * 4, j = e >> 4;

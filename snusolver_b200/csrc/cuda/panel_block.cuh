@@ -395,13 +395,46 @@ __global__ void __launch_bounds__(256, 2)
         auto tinv = [&](int u) {
           return INV + f.inv_off + (int64_t)step * 2 * NB * NB + u * NB * NB;
         };
-        if (tk.chunk == t) {
+        const bool own = tk.chunk == t;
+        // the next tile's owner (a full tile t: the block goes on)
+        const bool next = tk.chunk == t + 1 && k1 < K1;
+        if (next) {
+          const int c0n = k1, ncn = min(NB, K1 - c0n);  // our tile's columns
+          // (1) while tile t is factored: S2 = tile t's rows in our
+          // columns, with the previous step's update that its owner left
+          if (t > 0) {
+            // (step t - 1's flags [4 (step - 1) + 3] and [+ 1])
+            if (threadIdx.x == 0 && (!wait_flag(tflag(-1), err) ||
+                                     !wait_flag(tflag(-3), err)))
+              bad = 1;
+            __syncthreads();
+            if (bad) return;
+            T acc[4][4];
+            pb_load(S0, Fo + k0 + (k0 - NB) * ld, ld, NB, NB);  // L_t,t-1
+            pb_load(S1, Fo + (k0 - NB) + c0n * ld, ld, NB, ncn);  // U_t-1
+            __syncthreads();
+            pb_mm(acc, S0, S1, NB);
+            pb_load(S2, Fo + k0 + c0n * ld, ld, NB, ncn);
+            __syncthreads();
+            pb_sub(S2, NB, ncn, acc);
+          } else {
+            pb_load(S2, Fo + k0 + c0n * ld, ld, NB, ncn);
+          }
+        }
+        if (own || (next && f.p > 2 * OB_COLS)) {
           // owner: the diagonal tile (its columns are up to date)
           // (Linv comes back in S0, product layout; the tile from S0 when
-          // our work as the next owner left it there)
-          diag_tile<T>(f, F, INV, k0, step, eps, dflags, S0, S1, S2, S0,
-                       pre ? S0 : (const T*)nullptr);
+          // our work as the next owner left it there).  The next owner of
+          // a long front (a chain of separator tiles) runs this same call
+          // once, dry, on a 16 x 16 scratch tile in S0 / S1 (S2 keeps tile
+          // t's rows) while tile t is factored: the chain moves to another
+          // SM at every tile, and its code would otherwise start cold there
+          diag_tile<T>(f, F, INV, own ? k0 : f.p - SB, step, eps, dflags, S0,
+                       S1, own ? S2 : S1, own ? S0 : (T*)nullptr,
+                       own ? (pre ? S0 : (const T*)nullptr) : S0, !own);
           __syncthreads();
+        }
+        if (own) {
           if (threadIdx.x == 0) raise_flag(tflag(0));
           const int pk0 = K0 + NB * max(deferred, 0);
           if (deferred >= 0) {
@@ -448,29 +481,9 @@ __global__ void __launch_bounds__(256, 2)
           }
           break;  // the owner's rows are complete in this block
         }
-        if (tk.chunk == t + 1 && k1 < K1) {
-          // the next tile's owner (a full tile t: the block goes on)
+        if (next) {
           const int c0 = k1, nc = min(NB, K1 - c0);  // our tile's columns
           T acc[4][4];
-          // (1) while tile t is factored: S2 = tile t's rows in our
-          // columns, with the previous step's update that its owner left
-          if (t > 0) {
-            // (step t - 1's flags [4 (step - 1) + 3] and [+ 1])
-            if (threadIdx.x == 0 && (!wait_flag(tflag(-1), err) ||
-                                     !wait_flag(tflag(-3), err)))
-              bad = 1;
-            __syncthreads();
-            if (bad) return;
-            pb_load(S0, Fo + k0 + (k0 - NB) * ld, ld, NB, NB);  // L_t,t-1
-            pb_load(S1, Fo + (k0 - NB) + c0 * ld, ld, NB, nc);  // U_t-1
-            __syncthreads();
-            pb_mm(acc, S0, S1, NB);
-            pb_load(S2, Fo + k0 + c0 * ld, ld, NB, nc);
-            __syncthreads();
-            pb_sub(S2, NB, nc, acc);
-          } else {
-            pb_load(S2, Fo + k0 + c0 * ld, ld, NB, nc);
-          }
           // (2) tile t factored: its U rows here (Linv_t S2), our L block
           // (A Uinv_t) and the update of our diagonal tile, kept in S0
           if (threadIdx.x == 0 && !wait_flag(tflag(0), err)) bad = 1;
