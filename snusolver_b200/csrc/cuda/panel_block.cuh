@@ -421,14 +421,15 @@ __global__ void __launch_bounds__(256, 2)
             pb_load(S2, Fo + k0 + c0n * ld, ld, NB, ncn);
           }
         }
-        if (own || (next && f.p > 2 * OB_COLS)) {
+        if (own || (next && f.p > OB_COLS)) {
           // owner: the diagonal tile (its columns are up to date)
           // (Linv comes back in S0, product layout; the tile from S0 when
           // our work as the next owner left it there).  The next owner of
-          // a long front (a chain of separator tiles) runs this same call
-          // once, dry, on a 16 x 16 scratch tile in S0 / S1 (S2 keeps tile
-          // t's rows) while tile t is factored: the chain moves to another
-          // SM at every tile, and its code would otherwise start cold there
+          // a front of more than one outer block (a long chain) runs this
+          // same call once, dry, on a 16 x 16 scratch tile in S0 / S1 (S2
+          // keeps tile t's rows) while tile t is factored: the chain moves
+          // to another SM at every tile, and its code would otherwise start
+          // cold there
           diag_tile<T>(f, F, INV, own ? k0 : f.p - SB, step, eps, dflags, S0,
                        S1, own ? S2 : S1, own ? S0 : (T*)nullptr,
                        own ? (pre ? S0 : (const T*)nullptr) : S0, !own);
