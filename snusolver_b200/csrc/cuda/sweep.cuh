@@ -104,19 +104,35 @@ __device__ __forceinline__ void stage_inv(T* Xs, const T* inv) {
 }
 
 // out[i][r] = sum_m Xs[i + m NB] in[m][r] for the kb x nr block; written to
-// Yf (ld p) as well.  Called by all threads of the CTA.
+// Yf (ld p) as well.  Called by all DIAG_ROWS threads of the CTA.  Thread
+// t takes row i = t % NB and columns r = t / NB + (DIAG_ROWS / NB) q: its
+// dot products share row i of the inverse and run side by side, each
+// summed over m in order.
 template <typename T, int R>
 __device__ __forceinline__ void tile_apply(const T* Xs, T (*in)[R],
                                            T (*out)[R], T* Yf, int ldy, int k0,
                                            int kb, int r0, int nr) {
-  for (int e = threadIdx.x; e < NB * R; e += blockDim.x) {
-    const int i = e % NB, r = e / NB;
-    T a = (T)0;
-#pragma unroll 16
-    for (int m = 0; m < NB; m++) a += Xs[i + m * NB] * in[m][r];
-    const bool ok = i < kb && r < nr;
-    out[i][r] = ok ? a : (T)0;
-    if (ok) Yf[k0 + i + (int64_t)(r0 + r) * ldy] = a;
+  static_assert(DIAG_ROWS % NB == 0, "a chunk is whole tiles");
+  constexpr int RS = DIAG_ROWS / NB, PER = (R + RS - 1) / RS;
+  const int i = threadIdx.x % NB, rb = threadIdx.x / NB;
+  T a[PER];
+#pragma unroll
+  for (int q = 0; q < PER; q++) a[q] = (T)0;
+#pragma unroll 8
+  for (int m = 0; m < NB; m++) {
+    const T x = Xs[i + m * NB];
+#pragma unroll
+    for (int q = 0; q < PER; q++)
+      if (rb + RS * q < R) a[q] += x * in[m][rb + RS * q];
+  }
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int r = rb + RS * q;
+    if (r < R) {
+      const bool ok = i < kb && r < nr;
+      out[i][r] = ok ? a[q] : (T)0;
+      if (ok) Yf[k0 + i + (int64_t)(r0 + r) * ldy] = a[q];
+    }
   }
 }
 
